@@ -1,0 +1,237 @@
+/*
+ * przmgpu.h -- C ABI of the B200 PRZM compression path (libprzmgpu.so).
+ *
+ * Drop-in boundary for the reference's Go `gpu` package (Lemon4ksan/przm,
+ * gpu/bridge.go, gpu/types.go, gpu/memory.go).  Every entry point below
+ * names the reference function it replaces.  A Go caller binds these through
+ * cgo; Python tests bind them through ctypes.
+ *
+ * Conventions
+ *   - status: int32, 0 = OK, negative = error (PRZMG_ERR_*); the numeric
+ *     values of the shared codes follow include/przm_dec.h of the reference;
+ *   - the caller owns every host buffer; the library owns device memory of a
+ *     context (grow-only pools, like ensureSlotCap, gpu/bridge.go:807-922);
+ *   - device pointers and CUDA streams travel as uint64_t (the reference
+ *     passes uint64 device pointers and uintptr streams);
+ *   - a context serialises its calls with an internal mutex, as every
+ *     GPUCompressor method does (for example gpu/bridge.go:1487-1488);
+ *   - empty inputs succeed with zero-length results (gpu/bridge.go:1089-1091).
+ */
+#ifndef PRZMGPU_H
+#define PRZMGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PRZMG_OK 0
+#define PRZMG_ERR_INVALID_ARG (-1)       /* same value as PRZM_ERR_CORRUPTED_FRAME */
+#define PRZMG_ERR_BUFFER_TOO_SMALL (-4)  /* PRZM_ERR_BUFFER_TOO_SMALL */
+#define PRZMG_ERR_EXCEEDS_MAX_BLOCK (-5) /* PRZM_ERR_EXCEEDS_MAX_BLOCK */
+#define PRZMG_ERR_CUDA (-10)             /* a CUDA runtime call failed (cuCheck, gpu/bridge.go:24-29) */
+#define PRZMG_ERR_UNAVAILABLE (-11)      /* no usable device (IsAvailable() == false) */
+#define PRZMG_ERR_MOCK (-12)             /* SetMockMatchErrorForTest is armed */
+#define PRZMG_ERR_DEVICE (-13)           /* a kernel reported an internal bound violation */
+#define PRZMG_ERR_NOT_FOUND (-14)        /* serving: unknown request id */
+#define PRZMG_ERR_BUSY (-15)             /* serving: admission refused (budget or queue full) */
+
+#define PRZMG_PROFILE_D2D 0   /* CompressD2D frame: flat sections, raw literals */
+#define PRZMG_PROFILE_ANS 1   /* match + tokenize + ANS frame (Mode 8 + V-ANS)   */
+
+#define PRZMG_NORM_GO 0       /* gpu.NormalizeFreq, container flag 0x01 */
+#define PRZMG_NORM_CPU 1      /* literals.NormalizeFrequencies, flag 0x00 */
+
+typedef struct przmg_ctx przmg_ctx;
+typedef struct przmg_batch przmg_batch;
+
+/* GPUProfile, gpu/types.go:55-71 */
+typedef struct {
+    uint64_t ingress_dma_bytes;
+    double ingress_dma_time_ms;
+    double ingress_dma_bandwidth_gbps;
+    double kernel_time_ms;
+    double internal_vram_bandwidth_gbps;
+    uint64_t egress_dma_bytes;
+    double egress_dma_time_ms;
+    double egress_dma_bandwidth_gbps;
+    double total_round_trip_ms;
+    double end_to_end_bandwidth_gbps;
+    double pcie_overhead_percent;
+    char device_name[128];
+    int32_t sm_count;
+    int32_t pipelined_chunks;
+    uint64_t total_vram_bytes;
+} przmg_profile_t;
+
+/* TokenizerProfile, gpu/types.go:74-85 */
+typedef struct {
+    double kernel_time_ms;
+    double pass1_ms;
+    double pass2_ms;
+    double pass3_ms;
+    double total_round_trip_ms;
+    double throughput_gbps;
+    int64_t cmd_bytes;
+    int64_t offset_bytes;
+    int64_t literal_bytes;
+    int64_t num_chunks;
+} przmg_tokenizer_profile_t;
+
+/* DeviceTokenStreams, gpu/types.go:90-100 (pointers borrowed from the
+ * context; the next call on the context invalidates them, gpu/bridge.go:2122) */
+typedef struct {
+    uint64_t d_final_cmds;
+    uint64_t d_final_offs;
+    uint64_t d_final_lits;
+    uint64_t d_totals;
+    uint32_t cmd_len;
+    uint32_t off_len;
+    uint32_t lit_len;
+    uint32_t num_chunks;
+    uint64_t stream;
+} przmg_device_streams_t;
+
+/* LZ77Match, gpu/types.go:19-24 */
+typedef struct {
+    uint32_t position;
+    uint32_t offset;
+    uint16_t length;
+    uint8_t literal;
+    uint8_t reserved;
+} przmg_match_t;
+
+/* One input of a batch call (host buffers). */
+typedef struct {
+    const uint8_t* src;
+    uint64_t n;
+    uint8_t* dst;
+    uint64_t cap;
+    uint64_t out_len;   /* out: frame size */
+    int32_t status;     /* out */
+    int32_t reserved;
+} przmg_job_t;
+
+/* ---- discovery and lifetime ------------------------------------------- */
+int32_t przmg_is_available(void);                              /* IsAvailable, gpu/bridge.go:61 */
+int32_t przmg_init(int32_t device, przmg_ctx** out);            /* NewGPUCompressor, gpu/bridge.go:291 */
+int32_t przmg_get_global(przmg_ctx** out);                      /* GetGlobalCompressor, gpu/bridge.go:96 */
+void przmg_reset_global_for_test(void);                         /* ResetGlobalCompressorForTest, :117 */
+int32_t przmg_close(przmg_ctx* ctx);                            /* (*GPUCompressor).Close, :513 */
+void przmg_set_mock_unavailable(int32_t unavailable);           /* SetMockUnavailableForTest, :45 */
+void przmg_set_mock_match_error(int32_t code);                  /* SetMockMatchErrorForTest, :50 (0 clears) */
+/* ComputeMajor/ComputeMinor/DeviceName/SMCount/TotalVRAMBytes fields, :283-287 */
+int32_t przmg_device_info(przmg_ctx* ctx, int32_t* major, int32_t* minor, char* name, size_t name_cap,
+                          int32_t* sm_count, uint64_t* total_vram);
+const char* przmg_last_error(void);                             /* message of the calling thread's last error */
+
+/* ---- match finding ------------------------------------------------------ */
+/* MatchLZ77, gpu/bridge.go:1480 (radix strike for every size; > 16 MiB is
+ * streamed in 8 MiB chunks).  out must hold n entries. */
+int32_t przmg_match_lz77(przmg_ctx* ctx, const uint8_t* src, uint64_t n, przmg_match_t* out, uint64_t cap,
+                         uint64_t* n_out, przmg_profile_t* prof);
+/* Per-position match descriptors that Tokenize/CompressD2D consume: the
+ * slot's dMatch after launchMatchSearch, gpu/bridge.go:924-950 (tile finder
+ * for n <= 64 KiB, radix strike above; packing of gpu/types.go:27-33).
+ * desc must hold n entries. */
+int32_t przmg_match_table(przmg_ctx* ctx, const uint8_t* src, uint64_t n, uint32_t* desc);
+/* MatchLZ77Streaming, gpu/bridge.go:1461 (chunk <= 0 picks the default) */
+int32_t przmg_match_lz77_streaming(przmg_ctx* ctx, const uint8_t* src, uint64_t n, int64_t chunk,
+                                   przmg_match_t* out, uint64_t cap, uint64_t* n_out, przmg_profile_t* prof);
+
+/* ---- tokenization ------------------------------------------------------- */
+/* Tokenize, gpu/bridge.go:1895: lens[0..2] = cmd/off/lit bytes written. */
+int32_t przmg_tokenize(przmg_ctx* ctx, const uint8_t* src, uint64_t n, uint8_t* cmd, uint64_t cmd_cap, uint8_t* off,
+                       uint64_t off_cap, uint8_t* lit, uint64_t lit_cap, uint64_t lens[3],
+                       przmg_tokenizer_profile_t* prof);
+/* TokenizeDevice / TokenizeDeviceZeroCopy, gpu/bridge.go:2139, 2247 */
+int32_t przmg_tokenize_device(przmg_ctx* ctx, const uint8_t* src, uint64_t n, przmg_device_streams_t* out,
+                              przmg_tokenizer_profile_t* prof);
+/* DownloadDeviceBytes, gpu/bridge.go:2253 */
+int32_t przmg_download_device_bytes(przmg_ctx* ctx, uint64_t d_ptr, uint64_t size, uint8_t* dst);
+
+/* ---- frames ------------------------------------------------------------- */
+uint64_t przmg_frame_bound(uint64_t n);                         /* capacity a frame of n input bytes needs */
+/* EncodeD2D, gpu/bridge.go:2466 (window_log 0 picks 16/20/23 by size) */
+int32_t przmg_encode_d2d(przmg_ctx* ctx, const przmg_device_streams_t* streams, uint32_t usize, int32_t window_log,
+                         uint8_t* dst, uint64_t cap, uint64_t* out_len, przmg_profile_t* prof);
+/* CompressD2D, gpu/bridge.go:2486 */
+int32_t przmg_compress_d2d(przmg_ctx* ctx, const uint8_t* src, uint64_t n, uint8_t* dst, uint64_t cap,
+                           uint64_t* out_len, przmg_profile_t* prof);
+/* Compress with GPUAcceleration (api.go:15/32 + options.go:85): PRZMG_PROFILE_ANS
+ * is the entropy-coded frame; n must stay below 16 MiB (24-bit uSize). */
+int32_t przmg_compress(przmg_ctx* ctx, const uint8_t* src, uint64_t n, int32_t profile, uint8_t* dst, uint64_t cap,
+                       uint64_t* out_len, przmg_profile_t* prof);
+/* Many inputs in one call (no reference counterpart; the reference compresses
+ * one input per call).  batched = 1: one launch sequence for all inputs;
+ * batched = 0: one launch sequence and one synchronisation per input. */
+int32_t przmg_compress_batch(przmg_ctx* ctx, przmg_job_t* jobs, uint64_t njobs, int32_t profile, int32_t batched,
+                             przmg_profile_t* prof);
+
+/* Device-resident batches (inputs already in HBM; used for throughput runs). */
+int32_t przmg_batch_create(przmg_ctx* ctx, const uint64_t* sizes, uint64_t njobs, int32_t profile,
+                           przmg_batch** out);
+/* device base of the packed inputs and the per-input byte offsets (njobs) */
+int32_t przmg_batch_inputs(przmg_batch* b, uint64_t* d_in, uint64_t* offsets);
+/* device base of the frames and their byte offsets (njobs) */
+int32_t przmg_batch_outputs(przmg_batch* b, uint64_t* d_out, uint64_t* offsets);
+/* enqueue the whole pipeline on `stream` (0: the context stream); use_graph
+ * replays a captured CUDA graph of the same sequence */
+int32_t przmg_batch_enqueue(przmg_batch* b, uint64_t stream, int32_t use_graph);
+/* synchronise and read back frame sizes (njobs) and the kernel error word */
+int32_t przmg_batch_sizes(przmg_batch* b, uint32_t* sizes);
+/* kernels a single enqueue launches (for launch accounting) */
+int32_t przmg_batch_launch_count(przmg_batch* b);
+int32_t przmg_batch_destroy(przmg_batch* b);
+
+/* ---- histogram / flat pack / V-ANS ------------------------------------- */
+/* ComputeHistogramGPU, gpu/bridge.go:2890 */
+int32_t przmg_compute_histogram_gpu(przmg_ctx* ctx, uint64_t d_in, uint64_t n, uint64_t stream, uint32_t counts[256],
+                                    double* ms, double* gbps);
+/* ComputeHistogramHost, gpu/bridge.go:2961 */
+int32_t przmg_compute_histogram_host(przmg_ctx* ctx, const uint8_t* src, uint64_t n, uint32_t counts[256],
+                                     przmg_profile_t* prof);
+/* PackStreamFlatGPU, gpu/bridge.go:3033 (out_len = n + 5) */
+int32_t przmg_pack_stream_flat_gpu(przmg_ctx* ctx, uint64_t d_in, uint64_t d_out, uint64_t n, uint64_t stream,
+                                   uint64_t* out_len, double* ms, double* gbps);
+/* PackStreamFlatHost, gpu/bridge.go:3079 */
+int32_t przmg_pack_stream_flat_host(przmg_ctx* ctx, const uint8_t* src, uint64_t n, uint8_t* dst, uint64_t cap,
+                                    uint64_t* out_len, przmg_profile_t* prof);
+/* VANSEncode4xGPU, gpu/bridge.go:3161 (container flag 0x01) */
+int32_t przmg_vans_encode4x_gpu(przmg_ctx* ctx, uint64_t d_in, uint64_t d_out, uint64_t n, const uint16_t freq[256],
+                                const uint16_t cdf[257], const uint8_t* mat, uint32_t mat_len, uint64_t stream,
+                                uint64_t* out_len, double* ms, double* gbps);
+/* VANSEncode4xHost, gpu/bridge.go:3233 */
+int32_t przmg_vans_encode4x_host(przmg_ctx* ctx, const uint8_t* src, uint64_t n, uint8_t* dst, uint64_t cap,
+                                 uint64_t* out_len, przmg_profile_t* prof);
+/* Histogram + normalise + V-ANS of many device streams in one launch sequence
+ * (no reference counterpart: the reference encodes one stream per call).
+ * norm: PRZMG_NORM_GO (NormalizeFreq, flag 0x01) or PRZMG_NORM_CPU
+ * (NormalizeFrequencies, EncodeAdaptiveVANS4x, flag 0x00).  out_offs[i] must
+ * leave room for 1024 + 2 * lens[i] bytes. */
+int32_t przmg_vans_encode_batch(przmg_ctx* ctx, uint64_t d_in, const uint64_t* in_offs, const uint32_t* lens,
+                                uint64_t count, int32_t norm, uint64_t d_out, const uint64_t* out_offs,
+                                uint32_t* out_lens, uint64_t stream);
+
+/* host helpers */
+void przmg_normalize_freq(const uint32_t counts[256], uint32_t target_m, uint16_t freq[256]); /* NormalizeFreq, :2777 */
+void przmg_normalize_frequencies(const uint32_t counts[256], uint16_t freq[256]); /* literals.NormalizeFrequencies */
+void przmg_build_cdf(const uint16_t freq[256], uint16_t cdf[257]);                 /* BuildCDF, :2832 */
+uint32_t przmg_serialize_matrix(const uint16_t freq[256], uint8_t* out);          /* SerializeMatrix, :2844 (out >= 546) */
+
+/* ---- benchmarks ---------------------------------------------------------- */
+int32_t przmg_benchmark_vram_bandwidth(przmg_ctx* ctx, int32_t size_mb, int32_t iterations, double* gbps); /* :2674 */
+int32_t przmg_benchmark_d2d_entropy(przmg_ctx* ctx, int32_t size_mb, int32_t iterations, double* gbps);     /* :2547 */
+int32_t przmg_benchmark_entropy_vram(przmg_ctx* ctx, int32_t size_mb, int32_t iterations, double* gbps);   /* :3325 */
+
+/* ---- pinned host memory (gpu/memory.go:51-165) --------------------------- */
+int32_t przmg_alloc_pinned_host(uint64_t size, void** out); /* AllocPinnedHost */
+int32_t przmg_free_pinned_host(void* p);                    /* FreePinnedHost */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PRZMGPU_H */

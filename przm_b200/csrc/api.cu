@@ -1,0 +1,1033 @@
+// api.cu -- host side of libprzmgpu.so: contexts, the batch engine and the C
+// ABI declared in include/przmgpu.h.  All kernels are compiled into this one
+// translation unit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/przmgpu.h"
+#include "common.cuh"
+#include "entropy.cu"
+#include "frame.cu"
+#include "match.cu"
+#include "tokenize.cu"
+#include "streams.cu"
+
+using namespace pz;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+static std::atomic<int> g_mock_unavailable{0};
+static std::atomic<int> g_mock_match_err{0};
+
+static int32_t fail(int32_t code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+static int32_t cuda_fail(const char* what, cudaError_t e) {
+    return fail(PRZMG_ERR_CUDA, std::string(what) + " failed with CUDA error " + std::to_string((int)e) + " (" +
+                                    cudaGetErrorString(e) + ")");
+}
+#define CK(call)                                               \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return cuda_fail(#call, e_);    \
+    } while (0)
+
+extern "C" const char* przmg_last_error(void) { return g_err.c_str(); }
+
+// ---------------------------------------------------------------------------
+// grow-only device / pinned buffers
+// ---------------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes + bytes / 8 + 4096;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+struct HostBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap && p) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes + bytes / 8 + 4096;
+        cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+static inline uint64_t align16(uint64_t v) { return (v + 15) & ~15ull; }
+
+extern "C" uint64_t przmg_frame_bound(uint64_t n) { return 2 * n + (n >> 13) + 4096; }
+
+// ---------------------------------------------------------------------------
+// batch engine
+// ---------------------------------------------------------------------------
+struct Ctx;
+
+struct przmg_batch {
+    Ctx* ctx = nullptr;
+    int profile = 1;
+    bool force_radix = false;
+    bool owned = false;  // created through przmg_batch_create
+    uint32_t njobs = 0, ntiles = 0, nsmall = 0, nbig = 0;
+    std::vector<Job> jobs;
+    std::vector<TileRef> small;
+    std::vector<uint32_t> big;
+    std::vector<TokTile> tiles;
+    std::vector<uint64_t> in_offs, out_offs;
+    uint64_t in_bytes = 0, desc_words = 0, stream_bytes = 0, ans_bytes = 0, out_bytes = 0;
+    DevBuf d_in, d_jobs, d_small, d_big, d_tiles, d_desc, d_slots, d_tile_lens, d_streams, d_job_lens, d_hist, d_tabs,
+        d_infos, d_ans, d_outs, d_plans, d_sizes, d_out, d_misc;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int launches = 0;
+    ~przmg_batch() { drop_graph(); release(); }
+    void drop_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+    void release() {
+        DevBuf* all[] = {&d_in, &d_jobs, &d_small, &d_big, &d_tiles, &d_desc, &d_slots, &d_tile_lens, &d_streams,
+                         &d_job_lens, &d_hist, &d_tabs, &d_infos, &d_ans, &d_outs, &d_plans, &d_sizes, &d_out, &d_misc};
+        for (DevBuf* b : all) b->release();
+    }
+    uint32_t* err_word() const { return d_misc.as<uint32_t>(); }
+    uint32_t* work_word() const { return d_misc.as<uint32_t>() + 1; }
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    cudaDeviceProp prop{};
+    int sms = 148;
+    DevBuf d_meta8, d_ctxlut, d_radix, d_tags;
+    uint32_t radix_ctas = 0;
+    przmg_batch single;  // reused by the one-input calls
+    HostBuf h_in, h_out, h_aux;
+    DevBuf d_scr_in, d_scr_out, d_scr_aux, d_scr_tab;
+    cudaEvent_t ev[8] = {};
+};
+
+static int32_t ensure_radix(Ctx* c) {
+    const uint32_t want = 2 * (uint32_t)c->sms;
+    if (c->radix_ctas >= want) return PRZMG_OK;
+    CK(c->d_radix.ensure((size_t)want * kRadixBuckets * sizeof(uint64_t)));
+    CK(c->d_tags.ensure((size_t)want * sizeof(uint64_t)));
+    CK(cudaMemsetAsync(c->d_radix.p, 0, c->d_radix.cap, c->stream));
+    CK(cudaMemsetAsync(c->d_tags.p, 0, c->d_tags.cap, c->stream));
+    c->radix_ctas = want;
+    return PRZMG_OK;
+}
+
+// Lay out a batch for the given input sizes; (re)allocates only when a
+// buffer is too small, so repeated calls of similar size reuse memory.
+static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njobs, int profile, bool force_radix) {
+    b->drop_graph();
+    b->profile = profile;
+    b->force_radix = force_radix;
+    b->njobs = njobs;
+    b->jobs.assign(njobs, Job{});
+    b->small.clear();
+    b->big.clear();
+    b->tiles.clear();
+    b->in_offs.assign(njobs, 0);
+    b->out_offs.assign(njobs, 0);
+    uint64_t in = 0, desc = 0, str = 0, ans = 0, out = 0;
+    uint32_t tile0 = 0;
+    for (uint32_t i = 0; i < njobs; i++) {
+        Job& j = b->jobs[i];
+        const uint64_t n = sizes[i];
+        if (n >= (1ull << 32) - 4096) return fail(PRZMG_ERR_EXCEEDS_MAX_BLOCK, "input too large for one frame");
+        j.n = (uint32_t)n;
+        j.kind = (force_radix || n > kSmallMax) ? 1 : 0;
+        j.ntiles = (uint32_t)std::max<uint64_t>(1, (n + kTile - 1) / kTile);
+        j.tile0 = tile0;
+        j.profile = (uint32_t)profile;
+        j.in_off = in;
+        b->in_offs[i] = in;
+        in = align16(in + n + 64);
+        j.desc_off = desc;
+        const uint64_t ncand = n >= 8 ? (n - 8) / 8 + 1 : 0;
+        desc += j.kind == 0 ? align16(n + 1) : align16(ncand + 1);
+        j.cmd_cap = j.ntiles * kSlotCmd;
+        j.off_cap = j.ntiles * kSlotOff;
+        j.lit_cap = j.ntiles * kSlotLit;
+        j.str_off = str;
+        str += align16(stream_region_bytes(j));
+        j.ans_off = ans;
+        if (profile == 1) ans += align16(ans_region_bytes(j));
+        j.out_cap = (uint32_t)std::min<uint64_t>(przmg_frame_bound(n), 0xFFFFFFF0u);
+        j.out_off = out;
+        b->out_offs[i] = out;
+        out = align16(out + j.out_cap);
+        if (n > 0) {
+            if (j.kind == 0) for (uint32_t t = 0; t < j.ntiles; t++) b->small.push_back({i, t});
+            else b->big.push_back(i);
+            for (uint32_t t = 0; t < j.ntiles; t++) b->tiles.push_back({i, t});
+        }
+        tile0 += j.ntiles;
+    }
+    b->ntiles = tile0;
+    b->nsmall = (uint32_t)b->small.size();
+    b->nbig = (uint32_t)b->big.size();
+    b->in_bytes = in + 64;
+    b->desc_words = desc + 16;
+    b->stream_bytes = str + 64;
+    b->ans_bytes = ans + 64;
+    b->out_bytes = out + 64;
+    CK(b->d_in.ensure(b->in_bytes));
+    CK(b->d_jobs.ensure(sizeof(Job) * std::max<uint32_t>(njobs, 1)));
+    CK(b->d_small.ensure(sizeof(TileRef) * std::max<uint32_t>(b->nsmall, 1)));
+    CK(b->d_big.ensure(sizeof(uint32_t) * std::max<uint32_t>(b->nbig, 1)));
+    CK(b->d_tiles.ensure(sizeof(TokTile) * std::max<size_t>(b->tiles.size(), 1)));
+    CK(b->d_desc.ensure(b->desc_words * 4));
+    CK(b->d_slots.ensure((size_t)b->ntiles * kSlotStride));
+    CK(b->d_tile_lens.ensure((size_t)b->ntiles * S_COUNT * 4));
+    CK(b->d_streams.ensure(b->stream_bytes));
+    CK(b->d_job_lens.ensure((size_t)njobs * S_COUNT * 4 + 16));
+    CK(b->d_hist.ensure((size_t)njobs * 1024 * 4 + 16));
+    CK(b->d_tabs.ensure((size_t)njobs * 4 * 256 * sizeof(EncSym) + 16));
+    CK(b->d_infos.ensure((size_t)njobs * 4 * sizeof(TableInfo) + 16));
+    CK(b->d_ans.ensure(b->ans_bytes));
+    CK(b->d_outs.ensure((size_t)njobs * T_COUNT * sizeof(TaskOut) + 16));
+    CK(b->d_plans.ensure((size_t)njobs * sizeof(Plan) + 16));
+    CK(b->d_sizes.ensure((size_t)njobs * 4 + 16));
+    CK(b->d_out.ensure(b->out_bytes));
+    CK(b->d_misc.ensure(64));
+    cudaStream_t s = b->ctx->stream;
+    CK(cudaMemcpyAsync(b->d_jobs.p, b->jobs.data(), sizeof(Job) * njobs, cudaMemcpyHostToDevice, s));
+    if (b->nsmall) CK(cudaMemcpyAsync(b->d_small.p, b->small.data(), sizeof(TileRef) * b->nsmall, cudaMemcpyHostToDevice, s));
+    if (b->nbig) CK(cudaMemcpyAsync(b->d_big.p, b->big.data(), sizeof(uint32_t) * b->nbig, cudaMemcpyHostToDevice, s));
+    if (!b->tiles.empty())
+        CK(cudaMemcpyAsync(b->d_tiles.p, b->tiles.data(), sizeof(TokTile) * b->tiles.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(b->d_sizes.p, 0, (size_t)njobs * 4 + 16, s));
+    CK(cudaMemsetAsync(b->d_job_lens.p, 0, (size_t)njobs * S_COUNT * 4 + 16, s));
+    if (b->nbig) {
+        int32_t r = ensure_radix(b->ctx);
+        if (r) return r;
+    }
+    // the host-side vectors above must stay alive until the copies ran
+    CK(cudaStreamSynchronize(s));
+    return PRZMG_OK;
+}
+
+// Stages of one enqueue.  stop_after: 0 match only, 1 through tokenize +
+// gather, 2 the full frame pipeline.
+static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after) {
+    Ctx* c = b->ctx;
+    int launches = 0;
+    CK(cudaMemsetAsync(b->d_misc.p, 0, 16, s));
+    if (b->nsmall) {
+        const uint32_t grid = std::min<uint32_t>(b->nsmall, 8u * c->sms);
+        k_tile_find<<<grid, 256, kTileFindSmem, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_small.as<TileRef>(),
+                                                     b->nsmall, b->d_desc.as<uint32_t>());
+        CK(cudaGetLastError());
+        launches++;
+    }
+    if (b->nbig) {
+        const uint32_t grid = std::min<uint32_t>(b->nbig, c->radix_ctas);
+        k_radix_find<<<grid, kRadixThreads, kRadixSmem, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(),
+                                                              b->d_big.as<uint32_t>(), b->nbig, b->work_word(),
+                                                              c->d_radix.as<uint64_t>(), c->d_tags.as<uint64_t>(),
+                                                              b->d_desc.as<uint32_t>());
+        CK(cudaGetLastError());
+        launches++;
+    }
+    if (stop_after >= 1 && !b->tiles.empty()) {
+        const uint32_t nt = (uint32_t)b->tiles.size();
+        k_tokenize<<<(nt + 7) / 8, 256, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_tiles.as<TokTile>(), nt,
+                                               b->d_desc.as<uint32_t>(), b->d_slots.as<uint8_t>(),
+                                               b->d_tile_lens.as<uint32_t>(), b->err_word());
+        CK(cudaGetLastError());
+        uint32_t maxtiles = 1;
+        for (const Job& j : b->jobs) maxtiles = std::max(maxtiles, j.ntiles);
+        k_gather<<<std::min<uint32_t>(b->njobs, 16u * c->sms), kGatherThreads, (maxtiles + 1) * 4, s>>>(
+            b->d_jobs.as<Job>(), b->njobs, b->d_slots.as<uint8_t>(), b->d_tile_lens.as<uint32_t>(),
+            b->d_streams.as<uint8_t>(), b->d_job_lens.as<uint32_t>(), b->d_hist.as<uint32_t>(), b->err_word());
+        CK(cudaGetLastError());
+        launches += 2;
+    }
+    if (stop_after >= 2) {
+        if (b->profile == 1) {
+            k_normalize<<<b->njobs, 128, 0, s>>>(b->d_jobs.as<Job>(), b->njobs, b->d_job_lens.as<uint32_t>(),
+                                                 b->d_hist.as<uint32_t>(), b->d_tabs.as<EncSym>(), b->d_infos.as<TableInfo>());
+            CK(cudaGetLastError());
+            const uint32_t threads = b->njobs * T_COUNT * 4;
+            k_rans<<<(threads + 127) / 128, 128, 0, s>>>(b->d_jobs.as<Job>(), b->njobs, b->d_job_lens.as<uint32_t>(),
+                                                        b->d_streams.as<uint8_t>(), b->d_ans.as<uint8_t>(),
+                                                        b->d_tabs.as<EncSym>(), c->d_meta8.as<EncSym>(),
+                                                        c->d_ctxlut.as<uint8_t>(), b->d_outs.as<TaskOut>());
+            CK(cudaGetLastError());
+            launches += 2;
+        }
+        k_plan<<<(b->njobs + 127) / 128, 128, 0, s>>>(b->d_jobs.as<Job>(), b->njobs, b->d_job_lens.as<uint32_t>(),
+                                                      b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(),
+                                                      b->d_streams.as<uint8_t>(), b->d_plans.as<Plan>(),
+                                                      b->d_sizes.as<uint32_t>());
+        CK(cudaGetLastError());
+        k_assemble<<<std::min<uint32_t>(b->njobs, 16u * c->sms), kAsmThreads, 0, s>>>(
+            b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->njobs, b->d_job_lens.as<uint32_t>(), b->d_plans.as<Plan>(),
+            b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(), b->d_streams.as<uint8_t>(), b->d_ans.as<uint8_t>(),
+            b->d_out.as<uint8_t>());
+        CK(cudaGetLastError());
+        launches += 2;
+    }
+    b->launches = launches;
+    return PRZMG_OK;
+}
+
+static int32_t batch_check(przmg_batch* b) {
+    uint32_t err = 0;
+    CK(cudaMemcpyAsync(&err, b->err_word(), 4, cudaMemcpyDeviceToHost, b->ctx->stream));
+    CK(cudaStreamSynchronize(b->ctx->stream));
+    if (err) return fail(PRZMG_ERR_DEVICE, "device bound violation, error bits " + std::to_string(err));
+    return PRZMG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// context lifetime
+// ---------------------------------------------------------------------------
+static std::mutex g_global_mu;
+static Ctx* g_global = nullptr;
+
+extern "C" int32_t przmg_is_available(void) {
+    if (g_mock_unavailable.load()) return 0;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return 0;
+    for (int i = 0; i < n; i++) {
+        int major = 0;
+        if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, i) == cudaSuccess && major >= 10) return 1;
+    }
+    return 0;
+}
+
+static int32_t ctx_setup(Ctx* c) {
+    CK(cudaSetDevice(c->device));
+    CK(cudaGetDeviceProperties(&c->prop, c->device));
+    if (c->prop.major < 10) return fail(PRZMG_ERR_UNAVAILABLE, "compute capability 10.x (B200, sm_100a) required");
+    c->sms = c->prop.multiProcessorCount;
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (auto& e : c->ev) CK(cudaEventCreate(&e));
+    CK(cudaFuncSetAttribute(k_tile_find, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileFindSmem));
+    CK(cudaFuncSetAttribute(k_radix_find, cudaFuncAttributeMaxDynamicSharedMemorySize, kRadixSmem));
+    CK(c->d_meta8.ensure(8 * 256 * sizeof(EncSym)));
+    CK(c->d_ctxlut.ensure(256));
+    {
+        std::vector<EncSym> tab(8 * 256);
+        std::vector<uint8_t> lut(256);
+        build_meta8_tables(tab.data(), lut.data());
+        CK(cudaMemcpy(c->d_meta8.p, tab.data(), tab.size() * sizeof(EncSym), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(c->d_ctxlut.p, lut.data(), 256, cudaMemcpyHostToDevice));
+    }
+    c->single.ctx = c;
+    CK(cudaStreamSynchronize(c->stream));
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_init(int32_t device, przmg_ctx** out) {
+    if (!out) return fail(PRZMG_ERR_INVALID_ARG, "null output pointer");
+    *out = nullptr;
+    if (!przmg_is_available()) return fail(PRZMG_ERR_UNAVAILABLE, "cuda gpu acceleration not available");
+    Ctx* c = new Ctx();
+    c->device = device;
+    int32_t r = ctx_setup(c);
+    if (r) {
+        delete c;
+        return r;
+    }
+    *out = reinterpret_cast<przmg_ctx*>(c);
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_close(przmg_ctx* h) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c) return PRZMG_OK;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        cudaSetDevice(c->device);
+        cudaStreamSynchronize(c->stream);
+        c->single.drop_graph();
+        c->single.release();
+        DevBuf* bufs[] = {&c->d_meta8, &c->d_ctxlut, &c->d_radix, &c->d_tags, &c->d_scr_in, &c->d_scr_out, &c->d_scr_aux,
+                          &c->d_scr_tab};
+        for (DevBuf* b : bufs) b->release();
+        c->h_in.release();
+        c->h_out.release();
+        c->h_aux.release();
+        for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+        cudaStreamDestroy(c->stream);
+    }
+    {
+        std::lock_guard<std::mutex> g(g_global_mu);
+        if (g_global == c) g_global = nullptr;
+    }
+    delete c;
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_get_global(przmg_ctx** out) {
+    if (!out) return fail(PRZMG_ERR_INVALID_ARG, "null output pointer");
+    std::lock_guard<std::mutex> g(g_global_mu);
+    if (g_global) { *out = reinterpret_cast<przmg_ctx*>(g_global); return PRZMG_OK; }
+    if (!przmg_is_available()) return fail(PRZMG_ERR_UNAVAILABLE, "cuda gpu acceleration not available or compute capability < 10.0");
+    przmg_ctx* c = nullptr;
+    g_global_mu.unlock();
+    int32_t r = przmg_init(0, &c);
+    g_global_mu.lock();
+    if (r) return r;
+    if (g_global) {  // another thread won the race
+        g_global_mu.unlock();
+        przmg_close(c);
+        g_global_mu.lock();
+    } else {
+        g_global = reinterpret_cast<Ctx*>(c);
+    }
+    *out = reinterpret_cast<przmg_ctx*>(g_global);
+    return PRZMG_OK;
+}
+
+extern "C" void przmg_reset_global_for_test(void) {
+    Ctx* c;
+    {
+        std::lock_guard<std::mutex> g(g_global_mu);
+        c = g_global;
+        g_global = nullptr;
+    }
+    if (c) przmg_close(reinterpret_cast<przmg_ctx*>(c));
+}
+
+extern "C" void przmg_set_mock_unavailable(int32_t v) { g_mock_unavailable.store(v ? 1 : 0); }
+extern "C" void przmg_set_mock_match_error(int32_t code) { g_mock_match_err.store(code); }
+
+static int32_t mock_check() {
+    int m = g_mock_match_err.load();
+    if (m) return fail(PRZMG_ERR_MOCK, "mock match error " + std::to_string(m));
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_device_info(przmg_ctx* h, int32_t* major, int32_t* minor, char* name, size_t name_cap,
+                                     int32_t* sm_count, uint64_t* total_vram) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c) return fail(PRZMG_ERR_INVALID_ARG, "null context");
+    if (major) *major = c->prop.major;
+    if (minor) *minor = c->prop.minor;
+    if (name && name_cap) { std::snprintf(name, name_cap, "%s", c->prop.name); }
+    if (sm_count) *sm_count = c->sms;
+    if (total_vram) *total_vram = c->prop.totalGlobalMem;
+    return PRZMG_OK;
+}
+
+static void fill_profile(Ctx* c, przmg_profile_t* p) {
+    if (!p) return;
+    std::snprintf(p->device_name, sizeof p->device_name, "%.127s", c->prop.name);
+    p->sm_count = c->sms;
+    p->total_vram_bytes = c->prop.totalGlobalMem;
+    if (p->pipelined_chunks == 0) p->pipelined_chunks = 1;
+}
+
+static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+static double gbps(double bytes, double ms) { return ms > 0 ? bytes / (ms / 1000.0) / 1e9 : 0; }
+
+#define LOCKED(c)                                  \
+    std::lock_guard<std::mutex> lk_((c)->mu);      \
+    CK(cudaSetDevice((c)->device))
+
+// ---------------------------------------------------------------------------
+// one-input compress / tokenize
+// ---------------------------------------------------------------------------
+static int32_t single_run(Ctx* c, const uint8_t* src, uint64_t n, int profile, int stop_after, bool force_radix,
+                          przmg_profile_t* prof) {
+    przmg_batch* b = &c->single;
+    int32_t r = batch_prepare(b, &n, 1, profile, force_radix);
+    if (r) return r;
+    CK(c->h_in.ensure(n + 64));
+    std::memcpy(c->h_in.p, src, n);
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    CK(cudaMemcpyAsync(b->d_in.p, c->h_in.p, n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    r = batch_launch(b, c->stream, stop_after);
+    if (r) return r;
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    r = batch_check(b);
+    if (r) return r;
+    if (prof) {
+        *prof = przmg_profile_t{};
+        prof->ingress_dma_bytes = n;
+        prof->ingress_dma_time_ms = ev_ms(c->ev[0], c->ev[1]);
+        prof->ingress_dma_bandwidth_gbps = gbps((double)n, prof->ingress_dma_time_ms);
+        prof->kernel_time_ms = ev_ms(c->ev[1], c->ev[2]);
+        prof->internal_vram_bandwidth_gbps = gbps((double)n, prof->kernel_time_ms);
+    }
+    return PRZMG_OK;
+}
+
+static int32_t compress_one(Ctx* c, const uint8_t* src, uint64_t n, int profile, uint8_t* dst, uint64_t cap,
+                            uint64_t* out_len, przmg_profile_t* prof) {
+    if (out_len) *out_len = 0;
+    if (n == 0) { if (prof) { *prof = przmg_profile_t{}; fill_profile(c, prof); } return PRZMG_OK; }
+    if (!src || !dst || !out_len) return fail(PRZMG_ERR_INVALID_ARG, "null buffer");
+    if (profile == PRZMG_PROFILE_ANS && n >= (1u << 24))
+        return fail(PRZMG_ERR_EXCEEDS_MAX_BLOCK, "the frame header holds 24-bit sizes: input must be < 16 MiB");
+    int32_t r = single_run(c, src, n, profile, 2, false, prof);
+    if (r) return r;
+    przmg_batch* b = &c->single;
+    uint32_t size = 0;
+    CK(cudaMemcpyAsync(&size, b->d_sizes.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (size > cap) return fail(PRZMG_ERR_BUFFER_TOO_SMALL, "destination too small for the frame");
+    CK(c->h_out.ensure(size + 16));
+    CK(cudaEventRecord(c->ev[3], c->stream));
+    CK(cudaMemcpyAsync(c->h_out.p, b->d_out.p, size, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaEventRecord(c->ev[4], c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::memcpy(dst, c->h_out.p, size);
+    *out_len = size;
+    if (prof) {
+        prof->egress_dma_bytes = size;
+        prof->egress_dma_time_ms = ev_ms(c->ev[3], c->ev[4]);
+        prof->egress_dma_bandwidth_gbps = gbps((double)size, prof->egress_dma_time_ms);
+        prof->total_round_trip_ms = ev_ms(c->ev[0], c->ev[4]);
+        prof->end_to_end_bandwidth_gbps = gbps((double)n, prof->total_round_trip_ms);
+        if (prof->total_round_trip_ms > 0)
+            prof->pcie_overhead_percent = 100.0 * (prof->ingress_dma_time_ms + prof->egress_dma_time_ms) / prof->total_round_trip_ms;
+        fill_profile(c, prof);
+    }
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_compress_d2d(przmg_ctx* h, const uint8_t* src, uint64_t n, uint8_t* dst, uint64_t cap,
+                                      uint64_t* out_len, przmg_profile_t* prof) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c) return fail(PRZMG_ERR_INVALID_ARG, "null context");
+    if (int32_t m = mock_check()) return m;
+    LOCKED(c);
+    return compress_one(c, src, n, PRZMG_PROFILE_D2D, dst, cap, out_len, prof);
+}
+
+extern "C" int32_t przmg_compress(przmg_ctx* h, const uint8_t* src, uint64_t n, int32_t profile, uint8_t* dst,
+                                  uint64_t cap, uint64_t* out_len, przmg_profile_t* prof) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c) return fail(PRZMG_ERR_INVALID_ARG, "null context");
+    if (profile != PRZMG_PROFILE_D2D && profile != PRZMG_PROFILE_ANS) return fail(PRZMG_ERR_INVALID_ARG, "unknown profile");
+    if (int32_t m = mock_check()) return m;
+    LOCKED(c);
+    return compress_one(c, src, n, profile, dst, cap, out_len, prof);
+}
+
+static int32_t tokenize_common(Ctx* c, const uint8_t* src, uint64_t n, przmg_tokenizer_profile_t* prof, uint32_t lens6[6]) {
+    int32_t r = single_run(c, src, n, PRZMG_PROFILE_D2D, 1, false, nullptr);
+    if (r) return r;
+    przmg_batch* b = &c->single;
+    CK(cudaMemcpyAsync(lens6, b->d_job_lens.p, 24, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (prof) {
+        *prof = przmg_tokenizer_profile_t{};
+        prof->kernel_time_ms = ev_ms(c->ev[1], c->ev[2]);
+        prof->pass1_ms = prof->kernel_time_ms;
+        prof->total_round_trip_ms = ev_ms(c->ev[0], c->ev[2]);
+        prof->throughput_gbps = gbps((double)n, prof->kernel_time_ms);
+        prof->cmd_bytes = lens6[S_CMD];
+        prof->offset_bytes = lens6[S_OFF];
+        prof->literal_bytes = lens6[S_LIT];
+        prof->num_chunks = (n + kTile - 1) / kTile;
+    }
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_tokenize(przmg_ctx* h, const uint8_t* src, uint64_t n, uint8_t* cmd, uint64_t cmd_cap,
+                                  uint8_t* off, uint64_t off_cap, uint8_t* lit, uint64_t lit_cap, uint64_t lens[3],
+                                  przmg_tokenizer_profile_t* prof) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c || !lens) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    if (int32_t m = mock_check()) return m;
+    lens[0] = lens[1] = lens[2] = 0;
+    if (prof) *prof = przmg_tokenizer_profile_t{};
+    if (n == 0) return PRZMG_OK;
+    if (!src) return fail(PRZMG_ERR_INVALID_ARG, "null source");
+    LOCKED(c);
+    uint32_t l6[6];
+    int32_t r = tokenize_common(c, src, n, prof, l6);
+    if (r) return r;
+    if (l6[S_CMD] > cmd_cap || l6[S_OFF] > off_cap || l6[S_LIT] > lit_cap)
+        return fail(PRZMG_ERR_BUFFER_TOO_SMALL, "stream buffers too small");
+    przmg_batch* b = &c->single;
+    const Job& j = b->jobs[0];
+    const uint8_t* base = b->d_streams.as<uint8_t>() + j.str_off;
+    if (l6[S_CMD]) CK(cudaMemcpyAsync(cmd, base + stream_base(j, S_CMD), l6[S_CMD], cudaMemcpyDeviceToHost, c->stream));
+    if (l6[S_OFF]) CK(cudaMemcpyAsync(off, base + stream_base(j, S_OFF), l6[S_OFF], cudaMemcpyDeviceToHost, c->stream));
+    if (l6[S_LIT]) CK(cudaMemcpyAsync(lit, base + stream_base(j, S_LIT), l6[S_LIT], cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    lens[0] = l6[S_CMD];
+    lens[1] = l6[S_OFF];
+    lens[2] = l6[S_LIT];
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_tokenize_device(przmg_ctx* h, const uint8_t* src, uint64_t n, przmg_device_streams_t* out,
+                                         przmg_tokenizer_profile_t* prof) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c || !out) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    if (int32_t m = mock_check()) return m;
+    *out = przmg_device_streams_t{};
+    if (prof) *prof = przmg_tokenizer_profile_t{};
+    if (n == 0) return PRZMG_OK;
+    if (!src) return fail(PRZMG_ERR_INVALID_ARG, "null source");
+    LOCKED(c);
+    uint32_t l6[6];
+    int32_t r = tokenize_common(c, src, n, prof, l6);
+    if (r) return r;
+    przmg_batch* b = &c->single;
+    const Job& j = b->jobs[0];
+    uint8_t* base = b->d_streams.as<uint8_t>() + j.str_off;
+    // {cmd, off, lit} totals, as dTotals (przm_tokenizer.cuh:512-514)
+    uint32_t tot[3] = {l6[S_CMD], l6[S_OFF], l6[S_LIT]};
+    uint32_t* d_tot = b->d_misc.as<uint32_t>() + 4;
+    CK(cudaMemcpyAsync(d_tot, tot, 12, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out->d_final_cmds = (uint64_t)(uintptr_t)(base + stream_base(j, S_CMD));
+    out->d_final_offs = (uint64_t)(uintptr_t)(base + stream_base(j, S_OFF));
+    out->d_final_lits = (uint64_t)(uintptr_t)(base + stream_base(j, S_LIT));
+    out->d_totals = (uint64_t)(uintptr_t)d_tot;
+    out->cmd_len = l6[S_CMD];
+    out->off_len = l6[S_OFF];
+    out->lit_len = l6[S_LIT];
+    out->num_chunks = j.ntiles;
+    out->stream = (uint64_t)(uintptr_t)c->stream;
+    return PRZMG_OK;
+}
+
+// Per-position match table of Tokenize/CompressD2D (the slot's dMatch after
+// launchMatchSearch, gpu/bridge.go:924-950): tile finder for n <= 64 KiB,
+// radix strike otherwise (non-8-aligned positions are 0).
+extern "C" int32_t przmg_match_table(przmg_ctx* h, const uint8_t* src, uint64_t n, uint32_t* desc) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c) return fail(PRZMG_ERR_INVALID_ARG, "null context");
+    if (int32_t m = mock_check()) return m;
+    if (n == 0) return PRZMG_OK;
+    if (!src || !desc) return fail(PRZMG_ERR_INVALID_ARG, "null buffer");
+    LOCKED(c);
+    int32_t r = single_run(c, src, n, PRZMG_PROFILE_D2D, 0, false, nullptr);
+    if (r) return r;
+    przmg_batch* b = &c->single;
+    const Job& j = b->jobs[0];
+    const uint32_t* d = b->d_desc.as<uint32_t>() + j.desc_off;
+    if (j.kind == 0) {
+        CK(cudaMemcpyAsync(desc, d, 4 * n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return PRZMG_OK;
+    }
+    const uint64_t nd = n >= 8 ? (n - 8) / 8 + 1 : 0;
+    CK(c->h_out.ensure(4 * nd + 16));
+    if (nd) CK(cudaMemcpyAsync(c->h_out.p, d, 4 * nd, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::memset(desc, 0, 4 * n);
+    for (uint64_t k = 0; k < nd; k++) desc[8 * k] = c->h_out.as<uint32_t>()[k];
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_download_device_bytes(przmg_ctx* h, uint64_t d_ptr, uint64_t size, uint8_t* dst) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c) return fail(PRZMG_ERR_INVALID_ARG, "null context");
+    if (size == 0) return PRZMG_OK;
+    if (!d_ptr || !dst) return fail(PRZMG_ERR_INVALID_ARG, "null pointer");
+    LOCKED(c);
+    CK(cudaMemcpyAsync(dst, (const void*)(uintptr_t)d_ptr, size, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return PRZMG_OK;
+}
+
+// EncodeD2D: flat sections and header from device-resident streams
+// (encodeD2DLocked, gpu/bridge.go:2287-2458).
+extern "C" int32_t przmg_encode_d2d(przmg_ctx* h, const przmg_device_streams_t* st, uint32_t usize, int32_t window_log,
+                                    uint8_t* dst, uint64_t cap, uint64_t* out_len, przmg_profile_t* prof) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c || !st || !out_len) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    *out_len = 0;
+    if (usize == 0) return PRZMG_OK;
+    LOCKED(c);
+    const uint32_t l2 = st->cmd_len + 5, l3 = st->off_len + 5;
+    uint32_t wl = (uint32_t)window_log;
+    if (wl == 0) wl = d2d_wlog(usize);
+    const bool ext = usize > 65535 || l2 > 65535 || l3 > 65535 || wl > 16;
+    const uint32_t hdr = 8 + (ext ? 6 : 4) + 8;
+    const uint64_t total = (uint64_t)hdr + l2 + l3 + st->lit_len;
+    if (total > cap) return fail(PRZMG_ERR_BUFFER_TOO_SMALL, "destination too small for the frame");
+    CK(c->d_scr_out.ensure(total + 64));
+    CK(c->h_out.ensure(total + 64));
+    uint8_t* hb = c->h_out.as<uint8_t>();
+    uint8_t head[40];
+    uint32_t w = 0;
+    head[w++] = 'P'; head[w++] = 'R'; head[w++] = 'Z'; head[w++] = 'M';
+    head[w++] = ext ? 0x08 : 0;
+    head[w++] = (uint8_t)usize; head[w++] = (uint8_t)(usize >> 8); head[w++] = (uint8_t)(usize >> 16);
+    if (!ext) {
+        head[w++] = (uint8_t)l2; head[w++] = (uint8_t)(l2 >> 8); head[w++] = (uint8_t)l3; head[w++] = (uint8_t)(l3 >> 8);
+    } else {
+        head[w++] = (uint8_t)l2; head[w++] = (uint8_t)(l2 >> 8); head[w++] = (uint8_t)(l2 >> 16);
+        head[w++] = (uint8_t)l3; head[w++] = (uint8_t)(l3 >> 8); head[w++] = (uint8_t)(l3 >> 16);
+    }
+    for (int k = 0; k < 8; k++) head[w++] = 0;
+    head[hdr - 7] = (uint8_t)wl;
+    head[w++] = 0;
+    for (int k = 0; k < 4; k++) head[w++] = (uint8_t)(st->cmd_len >> (8 * k));
+    std::memcpy(hb, head, w);
+    uint8_t* d = c->d_scr_out.as<uint8_t>();
+    cudaStream_t s = c->stream;
+    CK(cudaEventRecord(c->ev[0], s));
+    CK(cudaMemcpyAsync(d, hb, w, cudaMemcpyHostToDevice, s));
+    if (st->cmd_len) CK(cudaMemcpyAsync(d + hdr + 5, (const void*)(uintptr_t)st->d_final_cmds, st->cmd_len, cudaMemcpyDeviceToDevice, s));
+    uint8_t h3[5] = {0, (uint8_t)st->off_len, (uint8_t)(st->off_len >> 8), (uint8_t)(st->off_len >> 16), (uint8_t)(st->off_len >> 24)};
+    std::memcpy(hb + 64, h3, 5);
+    CK(cudaMemcpyAsync(d + hdr + l2, hb + 64, 5, cudaMemcpyHostToDevice, s));
+    if (st->off_len) CK(cudaMemcpyAsync(d + hdr + l2 + 5, (const void*)(uintptr_t)st->d_final_offs, st->off_len, cudaMemcpyDeviceToDevice, s));
+    if (st->lit_len) CK(cudaMemcpyAsync(d + hdr + l2 + l3, (const void*)(uintptr_t)st->d_final_lits, st->lit_len, cudaMemcpyDeviceToDevice, s));
+    CK(cudaEventRecord(c->ev[1], s));
+    CK(cudaStreamSynchronize(s));
+    CK(cudaMemcpyAsync(hb, d, total, cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(c->ev[2], s));
+    CK(cudaStreamSynchronize(s));
+    std::memcpy(dst, hb, total);
+    *out_len = total;
+    if (prof) {
+        *prof = przmg_profile_t{};
+        prof->kernel_time_ms = ev_ms(c->ev[0], c->ev[1]);
+        prof->internal_vram_bandwidth_gbps = gbps((double)usize, prof->kernel_time_ms);
+        prof->egress_dma_bytes = total;
+        prof->total_round_trip_ms = ev_ms(c->ev[0], c->ev[2]);
+        fill_profile(c, prof);
+    }
+    return PRZMG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// many inputs per call
+// ---------------------------------------------------------------------------
+extern "C" int32_t przmg_compress_batch(przmg_ctx* h, przmg_job_t* jobs, uint64_t njobs, int32_t profile,
+                                        int32_t batched, przmg_profile_t* prof) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c || (!jobs && njobs)) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    if (profile != PRZMG_PROFILE_D2D && profile != PRZMG_PROFILE_ANS) return fail(PRZMG_ERR_INVALID_ARG, "unknown profile");
+    if (int32_t m = mock_check()) return m;
+    LOCKED(c);
+    for (uint64_t i = 0; i < njobs; i++) {
+        jobs[i].out_len = 0;
+        jobs[i].status = PRZMG_OK;
+        if (profile == PRZMG_PROFILE_ANS && jobs[i].n >= (1u << 24)) jobs[i].status = PRZMG_ERR_EXCEEDS_MAX_BLOCK;
+    }
+    if (!batched) {
+        for (uint64_t i = 0; i < njobs; i++) {
+            if (jobs[i].status || jobs[i].n == 0) continue;
+            uint64_t len = 0;
+            int32_t r = compress_one(c, jobs[i].src, jobs[i].n, profile, jobs[i].dst, jobs[i].cap, &len, nullptr);
+            jobs[i].status = r;
+            jobs[i].out_len = len;
+        }
+        if (prof) { *prof = przmg_profile_t{}; prof->pipelined_chunks = (int32_t)njobs; fill_profile(c, prof); }
+        return PRZMG_OK;
+    }
+    std::vector<uint64_t> sizes(njobs);
+    uint64_t total = 0;
+    for (uint64_t i = 0; i < njobs; i++) { sizes[i] = jobs[i].status ? 0 : jobs[i].n; total += sizes[i]; }
+    przmg_batch* b = &c->single;
+    int32_t r = batch_prepare(b, sizes.data(), (uint32_t)njobs, profile, false);
+    if (r) return r;
+    CK(c->h_in.ensure(b->in_bytes));
+    for (uint64_t i = 0; i < njobs; i++)
+        if (sizes[i]) std::memcpy(c->h_in.as<uint8_t>() + b->in_offs[i], jobs[i].src, sizes[i]);
+    cudaStream_t s = c->stream;
+    CK(cudaEventRecord(c->ev[0], s));
+    CK(cudaMemcpyAsync(b->d_in.p, c->h_in.p, b->in_bytes - 64, cudaMemcpyHostToDevice, s));
+    CK(cudaEventRecord(c->ev[1], s));
+    r = batch_launch(b, s, 2);
+    if (r) return r;
+    CK(cudaEventRecord(c->ev[2], s));
+    r = batch_check(b);
+    if (r) return r;
+    std::vector<uint32_t> fs(njobs);
+    CK(cudaMemcpyAsync(fs.data(), b->d_sizes.p, 4 * njobs, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    CK(c->h_out.ensure(b->out_bytes));
+    CK(cudaMemcpyAsync(c->h_out.p, b->d_out.p, b->out_bytes - 64, cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(c->ev[3], s));
+    CK(cudaStreamSynchronize(s));
+    uint64_t egress = 0;
+    for (uint64_t i = 0; i < njobs; i++) {
+        if (jobs[i].status || sizes[i] == 0) continue;
+        if (fs[i] > jobs[i].cap) { jobs[i].status = PRZMG_ERR_BUFFER_TOO_SMALL; continue; }
+        std::memcpy(jobs[i].dst, c->h_out.as<uint8_t>() + b->out_offs[i], fs[i]);
+        jobs[i].out_len = fs[i];
+        egress += fs[i];
+    }
+    if (prof) {
+        *prof = przmg_profile_t{};
+        prof->ingress_dma_bytes = total;
+        prof->ingress_dma_time_ms = ev_ms(c->ev[0], c->ev[1]);
+        prof->kernel_time_ms = ev_ms(c->ev[1], c->ev[2]);
+        prof->egress_dma_bytes = egress;
+        prof->total_round_trip_ms = ev_ms(c->ev[0], c->ev[3]);
+        prof->end_to_end_bandwidth_gbps = gbps((double)total, prof->total_round_trip_ms);
+        prof->internal_vram_bandwidth_gbps = gbps((double)total, prof->kernel_time_ms);
+        prof->pipelined_chunks = (int32_t)njobs;
+        fill_profile(c, prof);
+    }
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_batch_create(przmg_ctx* h, const uint64_t* sizes, uint64_t njobs, int32_t profile,
+                                      przmg_batch** out) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c || !out || (!sizes && njobs)) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    if (profile != PRZMG_PROFILE_D2D && profile != PRZMG_PROFILE_ANS) return fail(PRZMG_ERR_INVALID_ARG, "unknown profile");
+    for (uint64_t i = 0; i < njobs; i++)
+        if (profile == PRZMG_PROFILE_ANS && sizes[i] >= (1u << 24))
+            return fail(PRZMG_ERR_EXCEEDS_MAX_BLOCK, "the frame header holds 24-bit sizes: inputs must be < 16 MiB");
+    LOCKED(c);
+    przmg_batch* b = new przmg_batch();
+    b->ctx = c;
+    b->owned = true;
+    int32_t r = batch_prepare(b, sizes, (uint32_t)njobs, profile, false);
+    if (r) { delete b; return r; }
+    *out = b;
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_batch_inputs(przmg_batch* b, uint64_t* d_in, uint64_t* offsets) {
+    if (!b) return fail(PRZMG_ERR_INVALID_ARG, "null batch");
+    if (d_in) *d_in = (uint64_t)(uintptr_t)b->d_in.p;
+    if (offsets) std::copy(b->in_offs.begin(), b->in_offs.end(), offsets);
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_batch_outputs(przmg_batch* b, uint64_t* d_out, uint64_t* offsets) {
+    if (!b) return fail(PRZMG_ERR_INVALID_ARG, "null batch");
+    if (d_out) *d_out = (uint64_t)(uintptr_t)b->d_out.p;
+    if (offsets) std::copy(b->out_offs.begin(), b->out_offs.end(), offsets);
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_batch_enqueue(przmg_batch* b, uint64_t stream, int32_t use_graph) {
+    if (!b) return fail(PRZMG_ERR_INVALID_ARG, "null batch");
+    Ctx* c = b->ctx;
+    LOCKED(c);
+    cudaStream_t s = stream ? (cudaStream_t)(uintptr_t)stream : c->stream;
+    if (!use_graph) return batch_launch(b, s, 2);
+    if (!b->exec) {
+        cudaStream_t cap_s;
+        CK(cudaStreamCreateWithFlags(&cap_s, cudaStreamNonBlocking));
+        CK(cudaStreamBeginCapture(cap_s, cudaStreamCaptureModeThreadLocal));
+        int32_t r = batch_launch(b, cap_s, 2);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(cap_s, &g);
+        cudaStreamDestroy(cap_s);
+        if (r) { if (g) cudaGraphDestroy(g); return r; }
+        if (e != cudaSuccess) return cuda_fail("cudaStreamEndCapture", e);
+        b->graph = g;
+        CK(cudaGraphInstantiate(&b->exec, g, 0));
+    }
+    CK(cudaGraphLaunch(b->exec, s));
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_batch_sizes(przmg_batch* b, uint32_t* sizes) {
+    if (!b) return fail(PRZMG_ERR_INVALID_ARG, "null batch");
+    Ctx* c = b->ctx;
+    LOCKED(c);
+    CK(cudaDeviceSynchronize());
+    int32_t r = batch_check(b);
+    if (r) return r;
+    if (sizes && b->njobs) {
+        CK(cudaMemcpy(sizes, b->d_sizes.p, 4ull * b->njobs, cudaMemcpyDeviceToHost));
+    }
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_batch_launch_count(przmg_batch* b) { return b ? b->launches : 0; }
+
+extern "C" int32_t przmg_batch_destroy(przmg_batch* b) {
+    if (!b) return PRZMG_OK;
+    Ctx* c = b->ctx;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        cudaSetDevice(c->device);
+        cudaStreamSynchronize(c->stream);
+    }
+    if (b->owned) delete b;
+    return PRZMG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// MatchLZ77
+// ---------------------------------------------------------------------------
+static int32_t match_chunks(Ctx* c, const uint8_t* src, uint64_t n, uint64_t chunk, przmg_match_t* out, uint64_t cap,
+                            uint64_t* n_out, przmg_profile_t* prof) {
+    *n_out = 0;
+    if (prof) *prof = przmg_profile_t{};
+    if (n == 0) { fill_profile(c, prof); return PRZMG_OK; }
+    if (!src || !out) return fail(PRZMG_ERR_INVALID_ARG, "null buffer");
+    std::vector<uint64_t> sizes;
+    for (uint64_t base = 0; base < n; base += chunk) sizes.push_back(std::min<uint64_t>(chunk, n - base));
+    przmg_batch* b = &c->single;
+    int32_t r = batch_prepare(b, sizes.data(), (uint32_t)sizes.size(), PRZMG_PROFILE_D2D, true);
+    if (r) return r;
+    CK(c->h_in.ensure(b->in_bytes));
+    uint64_t base = 0;
+    for (size_t i = 0; i < sizes.size(); i++) {
+        std::memcpy(c->h_in.as<uint8_t>() + b->in_offs[i], src + base, sizes[i]);
+        base += sizes[i];
+    }
+    cudaStream_t s = c->stream;
+    CK(cudaEventRecord(c->ev[0], s));
+    CK(cudaMemcpyAsync(b->d_in.p, c->h_in.p, b->in_bytes - 64, cudaMemcpyHostToDevice, s));
+    CK(cudaEventRecord(c->ev[1], s));
+    r = batch_launch(b, s, 0);
+    if (r) return r;
+    // compaction per chunk into pos/desc arrays
+    uint64_t maxd = 0;
+    for (auto sz : sizes) maxd = std::max<uint64_t>(maxd, sz >= 8 ? (sz - 8) / 8 + 1 : 0);
+    const uint32_t nb_max = (uint32_t)((maxd + 1023) / 1024 + 1);
+    CK(c->d_scr_aux.ensure((size_t)(nb_max + 16) * 4 * sizes.size()));
+    CK(c->d_scr_out.ensure((size_t)2 * 4 * (n / 8 + 16)));
+    uint32_t* d_pos = c->d_scr_out.as<uint32_t>();
+    uint32_t* d_dsc = d_pos + (n / 8 + 16);
+    std::vector<uint32_t> totals(sizes.size(), 0);
+    uint64_t pos_base = 0;
+    for (size_t i = 0; i < sizes.size(); i++) {
+        const Job& j = b->jobs[i];
+        const uint32_t nd = j.n >= 8 ? (j.n - 8) / 8 + 1 : 0;
+        if (nd) {
+            const uint32_t nbk = (nd + 1023) / 1024;
+            uint32_t* cnt = c->d_scr_aux.as<uint32_t>() + i * (nb_max + 16);
+            uint32_t* tot = cnt + nb_max + 8;
+            const uint32_t* d8 = b->d_desc.as<uint32_t>() + j.desc_off;
+            k_compact_count<<<nbk, 1024, 0, s>>>(d8, nd, cnt);
+            k_compact_scan<<<1, 1024, 0, s>>>(cnt, nbk, tot);
+            CK(cudaMemcpyAsync(&totals[i], tot, 4, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            k_compact_scatter<<<nbk, 1024, 0, s>>>(d8, nd, cnt, (uint32_t)pos_base, d_pos + *n_out, d_dsc + *n_out);
+            CK(cudaGetLastError());
+            *n_out += totals[i];
+        }
+        pos_base += sizes[i];
+    }
+    CK(cudaEventRecord(c->ev[2], s));
+    const uint64_t m = *n_out;
+    if (m > cap) return fail(PRZMG_ERR_BUFFER_TOO_SMALL, "match buffer too small");
+    CK(c->h_out.ensure(8 * m + 64));
+    uint32_t* hp = c->h_out.as<uint32_t>();
+    if (m) {
+        CK(cudaMemcpyAsync(hp, d_pos, 4 * m, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(hp + m, d_dsc, 4 * m, cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaEventRecord(c->ev[3], s));
+    CK(cudaStreamSynchronize(s));
+    for (uint64_t k = 0; k < m; k++) {
+        out[k].position = hp[k];
+        out[k].offset = hp[m + k] & 0xFFFFFu;
+        out[k].length = (uint16_t)(hp[m + k] >> 20);
+        out[k].literal = 0;
+        out[k].reserved = 0;
+    }
+    if (prof) {
+        prof->ingress_dma_bytes = n;
+        prof->ingress_dma_time_ms = ev_ms(c->ev[0], c->ev[1]);
+        prof->ingress_dma_bandwidth_gbps = gbps((double)n, prof->ingress_dma_time_ms);
+        prof->kernel_time_ms = ev_ms(c->ev[1], c->ev[2]);
+        prof->internal_vram_bandwidth_gbps = gbps((double)n, prof->kernel_time_ms);
+        prof->egress_dma_bytes = 8 * m;
+        prof->egress_dma_time_ms = ev_ms(c->ev[2], c->ev[3]);
+        prof->egress_dma_bandwidth_gbps = gbps(8.0 * m, prof->egress_dma_time_ms);
+        prof->total_round_trip_ms = ev_ms(c->ev[0], c->ev[3]);
+        prof->end_to_end_bandwidth_gbps = gbps((double)n, prof->total_round_trip_ms);
+        if (prof->total_round_trip_ms > 0)
+            prof->pcie_overhead_percent = 100.0 * (prof->ingress_dma_time_ms + prof->egress_dma_time_ms) / prof->total_round_trip_ms;
+        prof->pipelined_chunks = (int32_t)sizes.size();
+        fill_profile(c, prof);
+    }
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_match_lz77(przmg_ctx* h, const uint8_t* src, uint64_t n, przmg_match_t* out, uint64_t cap,
+                                    uint64_t* n_out, przmg_profile_t* prof) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c || !n_out) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    if (int32_t m = mock_check()) return m;
+    LOCKED(c);
+    // > 16 MiB streams in 8 MiB chunks (gpu/bridge.go:1494-1496)
+    return match_chunks(c, src, n, n > (16ull << 20) ? (8ull << 20) : std::max<uint64_t>(n, 1), out, cap, n_out, prof);
+}
+
+extern "C" int32_t przmg_match_lz77_streaming(przmg_ctx* h, const uint8_t* src, uint64_t n, int64_t chunk,
+                                              przmg_match_t* out, uint64_t cap, uint64_t* n_out, przmg_profile_t* prof) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c || !n_out) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    if (int32_t m = mock_check()) return m;
+    LOCKED(c);
+    // chunk rule of matchLZ77StreamingLocked, gpu/bridge.go:1222-1233
+    uint64_t cs = chunk > 0 ? (uint64_t)chunk : std::max<uint64_t>(n / 2, 16ull << 20);
+    cs = std::min<uint64_t>(cs, 64ull << 20);
+    if ((n + cs - 1) / std::max<uint64_t>(cs, 1) <= 1) cs = std::max<uint64_t>(n, 1);
+    return match_chunks(c, src, n, cs, out, cap, n_out, prof);
+}
+
+// ---------------------------------------------------------------------------
+// histogram / flat pack / V-ANS single-stream APIs and the stream batch
+// ---------------------------------------------------------------------------
+#include "api_streams.inc"
+
+// ---------------------------------------------------------------------------
+// pinned memory
+// ---------------------------------------------------------------------------
+extern "C" int32_t przmg_alloc_pinned_host(uint64_t size, void** out) {
+    if (!out) return fail(PRZMG_ERR_INVALID_ARG, "null output pointer");
+    *out = nullptr;
+    if (size == 0) return PRZMG_OK;
+    CK(cudaHostAlloc(out, size, cudaHostAllocDefault));
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_free_pinned_host(void* p) {
+    if (!p) return PRZMG_OK;
+    CK(cudaFreeHost(p));
+    return PRZMG_OK;
+}

@@ -1,0 +1,150 @@
+// common.cuh -- shared constants, job descriptors and device helpers of the
+// PRZM B200 compression path.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pz {
+
+// ---- format constants (reference: gpu/kernel/przm_lz77.h:21-38,
+//      przm_lz77.cu:24-33, przm_ans.h:22-36, gpu/bridge.go:148-153) ----------
+constexpr uint32_t kTile = 32768;            // finder and tokenizer tile
+constexpr uint32_t kBuckets = 2048;          // tile-finder hash buckets
+constexpr uint32_t kHashPrime = 0x1E35A7BDu; // przm_gpu_hash4
+constexpr uint32_t kRadixBuckets = 524288;   // radix-strike table (2^19)
+constexpr uint64_t kRadixPrime = 0x9E3779B97F4A7C15ull;
+constexpr uint32_t kWindow = 1u << 20;       // Window1M passed by the bridge
+constexpr uint32_t kMaxLen32 = 4095;
+constexpr uint32_t kMaxOff32 = 1048575;
+constexpr uint32_t kSmallMax = 65536;        // n <= 64 KiB -> tile finder
+constexpr uint32_t kCandPerTile = kTile / 8; // radix candidates per tile
+
+// Per-tile output slots of the tokenizer.  Bounds: every command token covers
+// >= 4 input bytes per command byte (literal flush + token included), so a
+// tile emits <= 8192 + 4 command bytes; offsets are <= 3 bytes per >= 4-byte
+// explicit match; literals never exceed the tile.  Writes are checked against
+// these sizes on the device.
+constexpr uint32_t kSlotCmd = 8704;
+constexpr uint32_t kSlotOff = 24832;
+constexpr uint32_t kSlotLit = 33024;
+
+enum Stream : int { S_CMD = 0, S_OP = 1, S_META = 2, S_VAR = 3, S_OFF = 4, S_LIT = 5, S_COUNT = 6 };
+
+// ANS task slots per job: literal stream (adaptive) and the three command
+// substreams, each with the Meta8 and the adaptive model.
+enum Task : int { T_LIT = 0, T_OP_M8 = 1, T_OP_AD = 2, T_META_M8 = 3, T_META_AD = 4, T_VAR_M8 = 5, T_VAR_AD = 6, T_COUNT = 7 };
+
+// error bits reported through the per-batch status word
+enum Err : uint32_t { E_SLOT_OVERFLOW = 1, E_STREAM_OVERFLOW = 2, E_BAD_TOKEN = 4, E_TABLE = 8 };
+
+struct Job {
+    uint64_t in_off;    // input byte offset (16-byte aligned)
+    uint64_t desc_off;  // u32 index of this job's descriptor table
+    uint64_t str_off;   // byte offset of this job's stream region
+    uint64_t ans_off;   // byte offset of this job's ANS scratch region
+    uint64_t out_off;   // byte offset of this job's frame
+    uint32_t n;         // input bytes
+    uint32_t tile0;     // first global tile index
+    uint32_t ntiles;
+    uint32_t kind;      // 0: tile finder (n <= 64 KiB), 1: radix strike
+    uint32_t cmd_cap;   // capacity of cmd/op/meta/var streams
+    uint32_t off_cap;   // capacity of the offset stream
+    uint32_t lit_cap;   // capacity of the literal stream
+    uint32_t profile;   // 0: CompressD2D frame (P0), 1: entropy-coded frame (P1)
+    uint32_t out_cap;
+    uint32_t pad;
+};
+
+// byte offsets of the six streams inside a job's stream region
+__host__ __device__ inline uint64_t stream_base(const Job& j, int s) {
+    const uint64_t c = j.cmd_cap, o = j.off_cap;
+    switch (s) {
+        case S_CMD: return 0;
+        case S_OP: return c;
+        case S_META: return 2 * c;
+        case S_VAR: return 3 * c;
+        case S_OFF: return 4 * c;
+        default: return 4 * c + o;
+    }
+}
+__host__ __device__ inline uint64_t stream_region_bytes(const Job& j) {
+    return 4ull * j.cmd_cap + j.off_cap + j.lit_cap;
+}
+
+// ANS scratch of one task: four lane byte streams then four lane count
+// words (2 bits per round).  L = symbol capacity of the task's stream.
+__host__ __device__ inline uint64_t ans_lane_cap(uint32_t L) { return 2ull * ((L + 3) / 4) + 16; }
+__host__ __device__ inline uint64_t ans_nbw_cap(uint32_t L) { return (((L + 3) / 4) + 15) / 16 + 1; }  // u32 words
+__host__ __device__ inline uint64_t ans_task_bytes(uint32_t L) {
+    uint64_t b = 4 * ans_lane_cap(L) + 4 * 4 * ans_nbw_cap(L);
+    return (b + 15) & ~15ull;
+}
+__host__ __device__ inline uint32_t task_cap(const Job& j, int t) { return t == T_LIT ? j.lit_cap : j.cmd_cap; }
+__host__ __device__ inline uint64_t ans_task_off(const Job& j, int t) {
+    uint64_t o = 0;
+    for (int k = 0; k < t; k++) o += ans_task_bytes(task_cap(j, k));
+    return o;
+}
+__host__ __device__ inline uint64_t ans_region_bytes(const Job& j) { return ans_task_off(j, T_COUNT); }
+
+// Encoding table entry for one symbol of one model:
+//   m   : 32-bit reciprocal so that floor(x_r / f) == umulhi(x_r, m) >> s for
+//         every x_r < 2^24 (Granlund-Montgomery 1994, round-up variant);
+//         f = 2^t uses m = 2^(32-t), s = 0; f = 1 uses m = 2^32-1 (one short)
+//         with the deficit folded into cb.
+//   t1  : 4096 * f, the renormalisation bound (x >= t1 -> emit a byte)
+//   cb  : cumulative frequency c (+4095 when f == 1)
+//   cfs : (4096 - f) | s << 16
+struct __align__(16) EncSym {
+    uint32_t m, t1, cb, cfs;
+};
+
+// Per-task results of the rANS kernel.
+struct TaskOut {
+    uint32_t state[4];
+    uint32_t count[4];  // bytes emitted by each lane
+};
+
+// Per-job section plan computed by the selection kernel.
+struct Plan {
+    uint32_t frame_size;
+    uint32_t flags;
+    uint32_t l2, l3, l4;      // section sizes
+    uint32_t sub_len[3];      // packed op/meta/var substream sizes (Mode 8)
+    uint32_t sub_mode[3];     // 0 flat 0x09, 1 Meta8, 2 adaptive
+    uint32_t s2_mode;         // 0 flat 0x00 (P0), 1 Mode 8, 2 flat 0x09
+    uint32_t s4_mode;         // 0 raw, 1 V-ANS
+    uint32_t uncompressed;
+    uint32_t wlog;
+};
+
+struct TableInfo {            // adaptive model of one (job, stream)
+    uint32_t mat_len;
+    uint32_t active;
+    uint8_t mat[600];         // serialized 16x16 joint-nibble matrix (<= 2 + 32 + 512)
+};
+
+// ---- device helpers --------------------------------------------------------
+__device__ __forceinline__ uint32_t ld32_smem_u(const uint8_t* base, uint32_t i) {
+    // unaligned little-endian u32 from a 4-byte aligned shared buffer padded by 8 bytes
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(base) + (i >> 2);
+    return __funnelshift_r(w[0], w[1], (i & 3) * 8);
+}
+
+__device__ __forceinline__ uint64_t ld64_global_u(const uint8_t* p) {
+    // unaligned u64 through two aligned loads; buffers are padded by 16 bytes
+    uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uint64_t* w = reinterpret_cast<const uint64_t*>(a & ~uintptr_t(7));
+    uint32_t sh = (uint32_t)(a & 7) * 8;
+    uint64_t lo = __ldg(w), hi = __ldg(w + 1);
+    return sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
+}
+
+__device__ __forceinline__ uint32_t ld32_global_u(const uint8_t* p) { return (uint32_t)ld64_global_u(p); }
+
+__device__ __forceinline__ uint32_t pack_match32(uint32_t len, uint32_t off) {
+    if (len < 4 || off == 0) return 0;
+    return ((len > kMaxLen32 ? kMaxLen32 : len) << 20) | (off & 0xFFFFFu);
+}
+
+}  // namespace pz

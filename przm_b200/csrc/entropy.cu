@@ -1,0 +1,511 @@
+// entropy.cu -- frequency normalisation, 4-lane interleaved rANS (V-ANS and
+// Meta8) and stitching of the lane outputs into the reference byte order.
+#include "common.cuh"
+#include "meta8_tables.h"
+
+namespace pz {
+
+// ---------------------------------------------------------------------------
+// Encoding tables.
+// ---------------------------------------------------------------------------
+__host__ __device__ inline EncSym make_encsym(uint32_t f, uint32_t c) {
+    EncSym e;
+    if (f == 0) { e.m = 0; e.t1 = 0xFFFFFFFFu; e.cb = 0; e.cfs = 0; return e; }
+    uint32_t s = 0;
+    while ((2u << s) <= f) s++;  // floor(log2 f)
+    uint32_t cb = c;
+    if (f == 1) { e.m = 0xFFFFFFFFu; s = 0; cb = c + 4095; }
+    else if ((f & (f - 1)) == 0) { e.m = 1u << (32 - s); s = 0; }
+    else e.m = (uint32_t)(((1ull << (32 + s)) + f - 1) / f);
+    e.t1 = 4096u * f;
+    e.cb = cb;
+    e.cfs = (4096u - f) | (s << 16);
+    return e;
+}
+
+// SerializeMatrix (gpu/bridge.go:2844-2886) == EncodeJointNibbleFreq
+// (core/literals/literals.go:143-184).
+__host__ __device__ inline uint32_t serialize_matrix(const uint16_t* freq, uint8_t* out) {
+    uint32_t n = 0;
+    uint32_t rowMask = 0;
+    for (int h = 0; h < 16; h++)
+        for (int l = 0; l < 16; l++)
+            if (freq[(h << 4) | l]) { rowMask |= 1u << h; break; }
+    out[n++] = (uint8_t)rowMask;
+    out[n++] = (uint8_t)(rowMask >> 8);
+    for (int h = 0; h < 16; h++) {
+        if (!(rowMask & (1u << h))) continue;
+        uint32_t colMask = 0;
+        for (int l = 0; l < 16; l++)
+            if (freq[(h << 4) | l]) colMask |= 1u << l;
+        out[n++] = (uint8_t)colMask;
+        out[n++] = (uint8_t)(colMask >> 8);
+        for (int l = 0; l < 16; l++) {
+            if (!(colMask & (1u << l))) continue;
+            uint32_t w = freq[(h << 4) | l];
+            if (w < 128) out[n++] = (uint8_t)w;
+            else { out[n++] = (uint8_t)(0x80 | (w >> 8)); out[n++] = (uint8_t)(w & 0xFF); }
+        }
+    }
+    return n;
+}
+
+// ---------------------------------------------------------------------------
+// Go sort.Slice (pdqsort, Go standard library sort/zsortfunc.go, Go >= 1.19)
+// restated for the descending-remainder sort of NormalizeFreq
+// (gpu/bridge.go:2818-2824); it fixes where equal remainders land.
+// ---------------------------------------------------------------------------
+struct GoRem { uint32_t sym; uint64_t rem; };
+struct GoSort {
+    GoRem* v;
+    __host__ __device__ bool less(int i, int j) const { return v[i].rem > v[j].rem; }
+    __host__ __device__ void swap(int i, int j) { GoRem t = v[i]; v[i] = v[j]; v[j] = t; }
+    __host__ __device__ void insertion(int a, int b) {
+        for (int i = a + 1; i < b; i++)
+            for (int j = i; j > a && less(j, j - 1); j--) swap(j, j - 1);
+    }
+    __host__ __device__ void sift(int lo, int hi, int first) {
+        int root = lo;
+        for (;;) {
+            int child = 2 * root + 1;
+            if (child >= hi) return;
+            if (child + 1 < hi && less(first + child, first + child + 1)) child++;
+            if (!less(first + root, first + child)) return;
+            swap(first + root, first + child);
+            root = child;
+        }
+    }
+    __host__ __device__ void heap(int a, int b) {
+        int first = a, hi = b - a;
+        for (int i = (hi - 1) / 2; i >= 0; i--) sift(i, hi, first);
+        for (int i = hi - 1; i >= 0; i--) { swap(first, first + i); sift(0, i, first); }
+    }
+    __host__ __device__ static int bits_len(unsigned x) { int n = 0; while (x) { n++; x >>= 1; } return n; }
+    __host__ __device__ void break_patterns(int a, int b) {
+        int length = b - a;
+        if (length < 8) return;
+        uint64_t r = (uint64_t)length;
+        unsigned modulus = 1u << bits_len((unsigned)length);
+        int idx = a + (length / 4) * 2 - 1;
+        for (int i = 0; i < 3; i++) {
+            r ^= r << 13; r ^= r >> 7; r ^= r << 17;
+            int other = (int)((unsigned)r & (modulus - 1));
+            if (other >= length) other -= length;
+            swap(idx - 1 + i, a + other);
+        }
+    }
+    __host__ __device__ void order2(int& a, int& b, int& swaps) {
+        if (less(b, a)) { int t = a; a = b; b = t; swaps++; }
+    }
+    __host__ __device__ int median(int a, int b, int c, int& swaps) {
+        order2(a, b, swaps); order2(b, c, swaps); order2(a, b, swaps);
+        return b;
+    }
+    __host__ __device__ int choose_pivot(int a, int b, int& hint) {
+        int l = b - a, swaps = 0;
+        int i = a + l / 4 * 1, j = a + l / 4 * 2, k = a + l / 4 * 3;
+        if (l >= 8) {
+            if (l >= 50) {
+                i = median(i - 1, i, i + 1, swaps);
+                j = median(j - 1, j, j + 1, swaps);
+                k = median(k - 1, k, k + 1, swaps);
+            }
+            j = median(i, j, k, swaps);
+        }
+        hint = swaps == 0 ? 1 : (swaps == 12 ? 2 : 0);
+        return j;
+    }
+    __host__ __device__ void reverse(int a, int b) { for (int i = a, j = b - 1; i < j; i++, j--) swap(i, j); }
+    __host__ __device__ bool partial_insertion(int a, int b) {
+        int i = a + 1;
+        for (int step = 0; step < 5; step++) {
+            while (i < b && !less(i, i - 1)) i++;
+            if (i == b) return true;
+            if (b - a < 50) return false;
+            swap(i, i - 1);
+            if (i - a >= 2)
+                for (int j = i - 1; j >= 1; j--) { if (!less(j, j - 1)) break; swap(j, j - 1); }
+            if (b - i >= 2)
+                for (int j = i + 1; j < b; j++) { if (!less(j, j - 1)) break; swap(j, j - 1); }
+        }
+        return false;
+    }
+    __host__ __device__ int partition_equal(int a, int b, int pivot) {
+        swap(a, pivot);
+        int i = a + 1, j = b - 1;
+        for (;;) {
+            while (i <= j && !less(a, i)) i++;
+            while (i <= j && less(a, j)) j--;
+            if (i > j) break;
+            swap(i, j); i++; j--;
+        }
+        return i;
+    }
+    __host__ __device__ int partition(int a, int b, int pivot, bool& already) {
+        swap(a, pivot);
+        int i = a + 1, j = b - 1;
+        while (i <= j && less(i, a)) i++;
+        while (i <= j && !less(j, a)) j--;
+        if (i > j) { swap(j, a); already = true; return j; }
+        swap(i, j); i++; j--;
+        for (;;) {
+            while (i <= j && less(i, a)) i++;
+            while (i <= j && !less(j, a)) j--;
+            if (i > j) break;
+            swap(i, j); i++; j--;
+        }
+        swap(j, a);
+        already = false;
+        return j;
+    }
+    // pdqsort_func: the recursion goes to the smaller side, so its depth is
+    // at most log2(n) + 1 (<= 9 for the 256-entry remainder list)
+    __host__ __device__ void pdq(int a, int b, int limit) {
+        bool was_balanced = true, was_partitioned = true;
+        for (;;) {
+            int length = b - a;
+            if (length <= 12) { insertion(a, b); return; }
+            if (limit == 0) { heap(a, b); return; }
+            if (!was_balanced) { break_patterns(a, b); limit--; }
+            int hint;
+            int pivot = choose_pivot(a, b, hint);
+            if (hint == 2) { reverse(a, b); pivot = (b - 1) - (pivot - a); hint = 1; }
+            if (was_balanced && was_partitioned && hint == 1)
+                if (partial_insertion(a, b)) return;
+            if (a > 0 && !less(a - 1, pivot)) { a = partition_equal(a, b, pivot); continue; }
+            bool already;
+            int mid = partition(a, b, pivot, already);
+            was_partitioned = already;
+            int left = mid - a, right = b - mid, thr = length / 8;
+            if (left < right) {
+                was_balanced = left >= thr;
+                pdq(a, mid, limit);
+                a = mid + 1;
+            } else {
+                was_balanced = right >= thr;
+                pdq(mid + 1, b, limit);
+                b = mid;
+            }
+        }
+    }
+    __host__ __device__ void sort(int n) { pdq(0, n, bits_len((unsigned)n)); }
+};
+
+
+// ---------------------------------------------------------------------------
+// Normalisers (one warp per histogram).  All lanes return the same table.
+// ---------------------------------------------------------------------------
+
+// literals.NormalizeFrequencies + adjustFrequencySum
+// (core/literals/literals.go:78-140): f = 1 + c*(4096-unique)/total, then the
+// shortfall goes +1 each to the symbols with the largest counts (lowest
+// symbol first among equal counts).
+__device__ void warp_normalize_frequencies(const uint32_t* __restrict__ cnt /* smem */, uint16_t* __restrict__ freq /* smem */,
+                                           uint32_t lane) {
+    uint64_t total = 0;
+    uint32_t unique = 0;
+    for (uint32_t s = lane; s < 256; s += 32) { total += cnt[s]; unique += cnt[s] ? 1 : 0; }
+    for (int o = 16; o; o >>= 1) {
+        total += __shfl_xor_sync(0xFFFFFFFFu, total, o);
+        unique += __shfl_xor_sync(0xFFFFFFFFu, unique, o);
+    }
+    uint32_t sum = 0;
+    for (uint32_t s = lane; s < 256; s += 32) {
+        uint32_t f = 0;
+        if (cnt[s]) f = 1 + (uint32_t)(((uint64_t)cnt[s] * (4096 - unique)) / total);
+        freq[s] = (uint16_t)f;
+        sum += f;
+    }
+    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+    __syncwarp();
+    if (unique == 0) return;
+    const int diff = 4096 - (int)(sum & 0xFFFF);
+    if (diff > 0) {
+        // rank among active symbols by (count desc, symbol asc)
+        for (uint32_t s = lane; s < 256; s += 32) {
+            const uint32_t c = cnt[s];
+            if (!c) continue;
+            uint32_t rank = 0;
+            for (uint32_t t = 0; t < 256; t++) {
+                const uint32_t ct = cnt[t];
+                rank += (ct > c || (ct == c && ct != 0 && t < s)) ? 1 : 0;
+            }
+            if (rank < (uint32_t)diff) freq[s] = (uint16_t)(freq[s] + 1);
+        }
+    } else if (diff < 0 && lane == 0) {
+        for (int it = 0; it < -diff; it++)
+            for (int s = 255; s >= 0; s--)
+                if (freq[s] > 1) { freq[s]--; break; }
+    }
+    __syncwarp();
+}
+
+// gpu.NormalizeFreq (gpu/bridge.go:2777-2829): f = 1 + c*(M-active)/total,
+// then +1 to the symbols with the largest remainders in Go sort.Slice order.
+__device__ void warp_normalize_freq_go(const uint32_t* __restrict__ cnt, uint16_t* __restrict__ freq, GoRem* __restrict__ rems,
+                                       uint32_t lane) {
+    if (lane == 0) {
+        uint64_t total = 0;
+        int active = 0;
+        for (int s = 0; s < 256; s++) { freq[s] = 0; total += cnt[s]; active += cnt[s] ? 1 : 0; }
+        if (total != 0 && active != 0) {
+            const uint32_t rt = 4096 - (uint32_t)active;
+            uint32_t alloc = 0;
+            int nr = 0;
+            for (int s = 0; s < 256; s++) {
+                if (!cnt[s]) continue;
+                const uint64_t prod = (uint64_t)cnt[s] * rt;
+                const uint32_t add = (uint32_t)(prod / total);
+                freq[s] = (uint16_t)(1 + add);
+                alloc += 1 + add;
+                rems[nr].sym = (uint32_t)s;
+                rems[nr].rem = prod % total;
+                nr++;
+            }
+            if (alloc < 4096) {
+                const int diff = (int)(4096 - alloc);
+                GoSort g{rems};
+                g.sort(nr);
+                for (int i = 0; i < diff && i < nr; i++) freq[rems[i].sym]++;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// CDF + encoding table + serialized matrix of one normalised model.
+__device__ void warp_build_table(const uint16_t* __restrict__ freq /* smem */, EncSym* __restrict__ tab, TableInfo* __restrict__ info,
+                                 uint32_t lane) {
+    // exclusive prefix sum over 256 frequencies, 8 per lane in symbol order
+    uint32_t f[8], loc = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) { f[k] = freq[lane * 8 + k]; loc += f[k]; }
+    uint32_t x = loc;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    uint32_t c = x - loc;
+#pragma unroll
+    for (int k = 0; k < 8; k++) { tab[lane * 8 + k] = make_encsym(f[k], c); c += f[k]; }
+    if (lane == 0) {
+        uint32_t act = 0;
+        for (int s = 0; s < 256; s++) act += freq[s] ? 1 : 0;
+        info->active = act;
+        info->mat_len = serialize_matrix(freq, info->mat);
+    }
+}
+
+// One warp per (frame, model stream): lit, op, meta, var.
+__global__ void k_normalize(const Job* __restrict__ jobs, uint32_t njobs, const uint32_t* __restrict__ job_lens,
+                            const uint32_t* __restrict__ hist, EncSym* __restrict__ tabs, TableInfo* __restrict__ infos) {
+    __shared__ uint32_t s_cnt[4][256];
+    __shared__ uint16_t s_freq[4][256];
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t gw = blockIdx.x * 4 + w;
+    if (gw >= njobs * 4) return;
+    const uint32_t j = gw >> 2, si = gw & 3;
+    (void)job_lens;
+    for (uint32_t s = lane; s < 256; s += 32) s_cnt[w][s] = hist[(uint64_t)j * 1024 + si * 256 + s];
+    __syncwarp();
+    warp_normalize_frequencies(s_cnt[w], s_freq[w], lane);
+    warp_build_table(s_freq[w], tabs + (uint64_t)gw * 256, infos + gw, lane);
+    (void)jobs;
+}
+
+// ---------------------------------------------------------------------------
+// 4-lane interleaved rANS: one thread per lane.
+//
+// Encoder of core/literals/literals.go:289-341 / przm_ans.cu:270-313 and of
+// core/commands/vans_meta.go:104-138: lane = i & 3 of symbol i, symbols
+// consumed from the end, x starts at 65536, bytes leave from the low end
+// while x >= 4096*f, then x = (x/f)*4096 + c + x%f.  The reference writes all
+// lanes' bytes into one stream in processing order and reverses it; here each
+// lane writes its own bytes in order together with 2-bit counts per round,
+// and the stitch below interleaves them into exactly that reversed stream.
+// The division is a multiply-high by a per-symbol reciprocal (exact for
+// x < 2^24, see EncSym).
+// ---------------------------------------------------------------------------
+struct LaneIO {
+    uint8_t* bytes;     // lane byte stream
+    uint32_t* nbw;      // 2-bit emitted-byte counts, 16 rounds per word (round j -> word j/16)
+};
+
+__device__ __forceinline__ LaneIO lane_io(uint8_t* task_base, uint32_t cap, uint32_t l) {
+    LaneIO io;
+    io.bytes = task_base + (uint64_t)l * ans_lane_cap(cap);
+    io.nbw = reinterpret_cast<uint32_t*>(task_base + 4 * ans_lane_cap(cap)) + (uint64_t)l * ans_nbw_cap(cap);
+    return io;
+}
+
+template <bool kMeta8>
+__device__ __forceinline__ void rans_lane(const uint8_t* __restrict__ src, uint32_t n, uint32_t l,
+                                          const EncSym* __restrict__ tab, const uint8_t* __restrict__ ctxlut,
+                                          LaneIO io, uint32_t* out_state, uint32_t* out_count) {
+    uint32_t x = 65536, cnt = 0, acc = 0;
+    if (n > l) {
+        const int32_t J = (int32_t)((n - 1 - l) >> 2);
+        for (int32_t j = J; j >= 0; j--) {
+            const uint32_t i = 4u * (uint32_t)j + l;
+            const uint32_t s = src[i];
+            uint32_t ti = s;
+            if (kMeta8) ti |= (i ? (uint32_t)ctxlut[src[i - 1]] : 0u) << 8;
+            const EncSym e = tab[ti];
+            const uint32_t k = (x >= e.t1 ? 1u : 0u) + ((x >> 8) >= e.t1 ? 1u : 0u);
+            io.bytes[cnt] = (uint8_t)x;
+            io.bytes[cnt + 1] = (uint8_t)(x >> 8);
+            cnt += k;
+            const uint32_t xr = x >> (8 * k);
+            const uint32_t q = __umulhi(xr, e.m) >> (e.cfs >> 16);
+            x = xr + q * (e.cfs & 0xFFFFu) + e.cb;
+            acc |= k << (2 * (j & 15));
+            if ((j & 15) == 0) { io.nbw[j >> 4] = acc; acc = 0; }
+        }
+    }
+    *out_state = x;
+    *out_count = cnt;
+}
+
+// Meta8 static model (core/commands/vans_meta_tables.go) in EncSym form,
+// 8 x 256 entries, and the context classifier ContextMeta
+// (core/commands/vans_meta.go:46-69) as a 256-entry table; built on the host.
+inline void build_meta8_tables(EncSym* tab, uint8_t* ctxlut) {
+    for (int c = 0; c < 8; c++) {
+        uint32_t cum = 0;
+        for (int s = 0; s < 256; s++) {
+            tab[c * 256 + s] = make_encsym(przm_meta8_freq[c][s], cum);
+            cum += przm_meta8_freq[c][s];
+        }
+    }
+    for (int p = 0; p < 256; p++)
+        ctxlut[p] = p == 0 ? 0 : p < 4 ? 1 : p < 16 ? 2 : p < 32 ? 3 : p < 64 ? 4 : p < 128 ? 5 : p < 192 ? 6 : 7;
+}
+
+// Task eligibility for the entropy-coded frame (packSubstream,
+// core/commands/commands.go:371-406; PackageLiteralsSection selection).
+__host__ __device__ inline uint32_t task_len(const uint32_t* lens, int t) {
+    return t == T_LIT ? lens[S_LIT] : lens[S_OP + (t - 1) / 2];
+}
+__host__ __device__ inline bool task_active(const Job& job, const uint32_t* lens, int t) {
+    if (job.profile != 1) return false;
+    const uint32_t n = task_len(lens, t);
+    if (t == T_LIT) return n >= 1 && n <= (8u << 20);
+    if (lens[S_CMD] > (2u << 20)) return false;
+    const bool m8 = (t & 1) == 1;  // T_OP_M8, T_META_M8, T_VAR_M8 are odd
+    return n <= (2u << 20) && n >= (m8 ? 24u : 16u);
+}
+
+__global__ void __launch_bounds__(128) k_rans(const Job* __restrict__ jobs, uint32_t njobs,
+                                              const uint32_t* __restrict__ job_lens,
+                                              const uint8_t* __restrict__ streams, uint8_t* __restrict__ ans,
+                                              const EncSym* __restrict__ tabs, const EncSym* __restrict__ meta8,
+                                              const uint8_t* __restrict__ ctxlut, TaskOut* __restrict__ outs) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t task = g >> 2, l = g & 3;
+    if (task >= njobs * T_COUNT) return;
+    const uint32_t j = task / T_COUNT;
+    const int t = (int)(task % T_COUNT);
+    const Job job = jobs[j];
+    const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
+    if (!task_active(job, lens, t)) return;
+    const uint32_t n = task_len(lens, t);
+    const int s = t == T_LIT ? S_LIT : S_OP + (t - 1) / 2;
+    const uint8_t* src = streams + job.str_off + stream_base(job, s);
+    uint8_t* base = ans + job.ans_off + ans_task_off(job, t);
+    LaneIO io = lane_io(base, task_cap(job, t), l);
+    TaskOut* o = outs + task;
+    const bool m8 = t != T_LIT && (t & 1) == 1;
+    if (m8) {
+        rans_lane<true>(src, n, l, meta8, ctxlut, io, &o->state[l], &o->count[l]);
+    } else {
+        const int mi = t == T_LIT ? 0 : 1 + (t - 1) / 2;  // model index: lit, op, meta, var
+        rans_lane<false>(src, n, l, tabs + ((uint64_t)j * 4 + mi) * 256, nullptr, io, &o->state[l], &o->count[l]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Stitch: write the reference byte order of a 4-lane rANS stream, i.e. the
+// reversal of the interleaved emission sequence.  For rounds j = 0, 1, ...
+// and lanes l = 0..3 it places lane l's bytes of round j (last-emitted first).
+// Lane l's bytes of round j sit at count_l - (bytes of rounds <= j) in its own
+// stream because the lane emitted rounds in descending order.
+// Runs on a whole CTA; rounds are scanned 16 per thread per pass.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t sum2(uint32_t w) {  // sum of the 16 2-bit fields
+    w = (w & 0x33333333u) + ((w >> 2) & 0x33333333u);
+    w = (w + (w >> 4)) & 0x0F0F0F0Fu;
+    return (w * 0x01010101u) >> 24;
+}
+
+template <int NT>
+__device__ void block_stitch(const uint8_t* task_base, uint32_t cap, uint32_t n, const uint32_t* count,
+                             uint8_t* __restrict__ out) {
+    __shared__ uint32_t s_scan[NT];
+    __shared__ uint32_t s_carry[4];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t rounds = (n + 3) / 4;
+    const uint8_t* lb[4];
+    const uint32_t* nw[4];
+    for (uint32_t l = 0; l < 4; l++) {
+        lb[l] = task_base + (uint64_t)l * ans_lane_cap(cap);
+        nw[l] = reinterpret_cast<const uint32_t*>(task_base + 4 * ans_lane_cap(cap)) + (uint64_t)l * ans_nbw_cap(cap);
+    }
+    if (tid < 4) s_carry[tid] = 0;  // per-lane bytes of rounds already done
+    __syncthreads();
+    for (uint32_t r0 = 0; r0 < rounds; r0 += 16 * NT) {
+        const uint32_t rb = r0 + 16 * tid;  // this thread's first round (multiple of 16)
+        uint32_t w[4] = {0, 0, 0, 0}, c[4] = {0, 0, 0, 0};
+        if (rb < rounds) {
+            for (uint32_t l = 0; l < 4; l++) {
+                // lanes with no symbol in the top partial word have their bits
+                // cleared by construction (those rounds were never processed)
+                const uint32_t jmax = n > l ? (n - 1 - l) / 4 : 0;
+                if (n > l && rb <= jmax) {
+                    uint32_t v = nw[l][rb >> 4];
+                    const uint32_t top = jmax - rb;  // rounds of this word that exist
+                    if (top < 15) v &= (1u << (2 * (top + 1))) - 1u;
+                    w[l] = v;
+                    c[l] = sum2(v);
+                }
+            }
+        }
+        // block exclusive scan of the four per-lane counts packed in 8-bit
+        // fields would overflow; scan them one lane at a time instead
+        uint32_t pre[4];
+        for (uint32_t l = 0; l < 4; l++) {
+            s_scan[tid] = c[l];
+            __syncthreads();
+            for (uint32_t o = 1; o < NT; o <<= 1) {
+                uint32_t t = tid >= o ? s_scan[tid - o] : 0;
+                __syncthreads();
+                s_scan[tid] += t;
+                __syncthreads();
+            }
+            pre[l] = s_carry[l] + s_scan[tid] - c[l];
+            const uint32_t tot = s_scan[NT - 1];
+            __syncthreads();
+            if (tid == 0) s_carry[l] += tot;
+            __syncthreads();
+        }
+        if (rb < rounds) {
+            // output position of round rb = bytes of all lanes in rounds < rb
+            uint32_t op = pre[0] + pre[1] + pre[2] + pre[3];
+            uint32_t lp[4] = {pre[0], pre[1], pre[2], pre[3]};  // per-lane bytes of rounds < current
+            const uint32_t re = min(rounds, rb + 16);
+            for (uint32_t jr = rb; jr < re; jr++) {
+                const uint32_t sh = 2 * (jr & 15);
+                for (uint32_t l = 0; l < 4; l++) {
+                    const uint32_t k = (w[l] >> sh) & 3u;
+                    if (!k) continue;
+                    lp[l] += k;
+                    const uint32_t at = count[l] - lp[l];  // first (earliest-emitted) byte of this round
+                    if (k == 2) { out[op] = lb[l][at + 1]; out[op + 1] = lb[l][at]; op += 2; }
+                    else { out[op] = lb[l][at]; op += 1; }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace pz

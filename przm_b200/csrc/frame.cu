@@ -1,0 +1,216 @@
+// frame.cu -- section selection and PRZM frame assembly.
+//
+// Profile 0 is the CompressD2D frame (gpu/bridge.go:2287-2458 with
+// przm_write_frame_header_kernel, przm_ans.cu:497-539): flat 0x00 command and
+// offset sections, raw literals.
+// Profile 1 is the entropy-coded frame: Section 2 as PackageCommandsSection
+// (core/commands/commands.go:371-444, 537-568) when the command stream is at
+// most 2 MiB, Section 3 flat, Section 4 the adaptive V-ANS container
+// (core/literals/literals.go:368-384) when it beats the raw literals (or the
+// raw literals would be misread as a container), FlagNibble with a V-ANS
+// Section 4 (compress.go:990), and the uncompressed-frame fallback of
+// assembleContainer (compress.go:962-985).
+#include "common.cuh"
+
+namespace pz {
+
+__host__ __device__ inline uint32_t d2d_wlog(uint32_t n) { return n <= 65536 ? 16 : (n > 1048576 ? 23 : 20); }
+
+__device__ inline uint32_t tsum(const TaskOut& o) { return o.count[0] + o.count[1] + o.count[2] + o.count[3]; }
+
+__device__ inline uint32_t rd32b(const uint8_t* p) {
+    return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+}
+
+__global__ void k_plan(const Job* __restrict__ jobs, uint32_t njobs, const uint32_t* __restrict__ job_lens,
+                       const TableInfo* __restrict__ infos, const TaskOut* __restrict__ outs,
+                       const uint8_t* __restrict__ streams, Plan* __restrict__ plans, uint32_t* __restrict__ sizes) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    const Job job = jobs[j];
+    const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
+    Plan p = {};
+    const uint32_t n = job.n;
+    p.wlog = d2d_wlog(n);
+    if (n == 0) {  // empty input gives an empty result (gpu/bridge.go:2491-2493)
+        plans[j] = p;
+        sizes[j] = 0;
+        return;
+    }
+    if (job.profile == 0) {
+        p.l2 = lens[S_CMD] + 5;
+        p.l3 = lens[S_OFF] + 5;
+        p.l4 = lens[S_LIT];
+        const bool ext = n > 65535 || p.l2 > 65535 || p.l3 > 65535 || p.wlog > 16;
+        p.flags = ext ? 0x08 : 0;
+        p.frame_size = 8 + (ext ? 6 : 4) + 8 + p.l2 + p.l3 + p.l4;
+    } else {
+        const uint32_t cmd = lens[S_CMD];
+        p.s2_mode = 2;
+        p.l2 = 1 + cmd;
+        if (cmd <= (2u << 20)) {
+            uint32_t m8 = 13;
+            for (int sub = 0; sub < 3; sub++) {
+                const uint32_t len = lens[S_OP + sub];
+                uint32_t best = 1 + len, mode = 0;
+                const int tm = T_OP_M8 + 2 * sub, ta = tm + 1;
+                if (task_active(job, lens, tm)) {
+                    uint32_t sz = 24 + tsum(outs[(uint64_t)j * T_COUNT + tm]);
+                    if (sz < best) { best = sz; mode = 1; }
+                }
+                if (task_active(job, lens, ta)) {
+                    uint32_t sz = 8 + infos[(uint64_t)j * 4 + 1 + sub].mat_len + 16 + tsum(outs[(uint64_t)j * T_COUNT + ta]);
+                    if (sz < best) { best = sz; mode = 2; }
+                }
+                p.sub_len[sub] = best;
+                p.sub_mode[sub] = mode;
+                m8 += best;
+            }
+            if (m8 < cmd) { p.s2_mode = 1; p.l2 = m8; }
+        }
+        p.l3 = lens[S_OFF] + 5;
+        const uint32_t lit = lens[S_LIT];
+        p.l4 = lit;
+        bool fallback = false;
+        if (lit > 0) {
+            const uint8_t* lp = streams + job.str_off + stream_base(job, S_LIT);
+            bool raw_ok = true;
+            if (lit >= 8) {
+                if (lp[0] == 'V' && lp[1] == 'A' && lp[2] == 0x01) raw_ok = false;
+                else if (rd32b(lp + 4) == (uint32_t)(((uint64_t)rd32b(lp) + 1) / 2)) raw_ok = false;
+            }
+            bool vans = false;
+            uint32_t vsz = 0;
+            if (task_active(job, lens, T_LIT)) {
+                const uint32_t e = tsum(outs[(uint64_t)j * T_COUNT + T_LIT]);
+                if (e <= (8u << 20)) { vans = true; vsz = 8 + infos[(uint64_t)j * 4].mat_len + 16 + e; }
+            }
+            if (vans && (vsz < lit || !raw_ok)) { p.s4_mode = 1; p.l4 = vsz; }
+            else if (!raw_ok) fallback = true;
+        }
+        const bool ext = n > 65535 || p.l2 > 65535 || p.l3 > 65535 || p.wlog > 16;
+        p.flags = (p.s4_mode ? 0x80u : 0u) | (ext ? 0x08u : 0u);
+        const uint64_t comp = 8ull + (ext ? 6 : 4) + 8 + p.l2 + p.l3 + p.l4;
+        if (fallback || comp >= n) { p.uncompressed = 1; p.flags = 0x04; p.frame_size = 8 + n; }
+        else p.frame_size = (uint32_t)comp;
+    }
+    plans[j] = p;
+    sizes[j] = p.frame_size;
+}
+
+constexpr int kAsmThreads = 256;
+
+__device__ void block_copy(uint8_t* __restrict__ d, const uint8_t* __restrict__ s, uint32_t n) {
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) d[i] = s[i];
+}
+__device__ inline void put32(uint8_t* p, uint32_t v) {
+    p[0] = (uint8_t)v; p[1] = (uint8_t)(v >> 8); p[2] = (uint8_t)(v >> 16); p[3] = (uint8_t)(v >> 24);
+}
+
+// container: 'V','A',01,flags | LE32 n | [matrix] | 4 x LE32 state | stream
+__device__ uint32_t write_container(uint8_t* dst, uint8_t flags, uint32_t n, const TableInfo* info, const TaskOut& o,
+                                    const uint8_t* task_base, uint32_t cap) {
+    uint32_t h = 8 + (info ? info->mat_len : 0);
+    if (threadIdx.x == 0) {
+        dst[0] = 'V'; dst[1] = 'A'; dst[2] = 0x01; dst[3] = flags;
+        put32(dst + 4, n);
+        for (int k = 0; k < 4; k++) put32(dst + h + 4 * k, o.state[k]);
+    }
+    if (info) block_copy(dst + 8, info->mat, info->mat_len);
+    block_stitch<kAsmThreads>(task_base, cap, n, o.count, dst + h + 16);
+    return h + 16 + tsum(o);
+}
+
+__global__ void __launch_bounds__(kAsmThreads) k_assemble(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
+                                                          uint32_t njobs, const uint32_t* __restrict__ job_lens,
+                                                          const Plan* __restrict__ plans, const TableInfo* __restrict__ infos,
+                                                          const TaskOut* __restrict__ outs,
+                                                          const uint8_t* __restrict__ streams,
+                                                          const uint8_t* __restrict__ ans, uint8_t* __restrict__ out) {
+    for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
+        const Job job = jobs[j];
+        const Plan p = plans[j];
+        const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
+        uint8_t* f = out + job.out_off;
+        const uint32_t n = job.n;
+        __syncthreads();
+        if (n == 0) continue;
+        if (p.uncompressed) {
+            if (threadIdx.x == 0) {
+                f[0] = 'P'; f[1] = 'R'; f[2] = 'Z'; f[3] = 'M'; f[4] = 0x04;
+                f[5] = (uint8_t)n; f[6] = (uint8_t)(n >> 8); f[7] = (uint8_t)(n >> 16);
+            }
+            block_copy(f + 8, in + job.in_off, n);
+            continue;
+        }
+        const bool ext = (p.flags & 0x08) != 0;
+        uint32_t w = 8 + (ext ? 6 : 4);
+        if (threadIdx.x == 0) {
+            f[0] = 'P'; f[1] = 'R'; f[2] = 'Z'; f[3] = 'M'; f[4] = (uint8_t)p.flags;
+            f[5] = (uint8_t)n; f[6] = (uint8_t)(n >> 8); f[7] = (uint8_t)(n >> 16);
+            if (!ext) {
+                f[8] = (uint8_t)p.l2; f[9] = (uint8_t)(p.l2 >> 8);
+                f[10] = (uint8_t)p.l3; f[11] = (uint8_t)(p.l3 >> 8);
+            } else {
+                f[8] = (uint8_t)p.l2; f[9] = (uint8_t)(p.l2 >> 8); f[10] = (uint8_t)(p.l2 >> 16);
+                f[11] = (uint8_t)p.l3; f[12] = (uint8_t)(p.l3 >> 8); f[13] = (uint8_t)(p.l3 >> 16);
+            }
+            for (int k = 0; k < 8; k++) f[w + k] = 0;
+            f[w + 1] = (uint8_t)p.wlog;
+        }
+        w += 8;
+        const uint8_t* sreg = streams + job.str_off;
+        const uint8_t* abase = ans + job.ans_off;
+        // Section 2
+        uint8_t* s2 = f + w;
+        if (job.profile == 0) {
+            if (threadIdx.x == 0) { s2[0] = 0x00; put32(s2 + 1, lens[S_CMD]); }
+            block_copy(s2 + 5, sreg + stream_base(job, S_CMD), lens[S_CMD]);
+        } else if (p.s2_mode == 2) {
+            if (threadIdx.x == 0) s2[0] = 0x09;
+            block_copy(s2 + 1, sreg + stream_base(job, S_CMD), lens[S_CMD]);
+        } else {
+            if (threadIdx.x == 0) {
+                s2[0] = 0x08;
+                put32(s2 + 1, lens[S_CMD]);
+                put32(s2 + 5, p.sub_len[0]);
+                put32(s2 + 9, p.sub_len[1]);
+            }
+            uint32_t o = 13;
+            for (int sub = 0; sub < 3; sub++) {
+                const uint32_t len = lens[S_OP + sub];
+                uint8_t* d = s2 + o;
+                if (p.sub_mode[sub] == 0) {
+                    if (threadIdx.x == 0) d[0] = 0x09;
+                    block_copy(d + 1, sreg + stream_base(job, S_OP + sub), len);
+                } else {
+                    const int t = T_OP_M8 + 2 * sub + (p.sub_mode[sub] == 2 ? 1 : 0);
+                    const TaskOut to = outs[(uint64_t)j * T_COUNT + t];
+                    if (p.sub_mode[sub] == 1)
+                        write_container(d, 0x41, len, nullptr, to, abase + ans_task_off(job, t), task_cap(job, t));
+                    else
+                        write_container(d, 0x00, len, infos + (uint64_t)j * 4 + 1 + sub, to, abase + ans_task_off(job, t),
+                                        task_cap(job, t));
+                }
+                o += p.sub_len[sub];
+            }
+        }
+        w += p.l2;
+        // Section 3 (flat)
+        uint8_t* s3 = f + w;
+        if (threadIdx.x == 0) { s3[0] = 0x00; put32(s3 + 1, lens[S_OFF]); }
+        block_copy(s3 + 5, sreg + stream_base(job, S_OFF), lens[S_OFF]);
+        w += p.l3;
+        // Section 4
+        uint8_t* s4 = f + w;
+        if (p.s4_mode == 1) {
+            const TaskOut to = outs[(uint64_t)j * T_COUNT + T_LIT];
+            write_container(s4, 0x00, lens[S_LIT], infos + (uint64_t)j * 4, to, abase + ans_task_off(job, T_LIT),
+                            task_cap(job, T_LIT));
+        } else {
+            block_copy(s4, sreg + stream_base(job, S_LIT), lens[S_LIT]);
+        }
+    }
+}
+
+}  // namespace pz
