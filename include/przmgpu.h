@@ -170,6 +170,13 @@ int32_t przmg_compress(przmg_ctx* ctx, const uint8_t* src, uint64_t n, int32_t p
 int32_t przmg_compress_batch(przmg_ctx* ctx, przmg_job_t* jobs, uint64_t njobs, int32_t profile, int32_t batched,
                              przmg_profile_t* prof);
 
+/* Many inputs laid back to back in host memory (pinned for full speed):
+ * frames come back back to back in host_out; out_sizes (optional, njobs)
+ * receives each frame's size.  No reference counterpart. */
+int32_t przmg_compress_packed(przmg_ctx* ctx, const uint8_t* host_in, const uint64_t* sizes, uint64_t njobs,
+                              int32_t profile, uint8_t* host_out, uint64_t out_cap, uint32_t* out_sizes,
+                              uint64_t* out_total);
+
 /* Device-resident batches (inputs already in HBM; used for throughput runs). */
 int32_t przmg_batch_create(przmg_ctx* ctx, const uint64_t* sizes, uint64_t njobs, int32_t profile,
                            przmg_batch** out);
@@ -184,6 +191,20 @@ int32_t przmg_batch_enqueue(przmg_batch* b, uint64_t stream, int32_t use_graph);
 int32_t przmg_batch_sizes(przmg_batch* b, uint32_t* sizes);
 /* kernels a single enqueue launches (for launch accounting) */
 int32_t przmg_batch_launch_count(przmg_batch* b);
+/* copy back-to-back host inputs (sum of the sizes, pinned for full PCIe
+ * speed) into the batch's inputs, asynchronously on `stream` */
+int32_t przmg_batch_upload(przmg_batch* b, const uint8_t* host, uint64_t stream);
+/* synchronise, then copy the frames back to back into host (capacity cap);
+ * total = bytes written, sizes (optional) = per-frame sizes */
+int32_t przmg_batch_download(przmg_batch* b, uint8_t* host, uint64_t cap, uint64_t* total, uint32_t* sizes,
+                             uint64_t stream);
+/* one enqueue with CUDA events between the stages; ms[k] = device time of
+ * stage k (names from przmg_stage_name), count = stages reported */
+int32_t przmg_batch_stage_times(przmg_batch* b, float* ms, int32_t cap, int32_t* count);
+const char* przmg_stage_name(int32_t k);
+/* totals of the last run (synchronises): input, frame, literal, command and
+ * offset bytes, rANS symbols and emitted bytes, uncompressed frames */
+int32_t przmg_batch_stats(przmg_batch* b, uint64_t stats[8]);
 int32_t przmg_batch_destroy(przmg_batch* b);
 
 /* ---- histogram / flat pack / V-ANS ------------------------------------- */

@@ -111,7 +111,7 @@ struct przmg_batch {
     std::vector<uint64_t> in_offs, out_offs;
     uint64_t in_bytes = 0, desc_words = 0, stream_bytes = 0, ans_bytes = 0, out_bytes = 0;
     DevBuf d_in, d_jobs, d_small, d_big, d_tiles, d_desc, d_slots, d_tile_lens, d_streams, d_job_lens, d_hist, d_tabs,
-        d_infos, d_ans, d_outs, d_plans, d_sizes, d_out, d_misc;
+        d_infos, d_ans, d_outs, d_plans, d_sizes, d_out, d_misc, d_lists;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int launches = 0;
@@ -124,7 +124,8 @@ struct przmg_batch {
     }
     void release() {
         DevBuf* all[] = {&d_in, &d_jobs, &d_small, &d_big, &d_tiles, &d_desc, &d_slots, &d_tile_lens, &d_streams,
-                         &d_job_lens, &d_hist, &d_tabs, &d_infos, &d_ans, &d_outs, &d_plans, &d_sizes, &d_out, &d_misc};
+                         &d_job_lens, &d_hist, &d_tabs, &d_infos, &d_ans, &d_outs, &d_plans, &d_sizes, &d_out, &d_misc,
+                         &d_lists};
         for (DevBuf* b : all) b->release();
     }
     uint32_t* err_word() const { return d_misc.as<uint32_t>(); }
@@ -231,6 +232,7 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     CK(b->d_sizes.ensure((size_t)njobs * 4 + 16));
     CK(b->d_out.ensure(b->out_bytes));
     CK(b->d_misc.ensure(64));
+    CK(b->d_lists.ensure((size_t)2 * 4 * std::max<uint32_t>(njobs, 1) * 4 + 64));
     cudaStream_t s = b->ctx->stream;
     CK(cudaMemcpyAsync(b->d_jobs.p, b->jobs.data(), sizeof(Job) * njobs, cudaMemcpyHostToDevice, s));
     if (b->nsmall) CK(cudaMemcpyAsync(b->d_small.p, b->small.data(), sizeof(TileRef) * b->nsmall, cudaMemcpyHostToDevice, s));
@@ -250,10 +252,18 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
 
 // Stages of one enqueue.  stop_after: 0 match only, 1 through tokenize +
 // gather, 2 the full frame pipeline.
-static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after) {
+static const char* const kStageNames[] = {"tile_find", "radix_find", "tokenize", "gather",
+                                          "normalize", "rans", "plan", "assemble"};
+constexpr int kStages = 8;
+
+// ev (optional): kStages + 1 events; ev[0] before the first kernel and
+// ev[k + 1] after stage k (stages that do not run record back to back).
+static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cudaEvent_t* ev = nullptr) {
     Ctx* c = b->ctx;
     int launches = 0;
     CK(cudaMemsetAsync(b->d_misc.p, 0, 16, s));
+    auto mark = [&](int k) -> cudaError_t { return ev ? cudaEventRecord(ev[k], s) : cudaSuccess; };
+    CK(mark(0));
     if (b->nsmall) {
         const uint32_t grid = std::min<uint32_t>(b->nsmall, 8u * c->sms);
         k_tile_find<<<grid, 256, kTileFindSmem, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_small.as<TileRef>(),
@@ -261,6 +271,7 @@ static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after) {
         CK(cudaGetLastError());
         launches++;
     }
+    CK(mark(1));
     if (b->nbig) {
         const uint32_t grid = std::min<uint32_t>(b->nbig, c->radix_ctas);
         k_radix_find<<<grid, kRadixThreads, kRadixSmem, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(),
@@ -270,12 +281,14 @@ static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after) {
         CK(cudaGetLastError());
         launches++;
     }
+    CK(mark(2));
     if (stop_after >= 1 && !b->tiles.empty()) {
         const uint32_t nt = (uint32_t)b->tiles.size();
         k_tokenize<<<(nt + 7) / 8, 256, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_tiles.as<TokTile>(), nt,
                                                b->d_desc.as<uint32_t>(), b->d_slots.as<uint8_t>(),
                                                b->d_tile_lens.as<uint32_t>(), b->err_word());
         CK(cudaGetLastError());
+        CK(mark(3));
         uint32_t maxtiles = 1;
         for (const Job& j : b->jobs) maxtiles = std::max(maxtiles, j.ntiles);
         k_gather<<<std::min<uint32_t>(b->njobs, 16u * c->sms), kGatherThreads, (maxtiles + 1) * 4, s>>>(
@@ -283,31 +296,50 @@ static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after) {
             b->d_streams.as<uint8_t>(), b->d_job_lens.as<uint32_t>(), b->d_hist.as<uint32_t>(), b->err_word());
         CK(cudaGetLastError());
         launches += 2;
+    } else {
+        CK(mark(3));
     }
+    CK(mark(4));
     if (stop_after >= 2) {
         if (b->profile == 1) {
             k_normalize<<<b->njobs, 128, 0, s>>>(b->d_jobs.as<Job>(), b->njobs, b->d_job_lens.as<uint32_t>(),
                                                  b->d_hist.as<uint32_t>(), b->d_tabs.as<EncSym>(), b->d_infos.as<TableInfo>());
             CK(cudaGetLastError());
-            const uint32_t threads = b->njobs * T_COUNT * 4;
-            k_rans<<<(threads + 127) / 128, 128, 0, s>>>(b->d_jobs.as<Job>(), b->njobs, b->d_job_lens.as<uint32_t>(),
-                                                        b->d_streams.as<uint8_t>(), b->d_ans.as<uint8_t>(),
-                                                        b->d_tabs.as<EncSym>(), c->d_meta8.as<EncSym>(),
-                                                        c->d_ctxlut.as<uint8_t>(), b->d_outs.as<TaskOut>());
+            CK(mark(5));
+            const uint32_t list_cap = 4 * b->njobs;
+            uint32_t* lists = b->d_lists.as<uint32_t>();
+            uint32_t* counts = lists + 2 * list_cap;
+            k_task_list<<<1, 1024, 0, s>>>(b->d_jobs.as<Job>(), b->njobs, b->d_job_lens.as<uint32_t>(), lists, list_cap,
+                                           counts);
             CK(cudaGetLastError());
-            launches += 2;
+            const uint32_t nb_ad = (4 * b->njobs + 8 * kRansWarps - 1) / (8 * kRansWarps);
+            const uint32_t nb_m8 = (3 * b->njobs + 8 * kRansWarps - 1) / (8 * kRansWarps);
+            k_rans<<<nb_ad + nb_m8, kRansWarps * 32, kRansSmem, s>>>(
+                b->d_jobs.as<Job>(), b->d_job_lens.as<uint32_t>(), b->d_streams.as<uint8_t>(), b->d_ans.as<uint8_t>(),
+                b->d_tabs.as<EncSym>(), c->d_meta8.as<EncSym>(), c->d_ctxlut.as<uint8_t>(), lists, list_cap, counts, nb_ad,
+                b->d_outs.as<TaskOut>());
+            CK(cudaGetLastError());
+            launches += 3;
+            CK(mark(6));
+        } else {
+            CK(mark(5));
+            CK(mark(6));
         }
         k_plan<<<(b->njobs + 127) / 128, 128, 0, s>>>(b->d_jobs.as<Job>(), b->njobs, b->d_job_lens.as<uint32_t>(),
                                                       b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(),
                                                       b->d_streams.as<uint8_t>(), b->d_plans.as<Plan>(),
                                                       b->d_sizes.as<uint32_t>());
         CK(cudaGetLastError());
+        CK(mark(7));
         k_assemble<<<std::min<uint32_t>(b->njobs, 16u * c->sms), kAsmThreads, 0, s>>>(
             b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->njobs, b->d_job_lens.as<uint32_t>(), b->d_plans.as<Plan>(),
             b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(), b->d_streams.as<uint8_t>(), b->d_ans.as<uint8_t>(),
             b->d_out.as<uint8_t>());
         CK(cudaGetLastError());
         launches += 2;
+        CK(mark(8));
+    } else {
+        for (int k = 5; k <= 8; k++) CK(mark(k));
     }
     b->launches = launches;
     return PRZMG_OK;
@@ -347,6 +379,8 @@ static int32_t ctx_setup(Ctx* c) {
     for (auto& e : c->ev) CK(cudaEventCreate(&e));
     CK(cudaFuncSetAttribute(k_tile_find, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileFindSmem));
     CK(cudaFuncSetAttribute(k_radix_find, cudaFuncAttributeMaxDynamicSharedMemorySize, kRadixSmem));
+    CK(cudaFuncSetAttribute(k_rans, cudaFuncAttributeMaxDynamicSharedMemorySize, kRansSmem));
+    CK(cudaFuncSetAttribute(k_stream_rans, cudaFuncAttributeMaxDynamicSharedMemorySize, kRansSmem));
     CK(c->d_meta8.ensure(8 * 256 * sizeof(EncSym)));
     CK(c->d_ctxlut.ensure(256));
     {
@@ -883,6 +917,176 @@ extern "C" int32_t przmg_batch_sizes(przmg_batch* b, uint32_t* sizes) {
 }
 
 extern "C" int32_t przmg_batch_launch_count(przmg_batch* b) { return b ? b->launches : 0; }
+
+// Scatter of back-to-back inputs into the padded per-frame layout, and the
+// inverse gather of the frames into back-to-back output.
+__global__ void k_scatter_inputs(const uint8_t* __restrict__ packed, const uint64_t* __restrict__ src_off,
+                                 const Job* __restrict__ jobs, uint32_t njobs, uint8_t* __restrict__ in) {
+    for (uint32_t j = blockIdx.y; j < njobs; j += gridDim.y) {
+        const uint8_t* s = packed + src_off[j];
+        uint8_t* d = in + jobs[j].in_off;
+        const uint32_t n = jobs[j].n;
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d[i] = s[i];
+    }
+}
+
+__global__ void k_gather_frames(const uint8_t* __restrict__ out, const Job* __restrict__ jobs,
+                                const uint32_t* __restrict__ sizes, const uint64_t* __restrict__ dst_off, uint32_t njobs,
+                                uint8_t* __restrict__ packed) {
+    for (uint32_t j = blockIdx.y; j < njobs; j += gridDim.y) {
+        const uint8_t* s = out + jobs[j].out_off;
+        uint8_t* d = packed + dst_off[j];
+        const uint32_t n = sizes[j];
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d[i] = s[i];
+    }
+}
+
+static int32_t batch_upload_packed(przmg_batch* b, const uint8_t* host, cudaStream_t s) {
+    Ctx* c = b->ctx;
+    uint64_t total = 0;
+    std::vector<uint64_t> offs(b->njobs);
+    for (uint32_t i = 0; i < b->njobs; i++) { offs[i] = total; total += b->jobs[i].n; }
+    CK(c->d_scr_in.ensure(total + 64));
+    CK(c->d_scr_aux.ensure(8ull * b->njobs + 64));
+    CK(c->h_aux.ensure(8ull * b->njobs + 64));
+    std::memcpy(c->h_aux.p, offs.data(), 8ull * b->njobs);
+    if (total) CK(cudaMemcpyAsync(c->d_scr_in.p, host, total, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(c->d_scr_aux.p, c->h_aux.p, 8ull * b->njobs, cudaMemcpyHostToDevice, s));
+    if (b->njobs) {
+        k_scatter_inputs<<<dim3(64, std::min<uint32_t>(b->njobs, 4096)), 256, 0, s>>>(
+            c->d_scr_in.as<uint8_t>(), c->d_scr_aux.as<uint64_t>(), b->d_jobs.as<Job>(), b->njobs, b->d_in.as<uint8_t>());
+        CK(cudaGetLastError());
+    }
+    return PRZMG_OK;
+}
+
+static int32_t batch_download_packed(przmg_batch* b, uint8_t* host, uint64_t cap, uint64_t* total, uint32_t* sizes,
+                                     cudaStream_t s) {
+    Ctx* c = b->ctx;
+    std::vector<uint32_t> fs(b->njobs);
+    if (b->njobs) CK(cudaMemcpyAsync(fs.data(), b->d_sizes.p, 4ull * b->njobs, cudaMemcpyDeviceToHost, s));
+    uint32_t err = 0;
+    CK(cudaMemcpyAsync(&err, b->err_word(), 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (err) return fail(PRZMG_ERR_DEVICE, "device bound violation, error bits " + std::to_string(err));
+    std::vector<uint64_t> offs(b->njobs);
+    uint64_t t = 0;
+    for (uint32_t i = 0; i < b->njobs; i++) { offs[i] = t; t += fs[i]; }
+    if (sizes) std::copy(fs.begin(), fs.end(), sizes);
+    *total = t;
+    if (t > cap) return fail(PRZMG_ERR_BUFFER_TOO_SMALL, "output buffer too small for the frames");
+    CK(c->d_scr_out.ensure(t + 64));
+    CK(c->d_scr_aux.ensure(8ull * b->njobs + 64));
+    CK(c->h_aux.ensure(8ull * b->njobs + 64));
+    std::memcpy(c->h_aux.p, offs.data(), 8ull * b->njobs);
+    CK(cudaMemcpyAsync(c->d_scr_aux.p, c->h_aux.p, 8ull * b->njobs, cudaMemcpyHostToDevice, s));
+    if (b->njobs) {
+        k_gather_frames<<<dim3(64, std::min<uint32_t>(b->njobs, 4096)), 256, 0, s>>>(
+            b->d_out.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_sizes.as<uint32_t>(), c->d_scr_aux.as<uint64_t>(), b->njobs,
+            c->d_scr_out.as<uint8_t>());
+        CK(cudaGetLastError());
+    }
+    if (t) CK(cudaMemcpyAsync(host, c->d_scr_out.p, t, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_batch_upload(przmg_batch* b, const uint8_t* host, uint64_t stream) {
+    if (!b || (!host && b->njobs)) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    Ctx* c = b->ctx;
+    LOCKED(c);
+    return batch_upload_packed(b, host, stream ? (cudaStream_t)(uintptr_t)stream : c->stream);
+}
+
+extern "C" int32_t przmg_batch_download(przmg_batch* b, uint8_t* host, uint64_t cap, uint64_t* total, uint32_t* sizes,
+                                        uint64_t stream) {
+    if (!b || !total) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    Ctx* c = b->ctx;
+    LOCKED(c);
+    return batch_download_packed(b, host, cap, total, sizes, stream ? (cudaStream_t)(uintptr_t)stream : c->stream);
+}
+
+extern "C" int32_t przmg_batch_stage_times(przmg_batch* b, float* ms, int32_t cap, int32_t* count) {
+    if (!b || !ms || !count) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    Ctx* c = b->ctx;
+    LOCKED(c);
+    cudaEvent_t ev[kStages + 1];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    int32_t r = batch_launch(b, c->stream, 2, ev);
+    if (r == 0) {
+        cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) r = cuda_fail("cudaStreamSynchronize", e);
+    }
+    const int n = std::min<int>(cap, kStages);
+    for (int k = 0; k < n && r == 0; k++) ms[k] = ev_ms(ev[k], ev[k + 1]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    *count = n;
+    return r;
+}
+
+// Totals of the last run of a batch (synchronises):
+//   [0] input bytes   [1] frame bytes   [2] literal bytes   [3] command bytes
+//   [4] offset bytes  [5] rANS symbols of the active tasks
+//   [6] bytes the rANS lanes emitted   [7] frames stored uncompressed
+extern "C" int32_t przmg_batch_stats(przmg_batch* b, uint64_t stats[8]) {
+    if (!b || !stats) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    Ctx* c = b->ctx;
+    LOCKED(c);
+    for (int k = 0; k < 8; k++) stats[k] = 0;
+    const uint32_t nj = b->njobs;
+    std::vector<uint32_t> lens((size_t)nj * S_COUNT + 1), sizes(nj + 1);
+    std::vector<TaskOut> outs((size_t)nj * T_COUNT + 1);
+    std::vector<Plan> plans(nj + 1);
+    if (nj) {
+        CK(cudaMemcpyAsync(lens.data(), b->d_job_lens.p, 4ull * nj * S_COUNT, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(sizes.data(), b->d_sizes.p, 4ull * nj, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(plans.data(), b->d_plans.p, sizeof(Plan) * nj, cudaMemcpyDeviceToHost, c->stream));
+        if (b->profile == 1)
+            CK(cudaMemcpyAsync(outs.data(), b->d_outs.p, sizeof(TaskOut) * nj * T_COUNT, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    for (uint32_t j = 0; j < nj; j++) {
+        const uint32_t* l = &lens[(size_t)j * S_COUNT];
+        stats[0] += b->jobs[j].n;
+        stats[1] += sizes[j];
+        stats[2] += l[S_LIT];
+        stats[3] += l[S_CMD];
+        stats[4] += l[S_OFF];
+        stats[7] += plans[j].uncompressed;
+        if (b->profile != 1) continue;
+        for (int t = 0; t < T_COUNT; t++) {
+            if (!task_active(b->jobs[j], l, t)) continue;
+            stats[5] += task_len(l, t);
+            const TaskOut& o = outs[(size_t)j * T_COUNT + t];
+            stats[6] += (uint64_t)o.count[0] + o.count[1] + o.count[2] + o.count[3];
+        }
+    }
+    return PRZMG_OK;
+}
+
+extern "C" const char* przmg_stage_name(int32_t k) { return (k >= 0 && k < kStages) ? kStageNames[k] : ""; }
+
+extern "C" int32_t przmg_compress_packed(przmg_ctx* h, const uint8_t* host_in, const uint64_t* sizes, uint64_t njobs,
+                                         int32_t profile, uint8_t* host_out, uint64_t out_cap, uint32_t* out_sizes,
+                                         uint64_t* out_total) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c || !sizes || !out_total || (njobs && (!host_in || !host_out))) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    if (profile != PRZMG_PROFILE_D2D && profile != PRZMG_PROFILE_ANS) return fail(PRZMG_ERR_INVALID_ARG, "unknown profile");
+    for (uint64_t i = 0; i < njobs; i++)
+        if (profile == PRZMG_PROFILE_ANS && sizes[i] >= (1u << 24))
+            return fail(PRZMG_ERR_EXCEEDS_MAX_BLOCK, "the frame header holds 24-bit sizes: inputs must be < 16 MiB");
+    if (int32_t m = mock_check()) return m;
+    LOCKED(c);
+    przmg_batch* b = &c->single;
+    int32_t r = batch_prepare(b, sizes, (uint32_t)njobs, profile, false);
+    if (r) return r;
+    r = batch_upload_packed(b, host_in, c->stream);
+    if (r) return r;
+    r = batch_launch(b, c->stream, 2);
+    if (r) return r;
+    return batch_download_packed(b, host_out, out_cap, out_total, out_sizes, c->stream);
+}
+
 
 extern "C" int32_t przmg_batch_destroy(przmg_batch* b) {
     if (!b) return PRZMG_OK;

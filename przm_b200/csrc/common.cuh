@@ -73,11 +73,13 @@ __host__ __device__ inline uint64_t stream_region_bytes(const Job& j) {
 
 // ANS scratch of one task: four lane byte streams then four lane count
 // words (2 bits per round).  L = symbol capacity of the task's stream.
-__host__ __device__ inline uint64_t ans_lane_cap(uint32_t L) { return 2ull * ((L + 3) / 4) + 16; }
+// lane streams are written in 64-byte chunks (64-byte aligned), so every lane
+// region is a multiple of 64 with room for the last partial chunk
+__host__ __device__ inline uint64_t ans_lane_cap(uint32_t L) { return ((2ull * ((L + 3) / 4) + 128) + 63) & ~63ull; }
 __host__ __device__ inline uint64_t ans_nbw_cap(uint32_t L) { return (((L + 3) / 4) + 15) / 16 + 1; }  // u32 words
 __host__ __device__ inline uint64_t ans_task_bytes(uint32_t L) {
     uint64_t b = 4 * ans_lane_cap(L) + 4 * 4 * ans_nbw_cap(L);
-    return (b + 15) & ~15ull;
+    return (b + 63) & ~63ull;
 }
 __host__ __device__ inline uint32_t task_cap(const Job& j, int t) { return t == T_LIT ? j.lit_cap : j.cmd_cap; }
 __host__ __device__ inline uint64_t ans_task_off(const Job& j, int t) {

@@ -338,28 +338,98 @@ __device__ __forceinline__ LaneIO lane_io(uint8_t* task_base, uint32_t cap, uint
     return io;
 }
 
+// One rANS step (table entry e of the symbol already in registers): returns
+// the number k of low bytes of x the reference would emit (x >= 4096 f, and
+// again when x >> 8 >= 4096 f), and advances x.  The caller keeps the low
+// 16 bits of x from before the step; its first k bytes (low byte first) are
+// what the reference writes.
+__device__ __forceinline__ uint32_t rans_step(uint32_t& x, const EncSym& e) {
+    const uint32_t x8 = x >> 8, x16 = x >> 16;
+    const bool p1 = x >= e.t1, p2 = x8 >= e.t1;
+    const uint32_t xr = p2 ? x16 : (p1 ? x8 : x);
+    const uint32_t q = __umulhi(xr, e.m) >> (e.cfs >> 16);
+    x = xr + q * (e.cfs & 0xFFFFu) + e.cb;
+    return (uint32_t)p1 + (uint32_t)p2;
+}
+
+// Encodes lane l of one task.  Symbols of lane l are i = 4j + l, rounds j
+// from the top down.  Per round the lane stores the 16 low bits of x before
+// the step at raw[j] and the byte count k in 2 bits of nbw[j / 16]; the
+// stitch turns (raw, k) back into the reference byte order.  Rounds come in
+// groups of 16 (64 source bytes holding the four lanes' symbols); the top,
+// partial group takes the byte path, full groups are loaded one group ahead
+// and their 16 table entries are fetched before the dependent chain runs.
 template <bool kMeta8>
 __device__ __forceinline__ void rans_lane(const uint8_t* __restrict__ src, uint32_t n, uint32_t l,
                                           const EncSym* __restrict__ tab, const uint8_t* __restrict__ ctxlut,
                                           LaneIO io, uint32_t* out_state, uint32_t* out_count) {
-    uint32_t x = 65536, cnt = 0, acc = 0;
+    uint32_t x = 65536, cnt = 0;
+    uint16_t* raw = reinterpret_cast<uint16_t*>(io.bytes);
     if (n > l) {
-        const int32_t J = (int32_t)((n - 1 - l) >> 2);
-        for (int32_t j = J; j >= 0; j--) {
-            const uint32_t i = 4u * (uint32_t)j + l;
-            const uint32_t s = src[i];
-            uint32_t ti = s;
-            if (kMeta8) ti |= (i ? (uint32_t)ctxlut[src[i - 1]] : 0u) << 8;
-            const EncSym e = tab[ti];
-            const uint32_t k = (x >= e.t1 ? 1u : 0u) + ((x >> 8) >= e.t1 ? 1u : 0u);
-            io.bytes[cnt] = (uint8_t)x;
-            io.bytes[cnt + 1] = (uint8_t)(x >> 8);
-            cnt += k;
-            const uint32_t xr = x >> (8 * k);
-            const uint32_t q = __umulhi(xr, e.m) >> (e.cfs >> 16);
-            x = xr + q * (e.cfs & 0xFFFFu) + e.cb;
-            acc |= k << (2 * (j & 15));
-            if ((j & 15) == 0) { io.nbw[j >> 4] = acc; acc = 0; }
+        const uint32_t J = (n - 1 - l) >> 2;
+        const bool vec = (reinterpret_cast<uintptr_t>(src) & 15) == 0;
+        const uint32_t G = vec ? (J >> 4) : 0;
+        {
+            uint32_t acc = 0;
+            for (int32_t j = (int32_t)J; j >= (int32_t)(16 * G); j--) {
+                const uint32_t i = 4u * (uint32_t)j + l;
+                uint32_t ti = src[i];
+                if (kMeta8) ti |= (i ? (uint32_t)ctxlut[src[i - 1]] : 0u) << 8;
+                raw[j] = (uint16_t)x;
+                const uint32_t k = rans_step(x, tab[ti]);
+                cnt += k;
+                acc |= k << (2 * (j & 15));
+                if ((j & 15) == 0) {
+                    io.nbw[j >> 4] = acc;
+                    acc = 0;
+                }
+            }
+        }
+        if (G > 0) {
+            const uint4* s4 = reinterpret_cast<const uint4*>(src);
+            uint4* r4 = reinterpret_cast<uint4*>(raw);
+            const uint32_t sel = 0x4440u | l;        // __byte_perm selector of byte l
+            const uint32_t selp = 0x4440u | (l - 1);  // byte l-1 (l >= 1)
+            uint4 cur[4], nxt[4];
+#pragma unroll
+            for (int v = 0; v < 4; v++) cur[v] = __ldg(s4 + 4 * (G - 1) + v);
+            for (int32_t g = (int32_t)G - 1; g >= 0; g--) {
+                if (g > 0) {
+#pragma unroll
+                    for (int v = 0; v < 4; v++) nxt[v] = __ldg(s4 + 4 * (g - 1) + v);
+                }
+                const uint32_t w[16] = {cur[0].x, cur[0].y, cur[0].z, cur[0].w, cur[1].x, cur[1].y, cur[1].z, cur[1].w,
+                                        cur[2].x, cur[2].y, cur[2].z, cur[2].w, cur[3].x, cur[3].y, cur[3].z, cur[3].w};
+                EncSym e[16];
+#pragma unroll
+                for (int r = 0; r < 16; r++) {
+                    uint32_t ti = __byte_perm(w[r], 0, sel);
+                    if (kMeta8) {
+                        uint32_t prev;
+                        if (l > 0) prev = __byte_perm(w[r], 0, selp);
+                        else prev = r > 0 ? (w[r - 1] >> 24) : ((g > 0 ? nxt[3].w : 0u) >> 24);
+                        const bool first = (g == 0 && r == 0 && l == 0);
+                        ti |= (first ? 0u : (uint32_t)ctxlut[prev]) << 8;
+                    }
+                    e[r] = tab[ti];
+                }
+                uint32_t rec[16], acc = 0, kk = 0;
+#pragma unroll
+                for (int r = 15; r >= 0; r--) {
+                    rec[r] = x & 0xFFFFu;
+                    const uint32_t k = rans_step(x, e[r]);
+                    kk += k;
+                    acc |= k << (2 * r);
+                }
+                io.nbw[g] = acc;
+                cnt += kk;
+                r4[2 * g] = make_uint4(rec[0] | (rec[1] << 16), rec[2] | (rec[3] << 16), rec[4] | (rec[5] << 16),
+                                       rec[6] | (rec[7] << 16));
+                r4[2 * g + 1] = make_uint4(rec[8] | (rec[9] << 16), rec[10] | (rec[11] << 16),
+                                           rec[12] | (rec[13] << 16), rec[14] | (rec[15] << 16));
+#pragma unroll
+                for (int v = 0; v < 4; v++) cur[v] = nxt[v];
+            }
         }
     }
     *out_state = x;
@@ -395,41 +465,118 @@ __host__ __device__ inline bool task_active(const Job& job, const uint32_t* lens
     return n <= (2u << 20) && n >= (m8 ? 24u : 16u);
 }
 
-__global__ void __launch_bounds__(128) k_rans(const Job* __restrict__ jobs, uint32_t njobs,
-                                              const uint32_t* __restrict__ job_lens,
-                                              const uint8_t* __restrict__ streams, uint8_t* __restrict__ ans,
-                                              const EncSym* __restrict__ tabs, const EncSym* __restrict__ meta8,
-                                              const uint8_t* __restrict__ ctxlut, TaskOut* __restrict__ outs) {
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t task = g >> 2, l = g & 3;
-    if (task >= njobs * T_COUNT) return;
-    const uint32_t j = task / T_COUNT;
-    const int t = (int)(task % T_COUNT);
+// Task list: every active (frame, task) pair, split by model kind and
+// ordered longest-first (by the bit length of the symbol count) so that the
+// 8 tasks sharing a warp have similar lengths and the long chains start
+// first.  Entry = frame << 3 | task.  One block.
+__global__ void __launch_bounds__(1024) k_task_list(const Job* __restrict__ jobs, uint32_t njobs,
+                                                    const uint32_t* __restrict__ job_lens, uint32_t* __restrict__ lists,
+                                                    uint32_t list_cap, uint32_t* __restrict__ counts) {
+    __shared__ uint32_t s_cnt[2][33];
+    __shared__ uint32_t s_pos[2][33];
+    const uint32_t tid = threadIdx.x;
+    if (tid < 66) (&s_cnt[0][0])[tid] = 0;
+    __syncthreads();
+    const uint32_t total = njobs * T_COUNT;
+    for (uint32_t e = tid; e < total; e += blockDim.x) {
+        const uint32_t j = e / T_COUNT;
+        const int t = (int)(e % T_COUNT);
+        const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
+        const Job job = jobs[j];
+        if (!task_active(job, lens, t)) continue;
+        const uint32_t kind = (t != T_LIT && (t & 1)) ? 1u : 0u;
+        atomicAdd(&s_cnt[kind][32 - __clz(task_len(lens, t))], 1u);
+    }
+    __syncthreads();
+    if (tid < 2) {
+        uint32_t a = 0;
+        for (int b = 32; b >= 0; b--) { s_pos[tid][b] = a; a += s_cnt[tid][b]; }
+        counts[tid] = a;
+    }
+    __syncthreads();
+    for (uint32_t e = tid; e < total; e += blockDim.x) {
+        const uint32_t j = e / T_COUNT;
+        const int t = (int)(e % T_COUNT);
+        const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
+        const Job job = jobs[j];
+        if (!task_active(job, lens, t)) continue;
+        const uint32_t kind = (t != T_LIT && (t & 1)) ? 1u : 0u;
+        const uint32_t p = atomicAdd(&s_pos[kind][32 - __clz(task_len(lens, t))], 1u);
+        lists[kind * list_cap + p] = (j << 3) | (uint32_t)t;
+    }
+}
+
+constexpr int kRansWarps = 4;
+constexpr uint32_t kRansTabBytes = 8 * 256 * sizeof(EncSym);          // 8 models per warp (32 KiB)
+constexpr uint32_t kRansSmem = kRansWarps * kRansTabBytes;              // per-warp tables
+
+// Blocks [0, nb_ad) run adaptive-model tasks, the rest Meta8 tasks; each
+// warp takes 8 consecutive tasks of its list (4 lanes per task).
+__global__ void __launch_bounds__(kRansWarps * 32) k_rans(const Job* __restrict__ jobs,
+                                                          const uint32_t* __restrict__ job_lens,
+                                                          const uint8_t* __restrict__ streams, uint8_t* __restrict__ ans,
+                                                          const EncSym* __restrict__ tabs,
+                                                          const EncSym* __restrict__ meta8,
+                                                          const uint8_t* __restrict__ ctxlut,
+                                                          const uint32_t* __restrict__ lists, uint32_t list_cap,
+                                                          const uint32_t* __restrict__ counts, uint32_t nb_ad,
+                                                          TaskOut* __restrict__ outs) {
+    extern __shared__ __align__(16) uint8_t smem_r[];
+    __shared__ uint8_t s_lut[256];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool m8 = blockIdx.x >= nb_ad;
+    const uint32_t nlist = counts[m8 ? 1 : 0];
+    const uint32_t wg = (m8 ? blockIdx.x - nb_ad : blockIdx.x) * kRansWarps + warp;  // warp index in its list
+    EncSym* wtab = reinterpret_cast<EncSym*>(smem_r + warp * kRansTabBytes);
+    if (m8) {
+        // the block shares the 8 static models; every warp holds a copy
+        for (uint32_t i = lane; i < 8 * 256; i += 32) wtab[i] = meta8[i];
+        if (warp == 0) for (uint32_t i = lane; i < 256; i += 32) s_lut[i] = ctxlut[i];
+    }
+    const uint32_t slot = lane >> 2, l = lane & 3;
+    const uint32_t ti = wg * 8 + slot;
+    const bool have = ti < nlist;
+    uint32_t j = 0;
+    int t = 0;
+    if (have) {
+        const uint32_t e = lists[(m8 ? 1 : 0) * list_cap + ti];
+        j = e >> 3;
+        t = (int)(e & 7);
+    }
+    if (!m8) {
+        // this warp's 8 adaptive tables
+        for (uint32_t k = 0; k < 8; k++) {
+            const uint32_t tk = wg * 8 + k;
+            if (tk >= nlist) break;
+            const uint32_t e = lists[tk];
+            const uint32_t jj = e >> 3, tt = e & 7;
+            const uint32_t mi = tt == T_LIT ? 0 : 1 + (tt - 1) / 2;
+            const EncSym* src = tabs + ((uint64_t)jj * 4 + mi) * 256;
+            for (uint32_t i = lane; i < 256; i += 32) wtab[k * 256 + i] = src[i];
+        }
+    }
+    __syncthreads();
+    if (!have) return;
     const Job job = jobs[j];
     const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
-    if (!task_active(job, lens, t)) return;
     const uint32_t n = task_len(lens, t);
     const int s = t == T_LIT ? S_LIT : S_OP + (t - 1) / 2;
     const uint8_t* src = streams + job.str_off + stream_base(job, s);
     uint8_t* base = ans + job.ans_off + ans_task_off(job, t);
     LaneIO io = lane_io(base, task_cap(job, t), l);
-    TaskOut* o = outs + task;
-    const bool m8 = t != T_LIT && (t & 1) == 1;
-    if (m8) {
-        rans_lane<true>(src, n, l, meta8, ctxlut, io, &o->state[l], &o->count[l]);
-    } else {
-        const int mi = t == T_LIT ? 0 : 1 + (t - 1) / 2;  // model index: lit, op, meta, var
-        rans_lane<false>(src, n, l, tabs + ((uint64_t)j * 4 + mi) * 256, nullptr, io, &o->state[l], &o->count[l]);
-    }
+    TaskOut* o = outs + (uint64_t)j * T_COUNT + t;
+    if (m8) rans_lane<true>(src, n, l, wtab, s_lut, io, &o->state[l], &o->count[l]);
+    else rans_lane<false>(src, n, l, wtab + slot * 256, nullptr, io, &o->state[l], &o->count[l]);
 }
 
 // ---------------------------------------------------------------------------
 // Stitch: write the reference byte order of a 4-lane rANS stream, i.e. the
-// reversal of the interleaved emission sequence.  For rounds j = 0, 1, ...
-// and lanes l = 0..3 it places lane l's bytes of round j (last-emitted first).
-// Lane l's bytes of round j sit at count_l - (bytes of rounds <= j) in its own
-// stream because the lane emitted rounds in descending order.
-// Runs on a whole CTA; rounds are scanned 16 per thread per pass.
+// reversal of the interleaved emission sequence (the reference emits round
+// j's bytes lane 3 first, rounds from the top down, then reverses).  For
+// rounds j = 0, 1, ... and lanes l = 0..3 it places the k(l, j) bytes of
+// raw[l][j], second-emitted byte first.  Rounds are taken 16 per thread per
+// pass; one block-wide exclusive scan of the per-thread byte counts gives
+// every thread its output position.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t sum2(uint32_t w) {  // sum of the 16 2-bit fields
     w = (w & 0x33333333u) + ((w >> 2) & 0x33333333u);
@@ -438,73 +585,77 @@ __device__ __forceinline__ uint32_t sum2(uint32_t w) {  // sum of the 16 2-bit f
 }
 
 template <int NT>
-__device__ void block_stitch(const uint8_t* task_base, uint32_t cap, uint32_t n, const uint32_t* count,
-                             uint8_t* __restrict__ out) {
-    __shared__ uint32_t s_scan[NT];
-    __shared__ uint32_t s_carry[4];
+__device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s_warp, uint32_t& total) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t t = lane < NT / 32 ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, t, o);
+            if (lane >= (uint32_t)o) t += y;
+        }
+        s_warp[lane] = t;  // inclusive warp prefix
+    }
+    __syncthreads();
+    total = s_warp[NT / 32 - 1];
+    const uint32_t base = warp ? s_warp[warp - 1] : 0;
+    __syncthreads();
+    return base + x - v;
+}
+
+template <int NT>
+__device__ void block_stitch(const uint8_t* task_base, uint32_t cap, uint32_t n, uint8_t* __restrict__ out) {
+    __shared__ uint32_t s_warp[32];
     const uint32_t tid = threadIdx.x;
     const uint32_t rounds = (n + 3) / 4;
-    const uint8_t* lb[4];
+    const uint16_t* raw[4];
     const uint32_t* nw[4];
     for (uint32_t l = 0; l < 4; l++) {
-        lb[l] = task_base + (uint64_t)l * ans_lane_cap(cap);
+        raw[l] = reinterpret_cast<const uint16_t*>(task_base + (uint64_t)l * ans_lane_cap(cap));
         nw[l] = reinterpret_cast<const uint32_t*>(task_base + 4 * ans_lane_cap(cap)) + (uint64_t)l * ans_nbw_cap(cap);
     }
-    if (tid < 4) s_carry[tid] = 0;  // per-lane bytes of rounds already done
-    __syncthreads();
+    uint32_t carry = 0;
     for (uint32_t r0 = 0; r0 < rounds; r0 += 16 * NT) {
-        const uint32_t rb = r0 + 16 * tid;  // this thread's first round (multiple of 16)
-        uint32_t w[4] = {0, 0, 0, 0}, c[4] = {0, 0, 0, 0};
+        const uint32_t rb = r0 + 16 * tid;  // first round of this thread (multiple of 16)
+        uint32_t w[4] = {0, 0, 0, 0}, c = 0;
         if (rb < rounds) {
+#pragma unroll
             for (uint32_t l = 0; l < 4; l++) {
-                // lanes with no symbol in the top partial word have their bits
-                // cleared by construction (those rounds were never processed)
-                const uint32_t jmax = n > l ? (n - 1 - l) / 4 : 0;
-                if (n > l && rb <= jmax) {
-                    uint32_t v = nw[l][rb >> 4];
-                    const uint32_t top = jmax - rb;  // rounds of this word that exist
-                    if (top < 15) v &= (1u << (2 * (top + 1))) - 1u;
-                    w[l] = v;
-                    c[l] = sum2(v);
-                }
+                if (n <= l) continue;
+                const uint32_t jmax = (n - 1 - l) / 4;
+                if (rb > jmax) continue;
+                uint32_t v = nw[l][rb >> 4];
+                const uint32_t top = jmax - rb;  // rounds of this word the lane has
+                if (top < 15) v &= (1u << (2 * (top + 1))) - 1u;
+                w[l] = v;
+                c += sum2(v);
             }
         }
-        // block exclusive scan of the four per-lane counts packed in 8-bit
-        // fields would overflow; scan them one lane at a time instead
-        uint32_t pre[4];
-        for (uint32_t l = 0; l < 4; l++) {
-            s_scan[tid] = c[l];
-            __syncthreads();
-            for (uint32_t o = 1; o < NT; o <<= 1) {
-                uint32_t t = tid >= o ? s_scan[tid - o] : 0;
-                __syncthreads();
-                s_scan[tid] += t;
-                __syncthreads();
-            }
-            pre[l] = s_carry[l] + s_scan[tid] - c[l];
-            const uint32_t tot = s_scan[NT - 1];
-            __syncthreads();
-            if (tid == 0) s_carry[l] += tot;
-            __syncthreads();
-        }
+        uint32_t total;
+        uint32_t op = carry + block_exclusive_scan<NT>(c, s_warp, total);
+        carry += total;
         if (rb < rounds) {
-            // output position of round rb = bytes of all lanes in rounds < rb
-            uint32_t op = pre[0] + pre[1] + pre[2] + pre[3];
-            uint32_t lp[4] = {pre[0], pre[1], pre[2], pre[3]};  // per-lane bytes of rounds < current
             const uint32_t re = min(rounds, rb + 16);
             for (uint32_t jr = rb; jr < re; jr++) {
                 const uint32_t sh = 2 * (jr & 15);
+#pragma unroll
                 for (uint32_t l = 0; l < 4; l++) {
                     const uint32_t k = (w[l] >> sh) & 3u;
                     if (!k) continue;
-                    lp[l] += k;
-                    const uint32_t at = count[l] - lp[l];  // first (earliest-emitted) byte of this round
-                    if (k == 2) { out[op] = lb[l][at + 1]; out[op + 1] = lb[l][at]; op += 2; }
-                    else { out[op] = lb[l][at]; op += 1; }
+                    const uint32_t v = raw[l][jr];
+                    if (k == 2) { out[op] = (uint8_t)(v >> 8); out[op + 1] = (uint8_t)v; op += 2; }
+                    else { out[op] = (uint8_t)v; op += 1; }
                 }
             }
         }
-        __syncthreads();
     }
 }
 

@@ -117,7 +117,7 @@ __device__ uint32_t write_container(uint8_t* dst, uint8_t flags, uint32_t n, con
         for (int k = 0; k < 4; k++) put32(dst + h + 4 * k, o.state[k]);
     }
     if (info) block_copy(dst + 8, info->mat, info->mat_len);
-    block_stitch<kAsmThreads>(task_base, cap, n, o.count, dst + h + 16);
+    block_stitch<kAsmThreads>(task_base, cap, n, dst + h + 16);
     return h + 16 + tsum(o);
 }
 

@@ -73,15 +73,26 @@ __global__ void k_stream_norm(const STask* __restrict__ tasks, uint32_t ntasks, 
     warp_build_table(s_freq, tabs + (uint64_t)ti * 256, infos + ti, lane);
 }
 
-__global__ void __launch_bounds__(128) k_stream_rans(const STask* __restrict__ tasks, uint32_t ntasks,
-                                                     const EncSym* __restrict__ tabs, TaskOut* __restrict__ outs) {
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t ti = g >> 2, l = g & 3;
+// One warp per 8 tasks (4 lanes each), tables and rings in shared memory.
+__global__ void __launch_bounds__(kRansWarps * 32) k_stream_rans(const STask* __restrict__ tasks, uint32_t ntasks,
+                                                                 const EncSym* __restrict__ tabs,
+                                                                 TaskOut* __restrict__ outs) {
+    extern __shared__ __align__(16) uint8_t smem_s[];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t wg = blockIdx.x * kRansWarps + warp;
+    EncSym* wtab = reinterpret_cast<EncSym*>(smem_s + warp * kRansTabBytes);
+    for (uint32_t k = 0; k < 8; k++) {
+        const uint32_t tk = wg * 8 + k;
+        if (tk >= ntasks) break;
+        for (uint32_t i = lane; i < 256; i += 32) wtab[k * 256 + i] = tabs[(uint64_t)tk * 256 + i];
+    }
+    __syncwarp();
+    const uint32_t ti = wg * 8 + (lane >> 2), l = lane & 3;
     if (ti >= ntasks) return;
     const STask t = tasks[ti];
     if (t.n == 0) return;
     LaneIO io = lane_io(reinterpret_cast<uint8_t*>(t.scr), t.cap, l);
-    rans_lane<false>(reinterpret_cast<const uint8_t*>(t.src), t.n, l, tabs + (uint64_t)ti * 256, nullptr, io,
+    rans_lane<false>(reinterpret_cast<const uint8_t*>(t.src), t.n, l, wtab + (lane >> 2) * 256, nullptr, io,
                      &outs[ti].state[l], &outs[ti].count[l]);
 }
 
@@ -107,7 +118,7 @@ __global__ void __launch_bounds__(kStitchThreads) k_stream_stitch(const STask* _
         out_lens[ti] = h + 16 + o.count[0] + o.count[1] + o.count[2] + o.count[3];
     }
     for (uint32_t i = threadIdx.x; i < info->mat_len; i += kStitchThreads) dst[8 + i] = info->mat[i];
-    block_stitch<kStitchThreads>(reinterpret_cast<const uint8_t*>(t.scr), t.cap, t.n, o.count, dst + h + 16);
+    block_stitch<kStitchThreads>(reinterpret_cast<const uint8_t*>(t.scr), t.cap, t.n, dst + h + 16);
 }
 
 // PackStreamFlat (przm_ans.cu:202-234): 0x00 | LE32 n | payload.

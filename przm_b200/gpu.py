@@ -377,6 +377,20 @@ class GPUCompressor:
         frames = [bytes(o[: jobs[i].out_len]) for i, o in enumerate(outs)]
         return frames, [jobs[i].status for i in range(len(arrs))], GPUProfile.of(p)
 
+    def CompressPacked(self, host_in: np.ndarray, sizes, profile: int = PROFILE_ANS,
+                       host_out: np.ndarray | None = None) -> tuple[np.ndarray, np.ndarray]:
+        """Back-to-back inputs in one host buffer -> back-to-back frames and
+        their sizes (one upload, one launch sequence, one download)."""
+        sz = np.ascontiguousarray(sizes, np.uint64)
+        if host_out is None:
+            host_out = np.zeros(int(sum(FrameBound(int(s)) for s in sz)) + 64, np.uint8)
+        out_sizes = np.zeros(max(len(sz), 1), np.uint32)
+        total = C.c_uint64()
+        _check(L().przmg_compress_packed(self._h, C.c_void_p(host_in.ctypes.data), _ptr(sz), len(sz), profile,
+                                         C.c_void_p(host_out.ctypes.data), host_out.nbytes, _ptr(out_sizes),
+                                         C.byref(total)))
+        return host_out[: total.value], out_sizes[: len(sz)]
+
     # -- histogram / flat / V-ANS --
     def ComputeHistogramGPU(self, dIn: int, n: int, stream: int = 0):
         """gpu/bridge.go:2890 -> (counts, ms, GB/s)"""
@@ -485,6 +499,35 @@ class DeviceBatch:
 
     def launches(self) -> int:
         return int(L().przmg_batch_launch_count(self._h))
+
+    def upload(self, host_packed: np.ndarray, stream: int = 0) -> None:
+        """Back-to-back inputs (sum of sizes) from host memory (pinned for
+        full speed) into the batch, asynchronously on `stream`."""
+        _check(L().przmg_batch_upload(self._h, C.c_void_p(host_packed.ctypes.data), stream))
+
+    def download(self, host_out: np.ndarray, stream: int = 0) -> tuple[int, np.ndarray]:
+        """Synchronise and copy the frames back to back into host_out."""
+        total = C.c_uint64()
+        sizes = np.zeros(max(len(self.sizes), 1), np.uint32)
+        _check(L().przmg_batch_download(self._h, C.c_void_p(host_out.ctypes.data), host_out.nbytes, C.byref(total),
+                                        _ptr(sizes), stream))
+        return total.value, sizes[: len(self.sizes)]
+
+    STAT_KEYS = ("input_bytes", "frame_bytes", "literal_bytes", "command_bytes", "offset_bytes", "rans_symbols",
+                 "rans_emitted_bytes", "uncompressed_frames")
+
+    def stats(self) -> dict[str, int]:
+        """Totals of the last run."""
+        s = np.zeros(8, np.uint64)
+        _check(L().przmg_batch_stats(self._h, _ptr(s)))
+        return {k: int(v) for k, v in zip(self.STAT_KEYS, s)}
+
+    def stage_times(self) -> dict[str, float]:
+        """One enqueue with events between stages: {stage: device ms}."""
+        ms = (C.c_float * 16)()
+        n = C.c_int32()
+        _check(L().przmg_batch_stage_times(self._h, ms, 16, C.byref(n)))
+        return {L().przmg_stage_name(k).decode(): float(ms[k]) for k in range(n.value)}
 
     def close(self) -> None:
         if self._h:
