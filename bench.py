@@ -97,7 +97,7 @@ class ClockSampler:
     def start(self) -> None:
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -109,6 +109,14 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.rows.append([x.strip() for x in line.split(",")])
 
+    def ready(self, timeout: float = 5.0) -> None:
+        """Waits until nvidia-smi delivered its first sample, then forgets the
+        samples taken so far: only the ones from here on are reported."""
+        t0 = time.time()
+        while self.proc is not None and not self.rows and time.time() - t0 < timeout:
+            time.sleep(0.01)
+        self.skip = len(self.rows)
+
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -118,6 +126,7 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         self.thread.join(timeout=5)
+        self.rows = self.rows[getattr(self, "skip", 0):]
         sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -256,7 +265,7 @@ def main() -> None:
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
-    time.sleep(0.3)
+    clocks.ready()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
@@ -266,7 +275,6 @@ def main() -> None:
         e1.record(stream)
     e1.synchronize()
     torch.cuda.synchronize()
-    clk = clocks.stop()
     ms = e0.elapsed_time(e1) / args.steps
     if pg:
         t = torch.tensor([ms], device=f"cuda:{local}")
@@ -288,6 +296,7 @@ def main() -> None:
         a1.record(stream)
         a1.synchronize()
         e2e_ms.append(a0.elapsed_time(a1))
+    clk = clocks.stop()  # samples cover the device-timed and the end-to-end regions
     e2e_ms.sort()
     e2e_step = e2e_ms[len(e2e_ms) // 2] if e2e_ms else float("nan")
     if pg:

@@ -95,10 +95,11 @@ __host__ __device__ inline uint64_t ans_region_bytes(const Job& j) { return ans_
 //         f = 2^t uses m = 2^(32-t), s = 0; f = 1 uses m = 2^32-1 (one short)
 //         with the deficit folded into cb.
 //   t1  : 4096 * f, the renormalisation bound (x >= t1 -> emit a byte)
-//   cb  : cumulative frequency c (+4095 when f == 1)
-//   cfs : (4096 - f) | s << 16
+//   t2  : 256 * t1 saturated to 2^32-1 (x >= t2 -> emit a second byte)
+//   w   : cb | (4096 - f) << 13 | s << 25, cb = cumulative frequency c
+//         (+4095 when f == 1)
 struct __align__(16) EncSym {
-    uint32_t m, t1, cb, cfs;
+    uint32_t m, t1, t2, w;
 };
 
 // Per-task results of the rANS kernel.

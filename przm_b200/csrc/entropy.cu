@@ -10,7 +10,7 @@ namespace pz {
 // ---------------------------------------------------------------------------
 __host__ __device__ inline EncSym make_encsym(uint32_t f, uint32_t c) {
     EncSym e;
-    if (f == 0) { e.m = 0; e.t1 = 0xFFFFFFFFu; e.cb = 0; e.cfs = 0; return e; }
+    if (f == 0) { e.m = 0; e.t1 = 0xFFFFFFFFu; e.t2 = 0xFFFFFFFFu; e.w = 0; return e; }
     uint32_t s = 0;
     while ((2u << s) <= f) s++;  // floor(log2 f)
     uint32_t cb = c;
@@ -18,8 +18,9 @@ __host__ __device__ inline EncSym make_encsym(uint32_t f, uint32_t c) {
     else if ((f & (f - 1)) == 0) { e.m = 1u << (32 - s); s = 0; }
     else e.m = (uint32_t)(((1ull << (32 + s)) + f - 1) / f);
     e.t1 = 4096u * f;
-    e.cb = cb;
-    e.cfs = (4096u - f) | (s << 16);
+    const uint64_t t2 = 256ull * e.t1;
+    e.t2 = t2 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)t2;
+    e.w = cb | ((4096u - f) << 13) | (s << 25);
     return e;
 }
 
@@ -340,38 +341,124 @@ __device__ __forceinline__ LaneIO lane_io(uint8_t* task_base, uint32_t cap, uint
 
 // One rANS step (table entry e of the symbol already in registers): returns
 // the number k of low bytes of x the reference would emit (x >= 4096 f, and
-// again when x >> 8 >= 4096 f), and advances x.  The caller keeps the low
-// 16 bits of x from before the step; its first k bytes (low byte first) are
-// what the reference writes.
-__device__ __forceinline__ uint32_t rans_step(uint32_t& x, const EncSym& e) {
+// again when x >= 2^20 f), and advances x.  The caller keeps the low 16 bits
+// of x from before the step; its first k bytes (low byte first) are what the
+// reference writes.  x < 2^24 throughout, so x >= t2 can only hold for f < 16.
+// The three candidate states (0, 1 or 2 bytes shifted out) are computed side
+// by side and selected last, which keeps the compares off the multiply's
+// dependency chain.
+__device__ __forceinline__ uint32_t rans_next(uint32_t x, const EncSym& e) {
+    const uint32_t s = e.w >> 25, cf = (e.w >> 13) & 0xFFFu, cb = e.w & 0x1FFFu;
     const uint32_t x8 = x >> 8, x16 = x >> 16;
-    const bool p1 = x >= e.t1, p2 = x8 >= e.t1;
-    const uint32_t xr = p2 ? x16 : (p1 ? x8 : x);
-    const uint32_t q = __umulhi(xr, e.m) >> (e.cfs >> 16);
-    x = xr + q * (e.cfs & 0xFFFFu) + e.cb;
-    return (uint32_t)p1 + (uint32_t)p2;
+    const uint32_t a0 = x + cb + (__umulhi(x, e.m) >> s) * cf;
+    const uint32_t a1 = x8 + cb + (__umulhi(x8, e.m) >> s) * cf;
+    const uint32_t a2 = x16 + cb + (__umulhi(x16, e.m) >> s) * cf;
+    return x >= e.t2 ? a2 : (x >= e.t1 ? a1 : a0);
+}
+__device__ __forceinline__ uint32_t rans_step(uint32_t& x, const EncSym& e) {
+    const uint32_t k = (uint32_t)(x >= e.t1) + (uint32_t)(x >= e.t2);
+    x = rans_next(x, e);
+    return k;
+}
+
+// Table index of round r of a 16-round group (words w, group g, lane l).
+template <bool kMeta8>
+__device__ __forceinline__ uint32_t group_index(const uint32_t* w, uint32_t below, int r, int32_t g, uint32_t l,
+                                                uint32_t sel, uint32_t selp, const uint8_t* ctxlut) {
+    uint32_t ti = __byte_perm(w[r], 0, sel);
+    if (kMeta8) {
+        uint32_t prev;
+        if (l > 0) prev = __byte_perm(w[r], 0, selp);
+        else prev = r > 0 ? (w[r - 1] >> 24) : (below >> 24);
+        const bool first = (g == 0 && r == 0 && l == 0);
+        ti |= (first ? 0u : (uint32_t)ctxlut[prev]) << 8;
+    }
+    return ti;
+}
+
+__device__ __forceinline__ void words16(const uint4* c, uint32_t* w) {
+#pragma unroll
+    for (int v = 0; v < 4; v++) { w[4 * v] = c[v].x; w[4 * v + 1] = c[v].y; w[4 * v + 2] = c[v].z; w[4 * v + 3] = c[v].w; }
+}
+
+// Spreads the 16 bits of v to the even bit positions of a 32-bit word.
+__device__ __forceinline__ uint32_t spread16(uint32_t v) {
+    v = (v | (v << 8)) & 0x00FF00FFu;
+    v = (v | (v << 4)) & 0x0F0F0F0Fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+// The 16 chain steps of one full group with the entries already in
+// registers; writes the group's records and its 2-bit count word.
+__device__ __forceinline__ void encode_group(uint32_t& x, uint32_t& cnt, const EncSym* e, int32_t g, uint4* r4,
+                                             uint32_t* nbw) {
+    uint32_t rec[16], m1 = 0, m2 = 0;
+#pragma unroll
+    for (int r = 15; r >= 0; r--) {
+        rec[r] = x & 0xFFFFu;
+        m1 |= x >= e[r].t1 ? (1u << r) : 0u;
+        m2 |= x >= e[r].t2 ? (1u << r) : 0u;
+        x = rans_next(x, e[r]);
+    }
+    // k = p1 + p2 with p2 => p1: bit 0 = p1 ^ p2, bit 1 = p2
+    nbw[g] = spread16(m1 ^ m2) | (spread16(m2) << 1);
+    cnt += __popc(m1) + __popc(m2);
+    r4[2 * g] = make_uint4(rec[0] | (rec[1] << 16), rec[2] | (rec[3] << 16), rec[4] | (rec[5] << 16),
+                           rec[6] | (rec[7] << 16));
+    r4[2 * g + 1] = make_uint4(rec[8] | (rec[9] << 16), rec[10] | (rec[11] << 16), rec[12] | (rec[13] << 16),
+                               rec[14] | (rec[15] << 16));
+}
+
+// ---- per-lane symbol ring: cp.async copies of the 64-byte groups ---------
+// Each thread owns kRing slots of 64 bytes in its warp's ring; chunk v of
+// slot q of lane t sits at uint4 index (q * 4 + v) * 32 + t, so the 32 lanes
+// of one access touch 32 consecutive 16-byte words (no bank conflicts).
+constexpr int kRing = 4;                                              // groups in flight per lane
+constexpr uint32_t kRingBytesPerWarp = kRing * 4 * 32 * sizeof(uint4);  // 8 KiB
+
+__device__ __forceinline__ void ring_fetch(uint4* ring, uint32_t t, int32_t slot, const uint4* s4, int32_t g) {
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(ring + (((slot & (kRing - 1)) * 4 + v) << 5) + t);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(s4 + 4 * g + v) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void ring_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void ring_read(const uint4* ring, uint32_t t, int32_t slot, uint4* w) {
+#pragma unroll
+    for (int v = 0; v < 4; v++) w[v] = ring[(((slot & (kRing - 1)) * 4 + v) << 5) + t];
 }
 
 // Encodes lane l of one task.  Symbols of lane l are i = 4j + l, rounds j
 // from the top down.  Per round the lane stores the 16 low bits of x before
 // the step at raw[j] and the byte count k in 2 bits of nbw[j / 16]; the
 // stitch turns (raw, k) back into the reference byte order.  Rounds come in
-// groups of 16 (64 source bytes holding the four lanes' symbols); the top,
-// partial group takes the byte path, full groups are loaded one group ahead
-// and their 16 table entries are fetched before the dependent chain runs.
+// groups of 16 (the 64 source bytes 64g .. 64g + 63 hold the four lanes'
+// symbols); the rounds above the G = n / 64 full groups take the byte path.
+// Full groups stream through the thread's ring: the 64 bytes of group g - 4
+// are requested (cp.async, no register waits on them) while group g is
+// encoded, the words of group g - 1 are read from the ring one group ahead,
+// and the 16 table entries of group g are fetched before its chain runs.
 template <bool kMeta8>
 __device__ __forceinline__ void rans_lane(const uint8_t* __restrict__ src, uint32_t n, uint32_t l,
                                           const EncSym* __restrict__ tab, const uint8_t* __restrict__ ctxlut,
-                                          LaneIO io, uint32_t* out_state, uint32_t* out_count) {
+                                          uint4* ring, LaneIO io, uint32_t* out_state, uint32_t* out_count) {
     uint32_t x = 65536, cnt = 0;
     uint16_t* raw = reinterpret_cast<uint16_t*>(io.bytes);
+    const uint32_t t = threadIdx.x & 31;
     if (n > l) {
         const uint32_t J = (n - 1 - l) >> 2;
         const bool vec = (reinterpret_cast<uintptr_t>(src) & 15) == 0;
-        const uint32_t G = vec ? (J >> 4) : 0;
+        const int32_t G = vec ? (int32_t)(n >> 6) : 0;
         {
             uint32_t acc = 0;
-            for (int32_t j = (int32_t)J; j >= (int32_t)(16 * G); j--) {
+            for (int32_t j = (int32_t)J; j >= 16 * G; j--) {
                 const uint32_t i = 4u * (uint32_t)j + l;
                 uint32_t ti = src[i];
                 if (kMeta8) ti |= (i ? (uint32_t)ctxlut[src[i - 1]] : 0u) << 8;
@@ -388,48 +475,33 @@ __device__ __forceinline__ void rans_lane(const uint8_t* __restrict__ src, uint3
         if (G > 0) {
             const uint4* s4 = reinterpret_cast<const uint4*>(src);
             uint4* r4 = reinterpret_cast<uint4*>(raw);
-            const uint32_t sel = 0x4440u | l;        // __byte_perm selector of byte l
-            const uint32_t selp = 0x4440u | (l - 1);  // byte l-1 (l >= 1)
-            uint4 cur[4], nxt[4];
+            const uint32_t sel = 0x4440u | l;               // __byte_perm selector of byte l
+            const uint32_t selp = 0x4440u | ((l + 3) & 3);  // byte l-1 (used for l >= 1)
+            // prologue: groups G-1 .. G-kRing (clamped at 0), one commit group each
 #pragma unroll
-            for (int v = 0; v < 4; v++) cur[v] = __ldg(s4 + 4 * (G - 1) + v);
-            for (int32_t g = (int32_t)G - 1; g >= 0; g--) {
-                if (g > 0) {
-#pragma unroll
-                    for (int v = 0; v < 4; v++) nxt[v] = __ldg(s4 + 4 * (g - 1) + v);
-                }
-                const uint32_t w[16] = {cur[0].x, cur[0].y, cur[0].z, cur[0].w, cur[1].x, cur[1].y, cur[1].z, cur[1].w,
-                                        cur[2].x, cur[2].y, cur[2].z, cur[2].w, cur[3].x, cur[3].y, cur[3].z, cur[3].w};
+            for (int d = 0; d < kRing; d++) ring_fetch(ring, t, G - 1 - d, s4, max(G - 1 - d, 0));
+            ring_wait<kRing - 1>();
+            uint4 cur[4];
+            ring_read(ring, t, G - 1, cur);
+            for (int32_t g = G - 1; g >= 0; g--) {
+                ring_wait<kRing - 2>();  // group g - 1 has landed
+                uint4 nxt[4];
+                ring_read(ring, t, g - 1, nxt);
                 EncSym e[16];
+                {
+                    uint32_t w[16];
+                    words16(cur, w);
+                    const uint32_t below = g > 0 ? nxt[3].w : 0u;
 #pragma unroll
-                for (int r = 0; r < 16; r++) {
-                    uint32_t ti = __byte_perm(w[r], 0, sel);
-                    if (kMeta8) {
-                        uint32_t prev;
-                        if (l > 0) prev = __byte_perm(w[r], 0, selp);
-                        else prev = r > 0 ? (w[r - 1] >> 24) : ((g > 0 ? nxt[3].w : 0u) >> 24);
-                        const bool first = (g == 0 && r == 0 && l == 0);
-                        ti |= (first ? 0u : (uint32_t)ctxlut[prev]) << 8;
-                    }
-                    e[r] = tab[ti];
+                    for (int r = 15; r >= 0; r--) e[r] = tab[group_index<kMeta8>(w, below, r, g, l, sel, selp, ctxlut)];
                 }
-                uint32_t rec[16], acc = 0, kk = 0;
-#pragma unroll
-                for (int r = 15; r >= 0; r--) {
-                    rec[r] = x & 0xFFFFu;
-                    const uint32_t k = rans_step(x, e[r]);
-                    kk += k;
-                    acc |= k << (2 * r);
-                }
-                io.nbw[g] = acc;
-                cnt += kk;
-                r4[2 * g] = make_uint4(rec[0] | (rec[1] << 16), rec[2] | (rec[3] << 16), rec[4] | (rec[5] << 16),
-                                       rec[6] | (rec[7] << 16));
-                r4[2 * g + 1] = make_uint4(rec[8] | (rec[9] << 16), rec[10] | (rec[11] << 16),
-                                           rec[12] | (rec[13] << 16), rec[14] | (rec[15] << 16));
+                // the slot of group g is free once its words are in registers
+                ring_fetch(ring, t, g, s4, max(g - kRing, 0));
+                encode_group(x, cnt, e, g, r4, io.nbw);
 #pragma unroll
                 for (int v = 0; v < 4; v++) cur[v] = nxt[v];
             }
+            ring_wait<0>();
         }
     }
     *out_state = x;
@@ -506,9 +578,13 @@ __global__ void __launch_bounds__(1024) k_task_list(const Job* __restrict__ jobs
     }
 }
 
-constexpr int kRansWarps = 4;
+// One warp per block: the chains are latency-bound and every lane's 16
+// table loads per group go through the SM's shared-memory pipe, so warps
+// that share an SM slow each other down; with one warp per block the block
+// scheduler spreads the (longest-first) warps over distinct SMs.
+constexpr int kRansWarps = 1;
 constexpr uint32_t kRansTabBytes = 8 * 256 * sizeof(EncSym);          // 8 models per warp (32 KiB)
-constexpr uint32_t kRansSmem = kRansWarps * kRansTabBytes;              // per-warp tables
+constexpr uint32_t kRansSmem = kRansWarps * (kRansTabBytes + kRingBytesPerWarp);  // tables, rings
 
 // Blocks [0, nb_ad) run adaptive-model tasks, the rest Meta8 tasks; each
 // warp takes 8 consecutive tasks of its list (4 lanes per task).
@@ -528,6 +604,7 @@ __global__ void __launch_bounds__(kRansWarps * 32) k_rans(const Job* __restrict_
     const uint32_t nlist = counts[m8 ? 1 : 0];
     const uint32_t wg = (m8 ? blockIdx.x - nb_ad : blockIdx.x) * kRansWarps + warp;  // warp index in its list
     EncSym* wtab = reinterpret_cast<EncSym*>(smem_r + warp * kRansTabBytes);
+    uint4* wring = reinterpret_cast<uint4*>(smem_r + kRansWarps * kRansTabBytes + warp * kRingBytesPerWarp);
     if (m8) {
         // the block shares the 8 static models; every warp holds a copy
         for (uint32_t i = lane; i < 8 * 256; i += 32) wtab[i] = meta8[i];
@@ -565,8 +642,8 @@ __global__ void __launch_bounds__(kRansWarps * 32) k_rans(const Job* __restrict_
     uint8_t* base = ans + job.ans_off + ans_task_off(job, t);
     LaneIO io = lane_io(base, task_cap(job, t), l);
     TaskOut* o = outs + (uint64_t)j * T_COUNT + t;
-    if (m8) rans_lane<true>(src, n, l, wtab, s_lut, io, &o->state[l], &o->count[l]);
-    else rans_lane<false>(src, n, l, wtab + slot * 256, nullptr, io, &o->state[l], &o->count[l]);
+    if (m8) rans_lane<true>(src, n, l, wtab, s_lut, wring, io, &o->state[l], &o->count[l]);
+    else rans_lane<false>(src, n, l, wtab + slot * 256, nullptr, wring, io, &o->state[l], &o->count[l]);
 }
 
 // ---------------------------------------------------------------------------

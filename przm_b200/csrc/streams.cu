@@ -81,6 +81,7 @@ __global__ void __launch_bounds__(kRansWarps * 32) k_stream_rans(const STask* __
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t wg = blockIdx.x * kRansWarps + warp;
     EncSym* wtab = reinterpret_cast<EncSym*>(smem_s + warp * kRansTabBytes);
+    uint4* wring = reinterpret_cast<uint4*>(smem_s + kRansWarps * kRansTabBytes + warp * kRingBytesPerWarp);
     for (uint32_t k = 0; k < 8; k++) {
         const uint32_t tk = wg * 8 + k;
         if (tk >= ntasks) break;
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(kRansWarps * 32) k_stream_rans(const STask* __
     const STask t = tasks[ti];
     if (t.n == 0) return;
     LaneIO io = lane_io(reinterpret_cast<uint8_t*>(t.scr), t.cap, l);
-    rans_lane<false>(reinterpret_cast<const uint8_t*>(t.src), t.n, l, wtab + (lane >> 2) * 256, nullptr, io,
+    rans_lane<false>(reinterpret_cast<const uint8_t*>(t.src), t.n, l, wtab + (lane >> 2) * 256, nullptr, wring, io,
                      &outs[ti].state[l], &outs[ti].count[l]);
 }
 
