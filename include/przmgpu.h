@@ -236,6 +236,35 @@ int32_t przmg_vans_encode_batch(przmg_ctx* ctx, uint64_t d_in, const uint64_t* i
                                 uint64_t count, int32_t norm, uint64_t d_out, const uint64_t* out_offs,
                                 uint32_t* out_lens, uint64_t stream);
 
+/* ---- allocation-free V-ANS encode: no counterpart in the reference -------
+ * Histogram + normalise + V-ANS of ONE device stream: the same launch
+ * sequence and the same container bytes as przmg_vans_encode_batch with
+ * count == 1, for callers that must not allocate device memory (a serving
+ * loop whose device-memory budget is spent, an out-of-memory recovery path,
+ * or a stream that must not meet the device-wide synchronisation of
+ * cudaFree).  It allocates nothing: no cudaMalloc/cudaFree, no host staging
+ * copy, no context; all scratch is one file-scope __device__ array of about
+ * 2.3 MiB per device, so n is limited to PRZMG_NOALLOC_MAX_N symbols.
+ *   n > PRZMG_NOALLOC_MAX_N           -> PRZMG_ERR_EXCEEDS_MAX_BLOCK
+ *   out_cap < 1024 + 2 * n            -> PRZMG_ERR_BUFFER_TOO_SMALL
+ *   unknown norm or null address      -> PRZMG_ERR_INVALID_ARG
+ * (nothing is launched on an error; przmg_last_error() says why).
+ * Runs on the CURRENT device, asynchronously on `stream` (0 = the legacy
+ * default stream); the container length is written as a u32 to the device
+ * address d_out_len when the stream reaches it.  The first call on each
+ * device does setup (cudaGetSymbolAddress of the scratch with that device
+ * current, which may load the module, and the rANS kernel's shared-memory
+ * attribute): make one call on every device before capturing a stream.
+ * Nothing in the scratch has to start at zero: each call clears the 1 KiB
+ * histogram it counts into and overwrites the rest before reading it.
+ * All calls on one device share the one scratch, so calls that overlap in
+ * time (on two streams, or from two host threads) race and corrupt each
+ * other's output: serialise them (one stream, or a lock around the call
+ * and a wait for the stream). */
+#define PRZMG_NOALLOC_MAX_N (1u << 20)
+int32_t przmg_vans_encode_noalloc(uint64_t d_in, uint32_t n, int32_t norm, uint64_t d_out, uint64_t out_cap,
+                                  uint64_t d_out_len, uint64_t stream);
+
 /* host helpers */
 void przmg_normalize_freq(const uint32_t counts[256], uint32_t target_m, uint16_t freq[256]); /* NormalizeFreq, :2777 */
 void przmg_normalize_frequencies(const uint32_t counts[256], uint16_t freq[256]); /* literals.NormalizeFrequencies */

@@ -46,6 +46,8 @@ class Job(C.Structure):
                 ("reserved", i32)]
 
 
+NOALLOC_MAX_N = 1 << 20  # PRZMG_NOALLOC_MAX_N
+
 MATCH_DTYPE = np.dtype([("position", "<u4"), ("offset", "<u4"), ("length", "<u2"), ("literal", "u1"),
                         ("reserved", "u1")])
 
@@ -91,6 +93,7 @@ SIGNATURES: dict[str, tuple] = {
     "przmg_vans_encode4x_gpu": (i32, [vp, u64, u64, u64, vp, vp, vp, u32, u64, vp, vp, vp]),
     "przmg_vans_encode4x_host": (i32, [vp, vp, u64, vp, u64, vp, vp]),
     "przmg_vans_encode_batch": (i32, [vp, u64, vp, vp, u64, i32, u64, vp, vp, u64]),
+    "przmg_vans_encode_noalloc": (i32, [u64, u32, i32, u64, u64, u64, u64]),
     "przmg_normalize_freq": (None, [vp, u32, vp]),
     "przmg_normalize_frequencies": (None, [vp, vp]),
     "przmg_build_cdf": (None, [vp, vp]),

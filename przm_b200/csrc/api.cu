@@ -1220,6 +1220,11 @@ extern "C" int32_t przmg_match_lz77_streaming(przmg_ctx* h, const uint8_t* src, 
 #include "api_streams.inc"
 
 // ---------------------------------------------------------------------------
+// allocation-free single-stream V-ANS (static device scratch)
+// ---------------------------------------------------------------------------
+#include "noalloc.inc"
+
+// ---------------------------------------------------------------------------
 // pinned memory
 // ---------------------------------------------------------------------------
 extern "C" int32_t przmg_alloc_pinned_host(uint64_t size, void** out) {
