@@ -44,11 +44,15 @@ FRAME = 1 << 20
 # ---------------------------------------------------------------------------
 # CPU side: the oracle over the same frames on all host cores
 # ---------------------------------------------------------------------------
+def frame_seeds_of(rank_seed: int, idx) -> list[int]:
+    return [rank_seed + 7919 * i for i in idx]  # = shard.frame_seeds(rank)[i]
+
+
 def _cpu_worker(idx: list[int], rank_seed: int, barrier, q) -> None:
     sys.path.insert(0, ROOT)
     from oracle import oracle as O
     from przm_b200 import workloads as W
-    frames = [W.mixture(rank_seed + 7919 * i, FRAME)[0] for i in idx]
+    frames = [W.mixture(s, FRAME)[0] for s in frame_seeds_of(rank_seed, idx)]
     O.lib()
     barrier.wait()
     t0 = time.perf_counter()
@@ -175,7 +179,8 @@ def main() -> None:
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    rank_seed = 0x50525A4D + 2 + 1000003 * rank
+    from przm_b200 import shard
+    rank_seed = shard.rank_seed(rank)
     ncores = len(os.sched_getaffinity(0))
 
     if args.impl == "reference":
@@ -223,7 +228,7 @@ def main() -> None:
     from przm_b200 import workloads as W
 
     comp = gpu.GPUCompressor(local)
-    frames = [W.mixture(rank_seed + 7919 * i, FRAME)[0] for i in range(args.frames)]
+    frames = [W.mixture(s, FRAME)[0] for s in shard.frame_seeds(rank, args.frames)]
     sizes = [len(a) for a in frames]
     total = sum(sizes)
     host = np.empty(total, np.uint8)
@@ -277,9 +282,7 @@ def main() -> None:
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     if pg:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = shard.max_over_ranks(ms, pg, device=f"cuda:{local}")
         pg.barrier()
     value = world * total / (ms / 1e3) / 1e9
 
@@ -300,9 +303,7 @@ def main() -> None:
     e2e_ms.sort()
     e2e_step = e2e_ms[len(e2e_ms) // 2] if e2e_ms else float("nan")
     if pg:
-        t = torch.tensor([e2e_step], device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_step = float(t.item())
+        e2e_step = shard.max_over_ranks(e2e_step, pg, device=f"cuda:{local}")
 
     # plain per-frame launches (one launch sequence and one sync per frame)
     plain = None
