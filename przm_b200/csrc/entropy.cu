@@ -688,9 +688,29 @@ __device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s_warp, uint32_t&
     return base + x - v;
 }
 
+// Byte r (0..15) of the 16 u16 records held in two uint4.
+__device__ __forceinline__ uint32_t rec16(const uint4* v, int r) {
+    const uint4 q = v[r >> 3];
+    const uint32_t w = ((r >> 1) & 3) == 0 ? q.x : ((r >> 1) & 3) == 1 ? q.y : ((r >> 1) & 3) == 2 ? q.z : q.w;
+    return (r & 1) ? (w >> 16) : (w & 0xFFFFu);
+}
+
+// Bytes a stitch pass of NT threads x 16 rounds can produce (8 per round).
+template <int NT>
+struct StitchStage {
+    static constexpr uint32_t kBytes = NT * 16 * 8 + 16;
+};
+
+// Every pass: thread t takes rounds [r0 + 16t, r0 + 16t + 16) of the four
+// lanes (two 16-byte loads of records and one count word per lane), one
+// block scan gives its byte offset, it writes its bytes into a shared
+// staging buffer placed at the output's 16-byte phase, and the block then
+// stores the staged run with aligned 16-byte stores (byte stores only for
+// the partial first and last 16 bytes of the run).
 template <int NT>
 __device__ void block_stitch(const uint8_t* task_base, uint32_t cap, uint32_t n, uint8_t* __restrict__ out) {
     __shared__ uint32_t s_warp[32];
+    __shared__ __align__(16) uint8_t s_stage[StitchStage<NT>::kBytes];
     const uint32_t tid = threadIdx.x;
     const uint32_t rounds = (n + 3) / 4;
     const uint16_t* raw[4];
@@ -703,36 +723,58 @@ __device__ void block_stitch(const uint8_t* task_base, uint32_t cap, uint32_t n,
     for (uint32_t r0 = 0; r0 < rounds; r0 += 16 * NT) {
         const uint32_t rb = r0 + 16 * tid;  // first round of this thread (multiple of 16)
         uint32_t w[4] = {0, 0, 0, 0}, c = 0;
-        if (rb < rounds) {
+        uint4 rv[4][2];
 #pragma unroll
-            for (uint32_t l = 0; l < 4; l++) {
-                if (n <= l) continue;
-                const uint32_t jmax = (n - 1 - l) / 4;
-                if (rb > jmax) continue;
-                uint32_t v = nw[l][rb >> 4];
-                const uint32_t top = jmax - rb;  // rounds of this word the lane has
-                if (top < 15) v &= (1u << (2 * (top + 1))) - 1u;
-                w[l] = v;
-                c += sum2(v);
-            }
+        for (uint32_t l = 0; l < 4; l++) {
+            rv[l][0] = rv[l][1] = make_uint4(0, 0, 0, 0);
+            if (rb >= rounds || n <= l) continue;
+            const uint32_t jmax = (n - 1 - l) / 4;
+            if (rb > jmax) continue;
+            uint32_t v = nw[l][rb >> 4];
+            const uint32_t top = jmax - rb;  // rounds of this word the lane has
+            if (top < 15) v &= (1u << (2 * (top + 1))) - 1u;
+            w[l] = v;
+            c += sum2(v);
+            // rounds past jmax are in the lane region (it holds ceil(cap/4) + 64 records) and masked by w
+            const uint4* rp = reinterpret_cast<const uint4*>(raw[l] + rb);
+            rv[l][0] = rp[0];
+            rv[l][1] = rp[1];
         }
         uint32_t total;
-        uint32_t op = carry + block_exclusive_scan<NT>(c, s_warp, total);
-        carry += total;
-        if (rb < rounds) {
-            const uint32_t re = min(rounds, rb + 16);
-            for (uint32_t jr = rb; jr < re; jr++) {
-                const uint32_t sh = 2 * (jr & 15);
+        const uint32_t excl = block_exclusive_scan<NT>(c, s_warp, total);
+        uint8_t* dst = out + carry;
+        const uint32_t a = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15);
+        uint32_t q = a + excl;
 #pragma unroll
-                for (uint32_t l = 0; l < 4; l++) {
-                    const uint32_t k = (w[l] >> sh) & 3u;
-                    if (!k) continue;
-                    const uint32_t v = raw[l][jr];
-                    if (k == 2) { out[op] = (uint8_t)(v >> 8); out[op + 1] = (uint8_t)v; op += 2; }
-                    else { out[op] = (uint8_t)v; op += 1; }
+        for (int r = 0; r < 16; r++) {
+#pragma unroll
+            for (int l = 0; l < 4; l++) {
+                const uint32_t k = (w[l] >> (2 * r)) & 3u;
+                if (!k) continue;
+                const uint32_t v = rec16(rv[l], r);
+                if (k == 2) {
+                    s_stage[q] = (uint8_t)(v >> 8);
+                    s_stage[q + 1] = (uint8_t)v;
+                    q += 2;
+                } else {
+                    s_stage[q] = (uint8_t)v;
+                    q += 1;
                 }
             }
         }
+        __syncthreads();
+        uint8_t* g0 = dst - a;  // 16-byte aligned; only bytes [a, a + total) are written
+        const uint32_t end = a + total, nch = (end + 15) / 16;
+        for (uint32_t ch = tid; ch < nch; ch += NT) {
+            const uint32_t lo = ch * 16, hi = lo + 16;
+            if (lo >= a && hi <= end) {
+                *reinterpret_cast<uint4*>(g0 + lo) = *reinterpret_cast<const uint4*>(s_stage + lo);
+            } else {
+                for (uint32_t b = lo > a ? lo : a; b < (hi < end ? hi : end); b++) g0[b] = s_stage[b];
+            }
+        }
+        __syncthreads();  // the staging buffer is reused by the next pass
+        carry += total;
     }
 }
 

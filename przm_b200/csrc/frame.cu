@@ -100,8 +100,33 @@ __global__ void k_plan(const Job* __restrict__ jobs, uint32_t njobs, const uint3
 
 constexpr int kAsmThreads = 256;
 
+// Block-wide copy: byte stores up to the first 16-byte boundary of d, then
+// one aligned 16-byte store per thread per step (the source words are
+// loaded aligned and funnel-shifted into place), then the tail bytes.
+// Source buffers are padded, so reading up to 3 bytes past s + n is safe.
 __device__ void block_copy(uint8_t* __restrict__ d, const uint8_t* __restrict__ s, uint32_t n) {
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) d[i] = s[i];
+    const uint32_t head = min(n, (uint32_t)((16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15));
+    for (uint32_t i = threadIdx.x; i < head; i += blockDim.x) d[i] = s[i];
+    d += head;
+    s += head;
+    n -= head;
+    const uint32_t nv = n / 16;
+    const uint32_t so = (uint32_t)(reinterpret_cast<uintptr_t>(s) & 3);
+    const uint32_t* s4 = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(s) & ~uintptr_t(3));
+    uint4* d4 = reinterpret_cast<uint4*>(d);
+    for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) {
+        const uint32_t* p = s4 + 4 * v;
+        uint4 o;
+        if (so == 0) {
+            o = make_uint4(p[0], p[1], p[2], p[3]);
+        } else {
+            const uint32_t sh = 8 * so, w4 = p[4];
+            o = make_uint4(__funnelshift_r(p[0], p[1], sh), __funnelshift_r(p[1], p[2], sh),
+                           __funnelshift_r(p[2], p[3], sh), __funnelshift_r(p[3], w4, sh));
+        }
+        d4[v] = o;
+    }
+    for (uint32_t i = 16 * nv + threadIdx.x; i < n; i += blockDim.x) d[i] = s[i];
 }
 __device__ inline void put32(uint8_t* p, uint32_t v) {
     p[0] = (uint8_t)v; p[1] = (uint8_t)(v >> 8); p[2] = (uint8_t)(v >> 16); p[3] = (uint8_t)(v >> 24);
