@@ -108,10 +108,16 @@ struct przmg_batch {
     std::vector<TileRef> small;
     std::vector<uint32_t> big;
     std::vector<TokTile> tiles;
-    std::vector<uint64_t> in_offs, out_offs;
+    std::vector<uint64_t> in_offs, out_offs, up_offs;
     uint64_t in_bytes = 0, desc_words = 0, stream_bytes = 0, ans_bytes = 0, out_bytes = 0;
     DevBuf d_in, d_jobs, d_small, d_big, d_tiles, d_desc, d_slots, d_tile_lens, d_streams, d_job_lens, d_hist, d_tabs,
         d_infos, d_ans, d_outs, d_plans, d_sizes, d_out, d_misc, d_lists;
+    // radix-strike tables (one per finder CTA) and the packed upload/download
+    // staging belong to the batch, so batches on different streams never
+    // share scratch
+    DevBuf d_radix, d_tags, d_stage_in, d_stage_out, d_stage_offs, d_up_offs;
+    HostBuf h_offs;
+    uint32_t radix_ctas = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int launches = 0;
@@ -125,8 +131,10 @@ struct przmg_batch {
     void release() {
         DevBuf* all[] = {&d_in, &d_jobs, &d_small, &d_big, &d_tiles, &d_desc, &d_slots, &d_tile_lens, &d_streams,
                          &d_job_lens, &d_hist, &d_tabs, &d_infos, &d_ans, &d_outs, &d_plans, &d_sizes, &d_out, &d_misc,
-                         &d_lists};
+                         &d_lists, &d_radix, &d_tags, &d_stage_in, &d_stage_out, &d_stage_offs, &d_up_offs};
         for (DevBuf* b : all) b->release();
+        h_offs.release();
+        radix_ctas = 0;
     }
     uint32_t* err_word() const { return d_misc.as<uint32_t>(); }
     uint32_t* work_word() const { return d_misc.as<uint32_t>() + 1; }
@@ -138,22 +146,22 @@ struct Ctx {
     std::mutex mu;
     cudaDeviceProp prop{};
     int sms = 148;
-    DevBuf d_meta8, d_ctxlut, d_radix, d_tags;
-    uint32_t radix_ctas = 0;
+    DevBuf d_meta8, d_ctxlut;
     przmg_batch single;  // reused by the one-input calls
     HostBuf h_in, h_out, h_aux;
     DevBuf d_scr_in, d_scr_out, d_scr_aux, d_scr_tab;
     cudaEvent_t ev[8] = {};
 };
 
-static int32_t ensure_radix(Ctx* c) {
+static int32_t ensure_radix(przmg_batch* b) {
+    Ctx* c = b->ctx;
     const uint32_t want = 2 * (uint32_t)c->sms;
-    if (c->radix_ctas >= want) return PRZMG_OK;
-    CK(c->d_radix.ensure((size_t)want * kRadixBuckets * sizeof(uint64_t)));
-    CK(c->d_tags.ensure((size_t)want * sizeof(uint64_t)));
-    CK(cudaMemsetAsync(c->d_radix.p, 0, c->d_radix.cap, c->stream));
-    CK(cudaMemsetAsync(c->d_tags.p, 0, c->d_tags.cap, c->stream));
-    c->radix_ctas = want;
+    if (b->radix_ctas >= want) return PRZMG_OK;
+    CK(b->d_radix.ensure((size_t)want * kRadixBuckets * sizeof(uint64_t)));
+    CK(b->d_tags.ensure((size_t)want * sizeof(uint64_t)));
+    CK(cudaMemsetAsync(b->d_radix.p, 0, b->d_radix.cap, c->stream));
+    CK(cudaMemsetAsync(b->d_tags.p, 0, b->d_tags.cap, c->stream));
+    b->radix_ctas = want;
     return PRZMG_OK;
 }
 
@@ -233,7 +241,11 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     CK(b->d_out.ensure(b->out_bytes));
     CK(b->d_misc.ensure(64));
     CK(b->d_lists.ensure((size_t)2 * 4 * std::max<uint32_t>(njobs, 1) * 4 + 64));
+    CK(b->d_up_offs.ensure(8ull * std::max<uint32_t>(njobs, 1) + 64));
+    b->up_offs.assign(njobs, 0);
+    for (uint32_t i = 1; i < njobs; i++) b->up_offs[i] = b->up_offs[i - 1] + b->jobs[i - 1].n;
     cudaStream_t s = b->ctx->stream;
+    if (njobs) CK(cudaMemcpyAsync(b->d_up_offs.p, b->up_offs.data(), 8ull * njobs, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(b->d_jobs.p, b->jobs.data(), sizeof(Job) * njobs, cudaMemcpyHostToDevice, s));
     if (b->nsmall) CK(cudaMemcpyAsync(b->d_small.p, b->small.data(), sizeof(TileRef) * b->nsmall, cudaMemcpyHostToDevice, s));
     if (b->nbig) CK(cudaMemcpyAsync(b->d_big.p, b->big.data(), sizeof(uint32_t) * b->nbig, cudaMemcpyHostToDevice, s));
@@ -242,7 +254,7 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     CK(cudaMemsetAsync(b->d_sizes.p, 0, (size_t)njobs * 4 + 16, s));
     CK(cudaMemsetAsync(b->d_job_lens.p, 0, (size_t)njobs * S_COUNT * 4 + 16, s));
     if (b->nbig) {
-        int32_t r = ensure_radix(b->ctx);
+        int32_t r = ensure_radix(b);
         if (r) return r;
     }
     // the host-side vectors above must stay alive until the copies ran
@@ -273,10 +285,10 @@ static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cuda
     }
     CK(mark(1));
     if (b->nbig) {
-        const uint32_t grid = std::min<uint32_t>(b->nbig, c->radix_ctas);
+        const uint32_t grid = std::min<uint32_t>(b->nbig, b->radix_ctas);
         k_radix_find<<<grid, kRadixThreads, kRadixSmem, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(),
                                                               b->d_big.as<uint32_t>(), b->nbig, b->work_word(),
-                                                              c->d_radix.as<uint64_t>(), c->d_tags.as<uint64_t>(),
+                                                              b->d_radix.as<uint64_t>(), b->d_tags.as<uint64_t>(),
                                                               b->d_desc.as<uint32_t>());
         CK(cudaGetLastError());
         launches++;
@@ -419,7 +431,7 @@ extern "C" int32_t przmg_close(przmg_ctx* h) {
         cudaStreamSynchronize(c->stream);
         c->single.drop_graph();
         c->single.release();
-        DevBuf* bufs[] = {&c->d_meta8, &c->d_ctxlut, &c->d_radix, &c->d_tags, &c->d_scr_in, &c->d_scr_out, &c->d_scr_aux,
+        DevBuf* bufs[] = {&c->d_meta8, &c->d_ctxlut, &c->d_scr_in, &c->d_scr_out, &c->d_scr_aux,
                           &c->d_scr_tab};
         for (DevBuf* b : bufs) b->release();
         c->h_in.release();
@@ -944,17 +956,13 @@ __global__ void k_gather_frames(const uint8_t* __restrict__ out, const Job* __re
 static int32_t batch_upload_packed(przmg_batch* b, const uint8_t* host, cudaStream_t s) {
     Ctx* c = b->ctx;
     uint64_t total = 0;
-    std::vector<uint64_t> offs(b->njobs);
-    for (uint32_t i = 0; i < b->njobs; i++) { offs[i] = total; total += b->jobs[i].n; }
-    CK(c->d_scr_in.ensure(total + 64));
-    CK(c->d_scr_aux.ensure(8ull * b->njobs + 64));
-    CK(c->h_aux.ensure(8ull * b->njobs + 64));
-    std::memcpy(c->h_aux.p, offs.data(), 8ull * b->njobs);
-    if (total) CK(cudaMemcpyAsync(c->d_scr_in.p, host, total, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(c->d_scr_aux.p, c->h_aux.p, 8ull * b->njobs, cudaMemcpyHostToDevice, s));
+    for (uint32_t i = 0; i < b->njobs; i++) total += b->jobs[i].n;
+    CK(b->d_stage_in.ensure(total + 64));
+    if (total) CK(cudaMemcpyAsync(b->d_stage_in.p, host, total, cudaMemcpyHostToDevice, s));
     if (b->njobs) {
+        // b->d_up_offs holds the packed input offsets, written by batch_prepare
         k_scatter_inputs<<<dim3(64, std::min<uint32_t>(b->njobs, 4096)), 256, 0, s>>>(
-            c->d_scr_in.as<uint8_t>(), c->d_scr_aux.as<uint64_t>(), b->d_jobs.as<Job>(), b->njobs, b->d_in.as<uint8_t>());
+            b->d_stage_in.as<uint8_t>(), b->d_up_offs.as<uint64_t>(), b->d_jobs.as<Job>(), b->njobs, b->d_in.as<uint8_t>());
         CK(cudaGetLastError());
     }
     return PRZMG_OK;
@@ -975,18 +983,18 @@ static int32_t batch_download_packed(przmg_batch* b, uint8_t* host, uint64_t cap
     if (sizes) std::copy(fs.begin(), fs.end(), sizes);
     *total = t;
     if (t > cap) return fail(PRZMG_ERR_BUFFER_TOO_SMALL, "output buffer too small for the frames");
-    CK(c->d_scr_out.ensure(t + 64));
-    CK(c->d_scr_aux.ensure(8ull * b->njobs + 64));
-    CK(c->h_aux.ensure(8ull * b->njobs + 64));
-    std::memcpy(c->h_aux.p, offs.data(), 8ull * b->njobs);
-    CK(cudaMemcpyAsync(c->d_scr_aux.p, c->h_aux.p, 8ull * b->njobs, cudaMemcpyHostToDevice, s));
+    CK(b->d_stage_out.ensure(t + 64));
+    CK(b->d_stage_offs.ensure(8ull * b->njobs + 64));
+    CK(b->h_offs.ensure(8ull * b->njobs + 64));
+    std::memcpy(b->h_offs.p, offs.data(), 8ull * b->njobs);
+    CK(cudaMemcpyAsync(b->d_stage_offs.p, b->h_offs.p, 8ull * b->njobs, cudaMemcpyHostToDevice, s));
     if (b->njobs) {
         k_gather_frames<<<dim3(64, std::min<uint32_t>(b->njobs, 4096)), 256, 0, s>>>(
-            b->d_out.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_sizes.as<uint32_t>(), c->d_scr_aux.as<uint64_t>(), b->njobs,
-            c->d_scr_out.as<uint8_t>());
+            b->d_out.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_sizes.as<uint32_t>(), b->d_stage_offs.as<uint64_t>(), b->njobs,
+            b->d_stage_out.as<uint8_t>());
         CK(cudaGetLastError());
     }
-    if (t) CK(cudaMemcpyAsync(host, c->d_scr_out.p, t, cudaMemcpyDeviceToHost, s));
+    if (t) CK(cudaMemcpyAsync(host, b->d_stage_out.p, t, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return PRZMG_OK;
 }
