@@ -58,11 +58,45 @@ struct Emit {
         cmd_op(0xF0);
         cmd_varint(count);
     }
-    // copy count input bytes to the literal slot, spread over the lanes
+    // Literal bytes go to the literal slot in walk order.  Runs of up to 256
+    // bytes are copied one token late: each lane loads its 8 bytes now (two
+    // aligned words) and stores them at the next copy or at flush(), so the
+    // loads overlap the next token's descriptor search.  Longer runs are
+    // copied at once by the whole warp.  Source buffers are padded by 64
+    // bytes, so the aligned word loads never leave the input buffer.
+    uint32_t p_w0, p_w1, p_w2, p_sh, p_n;  // this lane's pending bytes: aligned words, byte shift, count
+    uint8_t* p_dst;
+    __device__ void flush() {
+        if (p_n) {
+            const uint32_t lo = p_sh ? __funnelshift_r(p_w0, p_w1, p_sh) : p_w0;
+            const uint32_t hi = p_sh ? __funnelshift_r(p_w1, p_w2, p_sh) : p_w1;
+            const uint64_t x = ((uint64_t)hi << 32) | lo;
+            for (uint32_t i = 0; i < p_n; i++) p_dst[i] = (uint8_t)(x >> (8 * i));
+        }
+        p_n = 0;
+    }
     __device__ void lits(const uint8_t* src, uint32_t count) {
+        if (count == 0) return;
         if (len[S_LIT] + count > kSlotLit) { ok = false; return; }
         uint8_t* d = base + slot_base(S_LIT) + len[S_LIT];
-        for (uint32_t i = lane; i < count; i += 32) d[i] = src[i];
+        flush();
+        if (count <= 256) {
+            const uint32_t o = 8 * lane;
+            if (o < count) {
+                const uintptr_t a = reinterpret_cast<uintptr_t>(src + o);
+                const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+                const uint32_t sh = (uint32_t)(a & 3) * 8;
+                // the 8 bytes at src + o; nothing here waits for the loads
+                p_w0 = __ldg(w);
+                p_w1 = __ldg(w + 1);
+                p_w2 = __ldg(w + 2);
+                p_sh = sh;
+                p_n = count - o < 8 ? count - o : 8;
+                p_dst = d + o;
+            }
+        } else {
+            for (uint32_t i = lane; i < count; i += 32) d[i] = src[i];
+        }
         len[S_LIT] += count;
     }
 };
@@ -127,6 +161,7 @@ __global__ void __launch_bounds__(256) k_tokenize(const uint8_t* __restrict__ in
         for (int s = 0; s < S_COUNT; s++) e.len[s] = 0;
         e.ok = true;
         e.lane = lane;
+        e.p_n = 0;
         int rep0 = tt.tile == 0 ? 1 : -1, rep1 = tt.tile == 0 ? 4 : -1, rep2 = tt.tile == 0 ? 8 : -1;
         uint32_t pos = start, litStart = start;
         auto dsc = [&](uint32_t q) -> uint32_t {
@@ -136,16 +171,23 @@ __global__ void __launch_bounds__(256) k_tokenize(const uint8_t* __restrict__ in
         };
         while (pos < end && e.ok) {
             // next position q >= pos holding a match descriptor (przm_tokenizer.cuh:170-194)
-            uint32_t q = 0xFFFFFFFFu, qd = 0;
+            // Each lane that sees a descriptor also loads the 4 source bytes
+            // at its position, so the run-length test below needs no second
+            // round trip to memory.
+            uint32_t q = 0xFFFFFFFFu, qd = 0, qw = 0, nd = 0;
             if (!radix) {
                 for (uint32_t w = pos; w < end; w += 32) {
                     uint32_t i = w + lane;
                     uint32_t v = i < end ? dj[i] : 0u;
+                    const uint32_t sw = v ? ld32_global_u(src + i) : 0u;
                     uint32_t m = __ballot_sync(0xFFFFFFFFu, v != 0);
                     if (m) {
                         int l = __ffs(m) - 1;
                         q = w + l;
                         qd = __shfl_sync(0xFFFFFFFFu, v, l);
+                        qw = __shfl_sync(0xFFFFFFFFu, sw, l);
+                        nd = __shfl_sync(0xFFFFFFFFu, v, (l + 1) & 31);  // descriptor at q + 1
+                        if (l == 31) nd = dsc(q + 1);
                         break;
                     }
                 }
@@ -154,51 +196,48 @@ __global__ void __launch_bounds__(256) k_tokenize(const uint8_t* __restrict__ in
                 for (uint32_t c = (pos + 7) >> 3; c < cend; c += 32) {
                     uint32_t i = c + lane;
                     uint32_t v = i < cend ? dj[i] : 0u;
+                    const uint32_t sw = v ? __ldg(reinterpret_cast<const uint32_t*>(src) + 2 * i) : 0u;
                     uint32_t m = __ballot_sync(0xFFFFFFFFu, v != 0);
                     if (m) {
                         int l = __ffs(m) - 1;
                         q = (c + l) * 8;
                         qd = __shfl_sync(0xFFFFFFFFu, v, l);
+                        qw = __shfl_sync(0xFFFFFFFFu, sw, l);
                         break;
                     }
                 }
+                // nd stays 0: q + 1 is never 8-aligned, so it has no descriptor
             }
             if (q >= end) break;
             uint32_t mLen = qd >> 20;
             const uint32_t d = qd & 0xFFFFFu;
             // lookahead (:196-216)
-            if (q + 1 < end) {
-                const uint32_t nd = dsc(q + 1);
-                if (nd != 0 && (nd >> 20) > mLen + 1) { pos = q + 1; continue; }
-            }
+            if (q + 1 < end && nd != 0 && (nd >> 20) > mLen + 1) { pos = q + 1; continue; }
             // run-length token (:218-286)
             if (q + 12 <= end) {
-                const uint32_t w4 = ld32_global_u(src + q);
-                const uint8_t b0 = (uint8_t)w4;
-                if (w4 == 0x01010101u * b0) {
+                const uint8_t b0 = (uint8_t)qw;
+                if (qw == 0x01010101u * b0) {
                     const uint32_t lim = q + min(end - q, 65535u);
                     const uint32_t r = warp_run_end(src, q + 4, lim, b0, lane) - q;
                     if (r >= 12 && r >= mLen) {
-                        if (q > litStart) {
-                            e.lit_op(q - litStart);
-                            e.lits(src + litStart, q - litStart);
-                        }
+                        if (q > litStart) e.lit_op(q - litStart);
                         e.cmd_op(0xF1);
                         e.cmd_varint(r);
-                        e.lits(src + q, 1);
+                        e.lits(src + litStart, q + 1 - litStart);  // pending literals, then the run byte
                         pos = q + r;
                         litStart = pos;
                         continue;
                     }
                 }
             }
-            // match (:289-320)
-            if (!(d > 0 && d <= q && mLen >= 4 && ld32_global_u(src + q) == ld32_global_u(src + q - d))) {
-                pos = q + 1;
-                continue;
-            }
+            // match (:289-320).  The reference re-checks d <= q, mLen >= 4 and
+            // the first 4 bytes here; every non-zero descriptor of both finders
+            // (k_tile_find, k_radix_find) already satisfies them.  Both finders
+            // also stop a match at its first mismatch unless it reached 4095
+            // bytes or the end of the data, so the forward extension can only
+            // continue a 4095-byte descriptor.
             if (q + mLen > end) mLen = end - q;
-            {
+            if (mLen >= kMaxLen32) {
                 const uint32_t lim = min(end - q, 65530u);
                 if (mLen < lim && src[q + mLen] == src[q - d + mLen])
                     mLen = warp_match_end(src, q, q - d, mLen, lim, lane);
@@ -209,11 +248,10 @@ __global__ void __launch_bounds__(256) k_tokenize(const uint8_t* __restrict__ in
             else if ((int)d == rep1 && rep1 > 0) k = 1;
             else if ((int)d == rep2 && rep2 > 0) k = 2;
             uint32_t litLen = q - litStart;
+            const uint32_t litAll = litLen;
             const uint32_t keep = k >= 0 ? (mLen <= 7 ? 7u : 15u) : 3u;
             if (litLen > keep) {
-                e.lit_op(litLen - keep);
-                e.lits(src + litStart, litLen - keep);
-                litStart = q - keep;
+                e.lit_op(litLen - keep);  // flushed literal op; its bytes go out with the rest below
                 litLen = keep;
             }
             const uint32_t base = mLen - 4 > 14 ? 15u : mLen - 4;
@@ -227,7 +265,7 @@ __global__ void __launch_bounds__(256) k_tokenize(const uint8_t* __restrict__ in
                 e.cmd_op((uint8_t)(0x80 | (litLen << 4) | base));
                 if (base == 15) e.cmd_varint(mLen - 19);
             }
-            e.lits(src + litStart, litLen);
+            e.lits(src + litStart, litAll);
             if (k < 0) {
                 e.off_varint(d);
                 rep2 = rep1; rep1 = rep0; rep0 = (int)d;
@@ -243,6 +281,7 @@ __global__ void __launch_bounds__(256) k_tokenize(const uint8_t* __restrict__ in
             e.lit_op(end - litStart);
             e.lits(src + litStart, end - litStart);
         }
+        e.flush();
         if (lane == 0) {
             for (int s = 0; s < S_COUNT; s++) tile_lens[S * S_COUNT + s] = e.len[s];
             if (!e.ok) atomicOr(err, (uint32_t)E_SLOT_OVERFLOW);
