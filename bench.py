@@ -170,6 +170,47 @@ def ncu_traffic() -> dict:
     return {}
 
 
+def gpu_local_cpus(dev: int) -> dict:
+    """Restricts this process to the CPUs local to the GPU (from sysfs), so
+    that pinned host buffers and the copy threads sit on the GPU's NUMA node."""
+    try:
+        import torch
+        p = torch.cuda.get_device_properties(dev)
+        bus = f"{p.pci_domain_id:04x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        base = f"/sys/bus/pci/devices/{bus}"
+        cpus = open(os.path.join(base, "local_cpulist")).read().strip()
+        node = open(os.path.join(base, "numa_node")).read().strip()
+        sel = set()
+        for part in cpus.split(","):
+            lo, _, hi = part.partition("-")
+            sel |= set(range(int(lo), int(hi or lo) + 1))
+        sel &= os.sched_getaffinity(0)
+        if sel:
+            os.sched_setaffinity(0, sel)
+        return {"pci": bus, "numa_node": node, "cpus": len(sel)}
+    except Exception as e:  # no sysfs entry: leave the affinity alone
+        return {"error": type(e).__name__}
+
+
+def link_gbs(hin, nbytes: int, dev_buf: int, stream) -> dict:
+    """Plain pinned H2D and D2H copy bandwidth of this box for `nbytes`."""
+    import ctypes
+    import torch
+    from przm_b200 import devmem
+    rt = devmem.rt()
+    out = {}
+    for name, kind in (("h2d", 1), ("d2h", 2)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        src, dst = (hin.ctypes.data, dev_buf) if kind == 1 else (dev_buf, hin.ctypes.data)
+        rt.cudaMemcpyAsync(ctypes.c_void_p(dst), ctypes.c_void_p(src), nbytes, kind, ctypes.c_void_p(stream.cuda_stream))
+        e1.record(stream)
+        e1.synchronize()
+        out[name] = round(nbytes / (e0.elapsed_time(e1) / 1e3) / 1e9, 2)
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -235,6 +276,7 @@ def main() -> None:
     from przm_b200 import gpu
     from przm_b200 import workloads as W
 
+    numa = gpu_local_cpus(local)  # pinned buffers below land on the GPU's NUMA node
     comp = gpu.GPUCompressor(local)
     frames = [W.mixture(s, FRAME)[0] for s in shard.frame_seeds(rank, args.frames)]
     sizes = [len(a) for a in frames]
@@ -336,6 +378,7 @@ def main() -> None:
         a1.synchronize()
         e2e_step = a0.elapsed_time(a1) / args.e2e_steps
     clk = clocks.stop()  # samples cover the device-timed and the end-to-end regions
+    link = link_gbs(hin, total, batch.d_out, stream)  # frames are no longer needed
     if pg:
         e2e_step = shard.max_over_ranks(e2e_step, pg, device=f"cuda:{local}")
 
@@ -397,7 +440,7 @@ def main() -> None:
                        "verified_frames": len(check) if verified else 0},
             "e2e": {"value": round(world * total / (e2e_step / 1e3) / 1e9, 3), "unit": "GB/s",
                     "h2d_bytes_per_step": total, "d2h_bytes_per_step": int(stats["frame_bytes"]) + 4 * args.frames,
-                    "ms_per_step": round(e2e_step, 3)},
+                    "ms_per_step": round(e2e_step, 3), "link_gbs": link, "host": numa},
             "roofline": roofline, "pipeline_roofline": pipeline, "stage_ms": {k: round(v, 3) for k, v in stages.items()},
             "cpu_baseline": cpu_base, "plain_per_frame": plain, "clocks": clk, "gpu_launches": gl,
         }

@@ -115,9 +115,10 @@ struct przmg_batch {
     // radix-strike tables (one per finder CTA) and the packed upload/download
     // staging belong to the batch, so batches on different streams never
     // share scratch
-    DevBuf d_radix, d_tags, d_stage_in, d_stage_out, d_stage_offs, d_up_offs;
+    DevBuf d_rtiles, d_rx_cnt, d_rx_parts, d_rx_ent, d_rx_key, d_rx_pred, d_stage_in, d_stage_out, d_stage_offs, d_up_offs;
     HostBuf h_offs;
-    uint32_t radix_ctas = 0;
+    std::vector<RxTile> rtiles;
+    uint64_t max_big_cand = 0;  // most radix candidates of one frame
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int launches = 0;
@@ -131,13 +132,12 @@ struct przmg_batch {
     void release() {
         DevBuf* all[] = {&d_in, &d_jobs, &d_small, &d_big, &d_tiles, &d_desc, &d_slots, &d_tile_lens, &d_streams,
                          &d_job_lens, &d_hist, &d_tabs, &d_infos, &d_ans, &d_outs, &d_plans, &d_sizes, &d_out, &d_misc,
-                         &d_lists, &d_radix, &d_tags, &d_stage_in, &d_stage_out, &d_stage_offs, &d_up_offs};
+                         &d_lists, &d_rtiles, &d_rx_cnt, &d_rx_parts, &d_rx_ent, &d_rx_key, &d_rx_pred, &d_stage_in,
+                         &d_stage_out, &d_stage_offs, &d_up_offs};
         for (DevBuf* b : all) b->release();
         h_offs.release();
-        radix_ctas = 0;
     }
     uint32_t* err_word() const { return d_misc.as<uint32_t>(); }
-    uint32_t* work_word() const { return d_misc.as<uint32_t>() + 1; }
 };
 
 struct Ctx {
@@ -153,18 +153,6 @@ struct Ctx {
     cudaEvent_t ev[8] = {};
 };
 
-static int32_t ensure_radix(przmg_batch* b) {
-    Ctx* c = b->ctx;
-    const uint32_t want = 2 * (uint32_t)c->sms;
-    if (b->radix_ctas >= want) return PRZMG_OK;
-    CK(b->d_radix.ensure((size_t)want * kRadixBuckets * sizeof(uint64_t)));
-    CK(b->d_tags.ensure((size_t)want * sizeof(uint64_t)));
-    CK(cudaMemsetAsync(b->d_radix.p, 0, b->d_radix.cap, c->stream));
-    CK(cudaMemsetAsync(b->d_tags.p, 0, b->d_tags.cap, c->stream));
-    b->radix_ctas = want;
-    return PRZMG_OK;
-}
-
 // Lay out a batch for the given input sizes; (re)allocates only when a
 // buffer is too small, so repeated calls of similar size reuse memory.
 static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njobs, int profile, bool force_radix) {
@@ -176,6 +164,8 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     b->small.clear();
     b->big.clear();
     b->tiles.clear();
+    b->rtiles.clear();
+    b->max_big_cand = 0;
     b->in_offs.assign(njobs, 0);
     b->out_offs.assign(njobs, 0);
     uint64_t in = 0, desc = 0, str = 0, ans = 0, out = 0;
@@ -207,8 +197,14 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
         b->out_offs[i] = out;
         out = align16(out + j.out_cap);
         if (n > 0) {
-            if (j.kind == 0) for (uint32_t t = 0; t < j.ntiles; t++) b->small.push_back({i, t});
-            else b->big.push_back(i);
+            if (j.kind == 0) {
+                for (uint32_t t = 0; t < j.ntiles; t++) b->small.push_back({i, t});
+            } else {
+                b->big.push_back(i);
+                b->max_big_cand = std::max<uint64_t>(b->max_big_cand, ncand);
+                const uint32_t nct = (uint32_t)((ncand + kCandPerTile - 1) / kCandPerTile);
+                for (uint32_t t = 0; t < nct; t++) b->rtiles.push_back({i, t});
+            }
             for (uint32_t t = 0; t < j.ntiles; t++) b->tiles.push_back({i, t});
         }
         tile0 += j.ntiles;
@@ -242,10 +238,20 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     CK(b->d_misc.ensure(64));
     CK(b->d_lists.ensure((size_t)2 * 4 * std::max<uint32_t>(njobs, 1) * 4 + 64));
     CK(b->d_up_offs.ensure(8ull * std::max<uint32_t>(njobs, 1) + 64));
+    if (b->nbig) {
+        CK(b->d_rtiles.ensure(sizeof(RxTile) * std::max<size_t>(b->rtiles.size(), 1)));
+        CK(b->d_rx_cnt.ensure((size_t)b->ntiles * kRxParts * 4 + 64));
+        CK(b->d_rx_parts.ensure((size_t)njobs * kRxParts * sizeof(uint2) + 64));
+        CK(b->d_rx_ent.ensure(b->desc_words * 4));
+        CK(b->d_rx_key.ensure(b->desc_words * 2));
+        CK(b->d_rx_pred.ensure(b->desc_words * 4));
+    }
     b->up_offs.assign(njobs, 0);
     for (uint32_t i = 1; i < njobs; i++) b->up_offs[i] = b->up_offs[i - 1] + b->jobs[i - 1].n;
     cudaStream_t s = b->ctx->stream;
     if (njobs) CK(cudaMemcpyAsync(b->d_up_offs.p, b->up_offs.data(), 8ull * njobs, cudaMemcpyHostToDevice, s));
+    if (!b->rtiles.empty())
+        CK(cudaMemcpyAsync(b->d_rtiles.p, b->rtiles.data(), sizeof(RxTile) * b->rtiles.size(), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(b->d_jobs.p, b->jobs.data(), sizeof(Job) * njobs, cudaMemcpyHostToDevice, s));
     if (b->nsmall) CK(cudaMemcpyAsync(b->d_small.p, b->small.data(), sizeof(TileRef) * b->nsmall, cudaMemcpyHostToDevice, s));
     if (b->nbig) CK(cudaMemcpyAsync(b->d_big.p, b->big.data(), sizeof(uint32_t) * b->nbig, cudaMemcpyHostToDevice, s));
@@ -253,10 +259,6 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
         CK(cudaMemcpyAsync(b->d_tiles.p, b->tiles.data(), sizeof(TokTile) * b->tiles.size(), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(b->d_sizes.p, 0, (size_t)njobs * 4 + 16, s));
     CK(cudaMemsetAsync(b->d_job_lens.p, 0, (size_t)njobs * S_COUNT * 4 + 16, s));
-    if (b->nbig) {
-        int32_t r = ensure_radix(b);
-        if (r) return r;
-    }
     // the host-side vectors above must stay alive until the copies ran
     CK(cudaStreamSynchronize(s));
     return PRZMG_OK;
@@ -284,14 +286,31 @@ static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cuda
         launches++;
     }
     CK(mark(1));
-    if (b->nbig) {
-        const uint32_t grid = std::min<uint32_t>(b->nbig, b->radix_ctas);
-        k_radix_find<<<grid, kRadixThreads, kRadixSmem, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(),
-                                                              b->d_big.as<uint32_t>(), b->nbig, b->work_word(),
-                                                              b->d_radix.as<uint64_t>(), b->d_tags.as<uint64_t>(),
-                                                              b->d_desc.as<uint32_t>());
+    if (b->nbig && !b->rtiles.empty()) {
+        const uint32_t nrt = (uint32_t)b->rtiles.size();
+        const uint32_t gt = std::min<uint32_t>(nrt, 16u * c->sms);
+        k_rx_count<<<gt, 256, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_rtiles.as<RxTile>(), nrt,
+                                      b->d_rx_cnt.as<uint32_t>());
         CK(cudaGetLastError());
-        launches++;
+        k_rx_scan<<<std::min<uint32_t>(b->nbig, 16u * c->sms), kRxParts, 0, s>>>(
+            b->d_jobs.as<Job>(), b->d_big.as<uint32_t>(), b->nbig, b->d_rx_cnt.as<uint32_t>(), b->d_rx_parts.as<uint2>());
+        CK(cudaGetLastError());
+        k_rx_scatter<<<gt, 256, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_rtiles.as<RxTile>(), nrt,
+                                        b->d_rx_cnt.as<uint32_t>(), b->d_rx_ent.as<uint32_t>(),
+                                        b->d_rx_key.as<uint16_t>());
+        CK(cudaGetLastError());
+        const uint32_t nwarps = b->nbig * kRxParts;
+        const uint32_t gr = std::min<uint32_t>((nwarps + kRxResolveWarps - 1) / kRxResolveWarps, 4u * c->sms);
+        k_rx_resolve<<<gr, kRxResolveWarps * 32, kRxResolveSmem, s>>>(
+            b->d_jobs.as<Job>(), b->d_big.as<uint32_t>(), b->nbig, b->d_rx_parts.as<uint2>(), b->d_rx_ent.as<uint32_t>(),
+            b->d_rx_key.as<uint16_t>(), b->d_rx_pred.as<uint32_t>());
+        CK(cudaGetLastError());
+        const uint32_t vx = std::max<uint32_t>(1, std::min<uint32_t>(64u, (uint32_t)((b->max_big_cand + 255) / 256)));
+        k_rx_verify<<<dim3(vx, std::min<uint32_t>(b->nbig, 65535u)), 256, 0, s>>>(
+            b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_big.as<uint32_t>(), b->d_rx_ent.as<uint32_t>(),
+            b->d_rx_pred.as<uint32_t>(), b->nbig, b->d_desc.as<uint32_t>());
+        CK(cudaGetLastError());
+        launches += 5;
     }
     CK(mark(2));
     if (stop_after >= 1 && !b->tiles.empty()) {
@@ -390,7 +409,7 @@ static int32_t ctx_setup(Ctx* c) {
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     for (auto& e : c->ev) CK(cudaEventCreate(&e));
     CK(cudaFuncSetAttribute(k_tile_find, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileFindSmem));
-    CK(cudaFuncSetAttribute(k_radix_find, cudaFuncAttributeMaxDynamicSharedMemorySize, kRadixSmem));
+    CK(cudaFuncSetAttribute(k_rx_resolve, cudaFuncAttributeMaxDynamicSharedMemorySize, kRxResolveSmem));
     CK(cudaFuncSetAttribute(k_rans, cudaFuncAttributeMaxDynamicSharedMemorySize, kRansSmem));
     CK(cudaFuncSetAttribute(k_stream_rans, cudaFuncAttributeMaxDynamicSharedMemorySize, kRansSmem));
     CK(c->d_meta8.ensure(8 * 256 * sizeof(EncSym)));
@@ -954,7 +973,6 @@ __global__ void k_gather_frames(const uint8_t* __restrict__ out, const Job* __re
 }
 
 static int32_t batch_upload_packed(przmg_batch* b, const uint8_t* host, cudaStream_t s) {
-    Ctx* c = b->ctx;
     uint64_t total = 0;
     for (uint32_t i = 0; i < b->njobs; i++) total += b->jobs[i].n;
     CK(b->d_stage_in.ensure(total + 64));
@@ -970,7 +988,6 @@ static int32_t batch_upload_packed(przmg_batch* b, const uint8_t* host, cudaStre
 
 static int32_t batch_download_packed(przmg_batch* b, uint8_t* host, uint64_t cap, uint64_t* total, uint32_t* sizes,
                                      cudaStream_t s) {
-    Ctx* c = b->ctx;
     std::vector<uint32_t> fs(b->njobs);
     if (b->njobs) CK(cudaMemcpyAsync(fs.data(), b->d_sizes.p, 4ull * b->njobs, cudaMemcpyDeviceToHost, s));
     uint32_t err = 0;

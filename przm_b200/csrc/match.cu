@@ -107,141 +107,249 @@ __global__ void __launch_bounds__(256) k_tile_find(const uint8_t* __restrict__ i
 }
 
 // ---------------------------------------------------------------------------
-// Radix-strike finder: one CTA per large frame (pulled from a work counter),
-// walking the frame's 8-aligned k-mer candidates 4096 at a time (one 32 KiB
-// tile).  Semantics of przm_lz77_radix_strike_kernel (przm_lz77.cu:156-213)
-// in sequential insertion order: the predecessor of candidate p is the latest
-// candidate q < p with the same 19-bit hash.  Inside a tile the predecessor
-// is resolved in shared memory (slot ids from a small hash, then one ordered
-// warp pass); across tiles it comes from the frame's 2^19-entry table in
-// global memory, whose entries carry a per-frame tag so it never needs
-// clearing.  Output: one descriptor per 8-aligned position (d8[p/8]).
+// Radix-strike finder, semantics of przm_lz77_radix_strike_kernel
+// (przm_lz77.cu:156-213) in sequential insertion order: candidate c (the
+// k-mer at byte 8c) takes as predecessor the latest candidate q < c with the
+// same 19-bit hash; the match is verified and extended against it.
+//
+// Candidates with equal hashes share the hash's top 8 bits, so each frame is
+// split into 256 partitions that never interact:
+//   k_rx_count   per 32 KiB tile (4096 candidates): candidates per partition;
+//   k_rx_scan    per frame: where each (tile, partition) run starts in the
+//                frame's partition-ordered candidate list;
+//   k_rx_scatter per tile: writes each candidate index (and its low 11 hash
+//                bits) to its slot, keeping position order inside a partition;
+//   k_rx_resolve one warp per (frame, partition): walks the partition's
+//                candidates in position order 32 at a time with a 2048-entry
+//                shared table of the latest candidate per low-11-bit key
+//                (ties inside the 32 resolved with __match_any_sync) and
+//                stores each candidate's predecessor next to it;
+//   k_rx_verify  one thread per candidate: verifies and extends the match
+//                against the predecessor and writes the descriptor.
+// Output: one descriptor per 8-aligned position (d8[c]), every candidate
+// written exactly once.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kRadixThreads = 512;
-constexpr uint32_t kSlotHash = 8192;
-constexpr uint32_t kRadixSmem = kSlotHash * 4 + kCandPerTile * 4 + 2 * kCandPerTile * 2 + kSlotHash * 2;
+constexpr uint32_t kRxKeyBits = 11;
+constexpr uint32_t kRxParts = 256;       // partitions: hash >> 11
+constexpr uint32_t kRxKeys = 2048;       // keys inside a partition: hash & 2047
+constexpr uint32_t kRxResolveWarps = 8;  // warps per k_rx_resolve block
+constexpr uint32_t kRxResolveSmem = kRxResolveWarps * kRxKeys * 4;
+
+struct RxTile { uint32_t job; uint32_t tile; };
 
 __device__ __forceinline__ uint32_t kmer_hash(uint64_t k) {
     return (uint32_t)((k * kRadixPrime) >> 43) & (kRadixBuckets - 1);
 }
+__host__ __device__ inline uint32_t rx_ncand(uint32_t n) { return n >= 8 ? (n - 8) / 8 + 1 : 0; }
 
-__global__ void __launch_bounds__(kRadixThreads) k_radix_find(const uint8_t* __restrict__ in,
-                                                              const Job* __restrict__ jobs,
-                                                              const uint32_t* __restrict__ big, uint32_t nbig,
-                                                              uint32_t* __restrict__ work, uint64_t* __restrict__ tables,
-                                                              uint64_t* __restrict__ tags, uint32_t* __restrict__ desc) {
-    extern __shared__ __align__(16) uint8_t smem_rf[];
-    uint32_t* s_key = reinterpret_cast<uint32_t*>(smem_rf);             // kSlotHash
-    uint32_t* s_h = s_key + kSlotHash;                                   // kCandPerTile
-    uint16_t* s_slot = reinterpret_cast<uint16_t*>(s_h + kCandPerTile);  // kCandPerTile
-    uint16_t* s_pred = s_slot + kCandPerTile;                            // kCandPerTile
-    uint16_t* s_last = s_pred + kCandPerTile;                            // kSlotHash
-    __shared__ uint32_t s_job;
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    uint64_t* table = tables + (uint64_t)blockIdx.x * kRadixBuckets;
-    uint64_t tag = tags[blockIdx.x];
-    for (;;) {
+__global__ void __launch_bounds__(256) k_rx_count(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
+                                                  const RxTile* __restrict__ rt, uint32_t nrt,
+                                                  uint32_t* __restrict__ cnt) {
+    __shared__ uint32_t s_cnt[kRxParts];
+    for (uint32_t T = blockIdx.x; T < nrt; T += gridDim.x) {
+        const RxTile tt = rt[T];
+        const Job job = jobs[tt.job];
+        const uint64_t* src = reinterpret_cast<const uint64_t*>(in + job.in_off);
+        const uint32_t C = rx_ncand(job.n), c0 = tt.tile * kCandPerTile, c1 = min(C, c0 + kCandPerTile);
         __syncthreads();
-        if (tid == 0) s_job = atomicAdd(work, 1u);
+        for (uint32_t i = threadIdx.x; i < kRxParts; i += 256) s_cnt[i] = 0;
         __syncthreads();
-        const uint32_t jx = s_job;
-        if (jx >= nbig) break;
-        tag++;
-        const Job job = jobs[big[jx]];
-        const uint8_t* src = in + job.in_off;
-        uint32_t* d8 = desc + job.desc_off;
-        const uint32_t n = job.n;
-        const uint32_t ncand_total = n >= 8 ? (n - 8) / 8 + 1 : 0;
-        for (uint32_t t0 = 0; t0 < ncand_total; t0 += kCandPerTile) {
-            const uint32_t nc = min(kCandPerTile, ncand_total - t0);
-            __syncthreads();
-            for (uint32_t i = tid; i < kSlotHash; i += kRadixThreads) { s_key[i] = 0; s_last[i] = 0xFFFFu; }
-            for (uint32_t c = tid; c < nc; c += kRadixThreads) {
-                uint64_t k = __ldg(reinterpret_cast<const uint64_t*>(src) + t0 + c);
-                s_h[c] = kmer_hash(k);
-            }
-            __syncthreads();
-            for (uint32_t c = tid; c < nc; c += kRadixThreads) {
-                const uint32_t key = s_h[c] + 1;
-                uint32_t sl = (key * 2654435761u) >> 19;  // 13-bit start slot
-                for (;;) {
-                    uint32_t prev = atomicCAS(&s_key[sl], 0u, key);
-                    if (prev == 0 || prev == key) break;
-                    sl = (sl + 1) & (kSlotHash - 1);
-                }
-                s_slot[c] = (uint16_t)sl;
-            }
-            __syncthreads();
-            if (warp == 0) {
-                for (uint32_t g = 0; g < nc; g += 32) {
-                    const uint32_t c = g + lane;
-                    const bool v = c < nc;
-                    const uint32_t act = __ballot_sync(0xFFFFFFFFu, v);
-                    const uint32_t sl = v ? s_slot[c] : 0xFFFFFFFFu;
-                    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, sl) & act;
-                    const uint32_t lower = peers & ((1u << lane) - 1u);
-                    uint32_t pred = 0xFFFFu;
-                    if (v) pred = lower ? g + (31 - __clz(lower)) : s_last[sl];
-                    __syncwarp();
-                    if (v) {
-                        s_pred[c] = (uint16_t)pred;
-                        if ((peers >> lane) == 1u) s_last[sl] = (uint16_t)c;
-                    }
-                    __syncwarp();
-                }
-            }
-            __syncthreads();
-            // resolve predecessors (table reads strictly before this tile's writes)
-            uint32_t prevs[kCandPerTile / kRadixThreads];
+        for (uint32_t c = c0 + threadIdx.x; c < c1; c += 256) atomicAdd(&s_cnt[kmer_hash(__ldg(src + c)) >> kRxKeyBits], 1u);
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < kRxParts; i += 256) cnt[(uint64_t)(job.tile0 + tt.tile) * kRxParts + i] = s_cnt[i];
+    }
+}
+
+// One block of kRxParts threads per large frame: thread b owns partition b.
+// Turns the per-tile counts into per-tile starting slots (in place) and
+// writes the partition's (start, length) pair.
+__global__ void __launch_bounds__(kRxParts) k_rx_scan(const Job* __restrict__ jobs, const uint32_t* __restrict__ big,
+                                                      uint32_t nbig, uint32_t* __restrict__ cnt,
+                                                      uint2* __restrict__ parts) {
+    __shared__ uint32_t s_warp[kRxParts / 32];
+    const uint32_t b = threadIdx.x, lane = b & 31, warp = b >> 5;
+    for (uint32_t x = blockIdx.x; x < nbig; x += gridDim.x) {
+        const uint32_t j = big[x];
+        const Job job = jobs[j];
+        const uint32_t nt = (rx_ncand(job.n) + kCandPerTile - 1) / kCandPerTile;
+        uint32_t* cj = cnt + (uint64_t)job.tile0 * kRxParts + b;
+        uint32_t total = 0;
+        for (uint32_t t = 0; t < nt; t++) total += cj[(uint64_t)t * kRxParts];
+        // exclusive scan of the partition totals
+        uint32_t v = total;
 #pragma unroll
-            for (uint32_t k = 0; k < kCandPerTile / kRadixThreads; k++) {
-                const uint32_t c = tid + k * kRadixThreads;
-                uint32_t pv = 0;  // candidate index + 1 of the predecessor, 0 = none
-                if (c < nc) {
-                    const uint32_t pr = s_pred[c];
-                    if (pr != 0xFFFFu) pv = t0 + pr + 1;
-                    else {
-                        const uint64_t e = table[s_h[c]];
-                        if ((e >> 32) == tag) pv = (uint32_t)e;
-                    }
-                }
-                prevs[k] = pv;
-            }
-            __syncthreads();
-            for (uint32_t c = tid; c < nc; c += kRadixThreads)
-                if (s_last[s_slot[c]] == c) table[s_h[c]] = (tag << 32) | (uint64_t)(t0 + c + 1);
-            // verify and extend (przm_lz77.cu:180-209); all loads are 8-aligned
-#pragma unroll
-            for (uint32_t k = 0; k < kCandPerTile / kRadixThreads; k++) {
-                const uint32_t c = tid + k * kRadixThreads;
-                if (c >= nc) continue;
-                uint32_t dsc = 0;
-                if (prevs[k]) {
-                    const uint32_t p = (t0 + c) * 8, q = (prevs[k] - 1) * 8;
-                    const uint32_t dist = p - q;
-                    if (dist <= kWindow && dist <= kMaxOff32) {
-                        const uint64_t* a = reinterpret_cast<const uint64_t*>(src + p);
-                        const uint64_t* b = reinterpret_cast<const uint64_t*>(src + q);
-                        if (__ldg(a) == __ldg(b)) {
-                            uint32_t L = 8;
-                            bool done = false;
-                            while ((uint64_t)p + L + 8 <= n && L + 8 <= kMaxLen32) {
-                                uint64_t x = __ldg(a + L / 8) ^ __ldg(b + L / 8);
-                                if (x) { L += (uint32_t)(__ffsll((long long)x) - 1) >> 3; done = true; break; }
-                                L += 8;
-                            }
-                            if (!done)
-                                while (p + L < n && src[p + L] == src[q + L] && L < kMaxLen32) L++;
-                            dsc = pack_match32(L, dist);
-                        }
-                    }
-                }
-                d8[t0 + c] = dsc;
-            }
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, v, o);
+            if (lane >= (uint32_t)o) v += y;
+        }
+        __syncthreads();
+        if (lane == 31) s_warp[warp] = v;
+        __syncthreads();
+        uint32_t start = v - total;
+        for (uint32_t w = 0; w < warp; w++) start += s_warp[w];
+        parts[(uint64_t)j * kRxParts + b] = make_uint2(start, total);
+        uint32_t run = start;
+        for (uint32_t t = 0; t < nt; t++) {
+            const uint32_t k = cj[(uint64_t)t * kRxParts];
+            cj[(uint64_t)t * kRxParts] = run;
+            run += k;
         }
     }
-    __syncthreads();
-    if (tid == 0) tags[blockIdx.x] = tag;
+}
+
+// 8 warps per tile, warp w taking candidates [c0 + 512w, c0 + 512w + 512)
+// in 16 rounds of 32; slots are assigned in position order.
+__global__ void __launch_bounds__(256) k_rx_scatter(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
+                                                    const RxTile* __restrict__ rt, uint32_t nrt,
+                                                    const uint32_t* __restrict__ off, uint32_t* __restrict__ ent,
+                                                    uint16_t* __restrict__ key) {
+    __shared__ uint32_t s_w[8][kRxParts];
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    for (uint32_t T = blockIdx.x; T < nrt; T += gridDim.x) {
+        const RxTile tt = rt[T];
+        const Job job = jobs[tt.job];
+        const uint64_t* src = reinterpret_cast<const uint64_t*>(in + job.in_off);
+        const uint32_t C = rx_ncand(job.n), c0 = tt.tile * kCandPerTile, c1 = min(C, c0 + kCandPerTile);
+        __syncthreads();
+        for (uint32_t i = tid; i < 8 * kRxParts; i += 256) (&s_w[0][0])[i] = 0;
+        __syncthreads();
+        uint32_t h[16];
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+            const uint32_t c = c0 + 512 * warp + 32 * r + lane;
+            h[r] = c < c1 ? kmer_hash(__ldg(src + c)) : 0xFFFFFFFFu;
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, h[r] >> kRxKeyBits);
+            if (h[r] != 0xFFFFFFFFu && (peers & lt) == 0) s_w[warp][h[r] >> kRxKeyBits] += __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        for (uint32_t pt = tid; pt < kRxParts; pt += 256) {
+            uint32_t base = off[(uint64_t)(job.tile0 + tt.tile) * kRxParts + pt];
+            for (int w = 0; w < 8; w++) {
+                const uint32_t k = s_w[w][pt];
+                s_w[w][pt] = base;
+                base += k;
+            }
+        }
+        __syncthreads();
+        uint32_t* ej = ent + job.desc_off;
+        uint16_t* kj = key + job.desc_off;
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+            const uint32_t c = c0 + 512 * warp + 32 * r + lane;
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, h[r] >> kRxKeyBits);
+            uint32_t slot = 0;
+            if (h[r] != 0xFFFFFFFFu) slot = s_w[warp][h[r] >> kRxKeyBits] + __popc(peers & lt);
+            __syncwarp();
+            if (h[r] != 0xFFFFFFFFu) {
+                if ((peers & lt) == 0) s_w[warp][h[r] >> kRxKeyBits] += __popc(peers);
+                ej[slot] = c;
+                kj[slot] = (uint16_t)(h[r] & (kRxKeys - 1));
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Verification and extension of candidate c against its predecessor q
+// (przm_lz77.cu:180-209): the match grows in 8-byte steps while
+// p + L + 8 <= n and L + 8 <= 4095, then byte by byte below 4095.  Four steps
+// are loaded per round trip (all loads 8-aligned; the input is padded by 64
+// bytes, so words past n are readable and only used where a step allows).
+__device__ __forceinline__ uint32_t rx_match(const uint8_t* src, uint32_t n, uint32_t c, uint32_t q) {
+    const uint32_t p = c * 8, pq = q * 8;
+    const uint32_t dist = p - pq;
+    if (dist > kWindow || dist > kMaxOff32) return 0;
+    const uint64_t* a = reinterpret_cast<const uint64_t*>(src + p);
+    const uint64_t* b = reinterpret_cast<const uint64_t*>(src + pq);
+    uint64_t x[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) x[k] = __ldg(a + k) ^ __ldg(b + k);
+    if (x[0]) return 0;
+    uint32_t L = 8;
+    int k0 = 1;
+    for (;;) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (k < k0) continue;
+            if (!((uint64_t)p + L + 8 <= n && L + 8 <= kMaxLen32)) goto bytes;
+            if (x[k]) return pack_match32(L + ((uint32_t)(__ffsll((long long)x[k]) - 1) >> 3), dist);
+            L += 8;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) x[k] = __ldg(a + L / 8 + k) ^ __ldg(b + L / 8 + k);
+        k0 = 0;
+    }
+bytes:
+    while (p + L < n && src[p + L] == src[pq + L] && L < kMaxLen32) L++;
+    return pack_match32(L, dist);
+}
+
+__global__ void __launch_bounds__(kRxResolveWarps * 32) k_rx_resolve(const Job* __restrict__ jobs,
+                                                                     const uint32_t* __restrict__ big, uint32_t nbig,
+                                                                     const uint2* __restrict__ parts,
+                                                                     const uint32_t* __restrict__ ent,
+                                                                     const uint16_t* __restrict__ key,
+                                                                     uint32_t* __restrict__ pred) {
+    extern __shared__ __align__(16) uint32_t smem_rx[];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t* table = smem_rx + warp * kRxKeys;  // latest candidate + 1 per key, 0 = none
+    const uint32_t nw = gridDim.x * kRxResolveWarps;
+    for (uint32_t x = blockIdx.x * kRxResolveWarps + warp; x < nbig * kRxParts; x += nw) {
+        const uint32_t j = big[x / kRxParts], b = x % kRxParts;
+        const Job job = jobs[j];
+        const uint2 pr = parts[(uint64_t)j * kRxParts + b];
+        if (pr.y == 0) continue;
+        for (uint32_t i = lane; i < kRxKeys / 4; i += 32) reinterpret_cast<uint4*>(table)[i] = make_uint4(0, 0, 0, 0);
+        __syncwarp();
+        const uint32_t* ej = ent + job.desc_off + pr.x;
+        const uint16_t* kj = key + job.desc_off + pr.x;
+        uint32_t* pj = pred + job.desc_off + pr.x;
+        // the next chunk's entries are loaded while this one resolves
+        uint32_t c = lane < pr.y ? ej[lane] : 0u;
+        uint32_t k = lane < pr.y ? kj[lane] : 0xFFFFu;
+        for (uint32_t i0 = 0; i0 < pr.y; i0 += 32) {
+            const uint32_t i = i0 + lane, inext = i + 32;
+            const uint32_t cn = inext < pr.y ? ej[inext] : 0u;
+            const uint32_t kn = inext < pr.y ? kj[inext] : 0xFFFFu;
+            const bool v = i < pr.y;
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, k);
+            const uint32_t lower = peers & lt;
+            const uint32_t from = lower ? 31u - __clz(lower) : lane;
+            const uint32_t cl = __shfl_sync(0xFFFFFFFFu, c, from);
+            uint32_t pv = 0;  // predecessor + 1
+            if (v) pv = lower ? cl + 1 : table[k];
+            __syncwarp();
+            if (v && (peers >> lane) == 1u) table[k] = c + 1;
+            __syncwarp();
+            if (v) pj[i] = pv;
+            c = cn;
+            k = kn;
+        }
+        __syncwarp();
+    }
+}
+
+// One thread per candidate of every large frame (grid.y = frame): verify and
+// extend against the resolved predecessor, write the descriptor.
+__global__ void __launch_bounds__(256) k_rx_verify(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
+                                                   const uint32_t* __restrict__ big, const uint32_t* __restrict__ ent,
+                                                   const uint32_t* __restrict__ pred, uint32_t nbig,
+                                                   uint32_t* __restrict__ desc) {
+    for (uint32_t y = blockIdx.y; y < nbig; y += gridDim.y) {
+        const Job job = jobs[big[y]];
+        const uint32_t C = rx_ncand(job.n);
+        const uint8_t* src = in + job.in_off;
+        const uint32_t* ej = ent + job.desc_off;
+        const uint32_t* pj = pred + job.desc_off;
+        uint32_t* d8 = desc + job.desc_off;
+        for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < C; i += gridDim.x * 256) {
+            const uint32_t c = ej[i], pv = pj[i];
+            d8[c] = pv ? rx_match(src, job.n, c, pv - 1) : 0u;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------

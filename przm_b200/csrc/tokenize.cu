@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(256) k_tokenize(const uint8_t* __restrict__ in
             }
             // match (:289-320).  The reference re-checks d <= q, mLen >= 4 and
             // the first 4 bytes here; every non-zero descriptor of both finders
-            // (k_tile_find, k_radix_find) already satisfies them.  Both finders
+            // (k_tile_find, k_rx_resolve) already satisfies them.  Both finders
             // also stop a match at its first mismatch unless it reached 4095
             // bytes or the end of the data, so the forward extension can only
             // continue a 4095-byte descriptor.
