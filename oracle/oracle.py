@@ -324,3 +324,40 @@ def ref_decode_meta8(container: bytes, n: int) -> bytes:
     if r != 0:
         raise ValueError(f"reference Meta8 decode error {r}")
     return bytes(out[:n])
+
+
+# --- the reference's own CUDA kernels (oracle/_ref/libprzm_ref_cuda.so) -----
+# Compiled from gpu/kernel/przm_lz77.cu with the host shim ref_cuda_shim.cu
+# (launch shapes of the Go bridge).  Arguments are raw device addresses; the
+# callers (GPU tests) own the buffers.  Buffer contracts, from the kernels:
+#   ref_histogram      d_hist 256 x u32, d_meta 4 x u32 (cleared first)
+#   ref_vans_encode4x  d_temp >= 2n + 64 bytes (the serial bit stream before
+#                      reversal), d_out >= 8 + mat_len + 16 + 2n + 64
+#   ref_tokenize       d_matches n x u32; per 32 KiB chunk 36864 bytes of
+#                      cmd/off/lit slot; d_lens 6 x chunks u32; d_totals 3 x
+#                      u32; all input reads stay below the tile end.
+
+_REFCUDA = None
+
+
+def ref_cuda_path() -> str:
+    return os.path.join(HERE, "_ref", "libprzm_ref_cuda.so")
+
+
+def ref_cuda_available() -> bool:
+    return os.path.exists(ref_cuda_path())
+
+
+def ref_cuda() -> C.CDLL:
+    global _REFCUDA
+    if _REFCUDA is None:
+        R = C.CDLL(ref_cuda_path())
+        vp, u32, u64 = C.c_void_p, C.c_uint32, C.c_uint64
+        R.ref_histogram.restype = C.c_int
+        R.ref_histogram.argtypes = [vp, u32, vp, vp, vp]
+        R.ref_vans_encode4x.restype = C.c_int
+        R.ref_vans_encode4x.argtypes = [vp, u32, vp, vp, vp, u32, vp, vp, vp, vp]
+        R.ref_tokenize.restype = C.c_int
+        R.ref_tokenize.argtypes = [vp, u64, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32, vp]
+        _REFCUDA = R
+    return _REFCUDA
