@@ -207,6 +207,34 @@ const char* przmg_stage_name(int32_t k);
 int32_t przmg_batch_stats(przmg_batch* b, uint64_t stats[8]);
 int32_t przmg_batch_destroy(przmg_batch* b);
 
+/* ---- serving: continuous batching (no reference counterpart; the reference
+ * has no request loop, the north-star serving pattern) ---------------------
+ * przmg_serve_create starts an engine on a context: up to max_inflight
+ * batches run at once, each on its own stream with its own resident device
+ * buffers, each laid out within mem_budget / max_inflight device bytes (and
+ * max_batch_bytes of input, 0 = no limit).  Requests are copied at submit;
+ * requests that arrive while batches run join the next batch.  A request's
+ * frame is byte-identical to a one-input przmg_compress of the same input and
+ * profile.  poll returns 1 when the frame is copied out (the request is then
+ * released), 0 while pending (wait = 0), < 0 on error; t_submit_ns/t_done_ns
+ * are steady-clock stamps of submission and of completion (frame on the
+ * host).  Status codes: PRZMG_ERR_BUSY (queue full), PRZMG_ERR_NOT_FOUND
+ * (unknown or released id), PRZMG_ERR_EXCEEDS_MAX_BLOCK (n >= 16 MiB for
+ * PRZMG_PROFILE_ANS), PRZMG_ERR_BUFFER_TOO_SMALL (dst smaller than the frame;
+ * the request stays pollable). */
+typedef struct przmg_server przmg_server;
+int32_t przmg_serve_create(przmg_ctx* ctx, int32_t profile, uint64_t mem_budget, int32_t max_inflight,
+                           uint64_t max_batch_bytes, przmg_server** out);
+int32_t przmg_serve_submit(przmg_server* s, const uint8_t* src, uint64_t n, uint64_t* id);
+int32_t przmg_serve_poll(przmg_server* s, uint64_t id, int32_t wait, uint8_t* dst, uint64_t cap, uint64_t* out_len,
+                         uint64_t* t_submit_ns, uint64_t* t_done_ns);
+/* stats[8]: batches launched, requests finished, input bytes, frame bytes,
+ * largest batch (requests), most batches in flight at once, requests pending,
+ * requests not yet polled */
+int32_t przmg_serve_stats(przmg_server* s, uint64_t stats[8]);
+/* finishes the batches in flight, then frees the engine */
+int32_t przmg_serve_destroy(przmg_server* s);
+
 /* ---- histogram / flat pack / V-ANS ------------------------------------- */
 /* ComputeHistogramGPU, gpu/bridge.go:2890 */
 int32_t przmg_compute_histogram_gpu(przmg_ctx* ctx, uint64_t d_in, uint64_t n, uint64_t stream, uint32_t counts[256],

@@ -7,8 +7,14 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/przmgpu.h"
@@ -155,7 +161,8 @@ struct Ctx {
 
 // Lay out a batch for the given input sizes; (re)allocates only when a
 // buffer is too small, so repeated calls of similar size reuse memory.
-static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njobs, int profile, bool force_radix) {
+static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njobs, int profile, bool force_radix,
+                             cudaStream_t setup = nullptr) {
     b->drop_graph();
     b->profile = profile;
     b->force_radix = force_radix;
@@ -248,7 +255,7 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     }
     b->up_offs.assign(njobs, 0);
     for (uint32_t i = 1; i < njobs; i++) b->up_offs[i] = b->up_offs[i - 1] + b->jobs[i - 1].n;
-    cudaStream_t s = b->ctx->stream;
+    cudaStream_t s = setup ? setup : b->ctx->stream;
     if (njobs) CK(cudaMemcpyAsync(b->d_up_offs.p, b->up_offs.data(), 8ull * njobs, cudaMemcpyHostToDevice, s));
     if (!b->rtiles.empty())
         CK(cudaMemcpyAsync(b->d_rtiles.p, b->rtiles.data(), sizeof(RxTile) * b->rtiles.size(), cudaMemcpyHostToDevice, s));
@@ -1243,6 +1250,11 @@ extern "C" int32_t przmg_match_lz77_streaming(przmg_ctx* h, const uint8_t* src, 
 // histogram / flat pack / V-ANS single-stream APIs and the stream batch
 // ---------------------------------------------------------------------------
 #include "api_streams.inc"
+
+// ---------------------------------------------------------------------------
+// serving: continuous batching of submitted requests
+// ---------------------------------------------------------------------------
+#include "serve.inc"
 
 // ---------------------------------------------------------------------------
 // allocation-free single-stream V-ANS (static device scratch)

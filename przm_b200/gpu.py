@@ -533,3 +533,44 @@ class DeviceBatch:
         if self._h:
             _check(L().przmg_batch_destroy(self._h))
         self._h = None
+
+
+class Server:
+    """Continuous-batching request engine over a compressor (przmg_serve_*):
+    submit inputs from any thread, poll for frames.  Up to `max_inflight`
+    batches run at once within `mem_budget` device bytes."""
+
+    def __init__(self, comp: GPUCompressor, profile: int = PROFILE_ANS, mem_budget: int = 64 << 30,
+                 max_inflight: int = 3, max_batch_bytes: int = 0):
+        h = C.c_void_p()
+        _check(L().przmg_serve_create(comp.handle, profile, mem_budget, max_inflight, max_batch_bytes, C.byref(h)))
+        self._h = h
+
+    def submit(self, src) -> int:
+        a = _u8(src)
+        rid = C.c_uint64()
+        _check(L().przmg_serve_submit(self._h, C.c_void_p(a.ctypes.data), len(a), C.byref(rid)))
+        return rid.value
+
+    def poll(self, rid: int, cap: int, wait: bool = True):
+        """(frame, t_submit_ns, t_done_ns), or None while pending (wait=False)."""
+        out = np.zeros(max(cap, 1), np.uint8)
+        n, t0, t1 = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        r = L().przmg_serve_poll(self._h, rid, 1 if wait else 0, C.c_void_p(out.ctypes.data), cap, C.byref(n),
+                                 C.byref(t0), C.byref(t1))
+        if r == 0:
+            return None
+        _check(r if r < 0 else 0)
+        return bytes(out[: n.value]), t0.value, t1.value
+
+    STAT_KEYS = ("batches", "done", "bytes_in", "bytes_out", "max_batch", "max_concurrent", "pending", "live")
+
+    def stats(self) -> dict[str, int]:
+        s = np.zeros(8, np.uint64)
+        _check(L().przmg_serve_stats(self._h, _ptr(s)))
+        return {k: int(v) for k, v in zip(self.STAT_KEYS, s)}
+
+    def close(self) -> None:
+        if self._h:
+            _check(L().przmg_serve_destroy(self._h))
+        self._h = None
