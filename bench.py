@@ -211,6 +211,35 @@ def link_gbs(hin, nbytes: int, dev_buf: int, stream) -> dict:
     return out
 
 
+def serve_measure(comp, count: int, fractions=(0.5,), seed: int = 0x50525A4D + 4) -> dict:
+    """Serving workload: `count` requests with log-normal sizes (median 64 KiB,
+    sigma 1.5, capped below 16 MiB) and mixed contents, through the
+    continuous-batching engine (64 GiB device budget, 3 batches in flight).
+    First all at once (saturation), then open-loop Poisson arrivals at the
+    given fractions of the saturated request rate.  Latency = the engine's
+    submit -> frame-on-host stamps."""
+    from przm_b200 import gpu, serving
+    from przm_b200 import workloads as W
+    sizes = W.config4_sizes(count)
+    inputs = [W.mixture(seed + 31 * i, int(s))[0] for i, s in enumerate(sizes)]
+    srv = gpu.Server(comp, gpu.PROFILE_ANS, mem_budget=64 << 30, max_inflight=3)
+    try:
+        serving.run_open_loop(srv, inputs[: min(200, count)], None)  # warm the slots' buffers
+        sat = serving.run_open_loop(srv, inputs, None)
+        rate_sat = count / sat["span_s"]
+        out = {"requests": count, "bytes": sat["bytes"], "budget_gib": 64, "inflight": 3,
+               "saturation": {"gbps": round(sat["gbps"], 3), "p50_ms": round(sat["p50_ms"], 3),
+                              "p99_ms": round(sat["p99_ms"], 3)}, "open_loop": []}
+        for f in fractions:
+            r = serving.run_open_loop(srv, inputs, f * rate_sat, seed=seed + int(1000 * f))
+            out["open_loop"].append({"load": f, "offered_gbps": round(r["offered_gbps"], 3), "gbps": round(r["gbps"], 3),
+                                     "p50_ms": round(r["p50_ms"], 3), "p99_ms": round(r["p99_ms"], 3)})
+        out["engine"] = srv.stats()
+    finally:
+        srv.close()
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -222,6 +251,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--frames", type=int, default=256, help="frames per GPU (smaller cases for profiling)")
     ap.add_argument("--inflight", type=int, default=3, help="batches in flight on separate streams")
+    ap.add_argument("--serve-requests", type=int, default=2000, help="requests of the serving measurement (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -392,6 +422,8 @@ def main() -> None:
         plain = {"frames": len(sub), "gbps_e2e": round(sum(len(a) for a in sub) / dt / 1e9, 3),
                  "identical_bytes": all(bytes(f) == O.compress_p1(a) for f, a in zip(fb[:2], sub[:2]))}
 
+    serve = serve_measure(comp, args.serve_requests) if args.serve_requests > 0 and rank == 0 else None
+
     # roofline of the dominant kernel
     peak, peak_kind = measured_peaks()
     dom = max(stages, key=stages.get)
@@ -443,6 +475,7 @@ def main() -> None:
                     "ms_per_step": round(e2e_step, 3), "link_gbs": link, "host": numa},
             "roofline": roofline, "pipeline_roofline": pipeline, "stage_ms": {k: round(v, 3) for k, v in stages.items()},
             "cpu_baseline": cpu_base, "plain_per_frame": plain, "clocks": clk, "gpu_launches": gl,
+            "serving": serve,
         }
         print(json.dumps(line), flush=True)
     for bt in batches:

@@ -212,7 +212,7 @@ int32_t przmg_batch_destroy(przmg_batch* b);
  * przmg_serve_create starts an engine on a context: up to max_inflight
  * batches run at once, each on its own stream with its own resident device
  * buffers, each laid out within mem_budget / max_inflight device bytes (and
- * max_batch_bytes of input, 0 = no limit).  Requests are copied at submit;
+ * max_batch_bytes of input, 0 = 256 MiB).  Requests are copied at submit;
  * requests that arrive while batches run join the next batch.  A request's
  * frame is byte-identical to a one-input przmg_compress of the same input and
  * profile.  poll returns 1 when the frame is copied out (the request is then

@@ -60,8 +60,10 @@ struct DevBuf {
         if (bytes <= cap && p) return cudaSuccess;
         if (p) cudaFree(p);
         p = nullptr;
+        // geometric growth: a buffer that keeps growing is reallocated
+        // O(log) times (cudaFree synchronises the device)
+        size_t want = std::max(bytes + bytes / 8, cap + cap / 2) + 4096;
         cap = 0;
-        size_t want = bytes + bytes / 8 + 4096;
         cudaError_t e = cudaMalloc(&p, want);
         if (e == cudaSuccess) cap = want;
         return e;
@@ -81,8 +83,8 @@ struct HostBuf {
         if (bytes <= cap && p) return cudaSuccess;
         if (p) cudaFreeHost(p);
         p = nullptr;
+        size_t want = std::max(bytes + bytes / 8, cap + cap / 2) + 4096;  // pinning is slow: grow geometrically
         cap = 0;
-        size_t want = bytes + bytes / 8 + 4096;
         cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
         if (e == cudaSuccess) cap = want;
         return e;
