@@ -324,7 +324,7 @@ static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cuda
     CK(mark(2));
     if (stop_after >= 1 && !b->tiles.empty()) {
         const uint32_t nt = (uint32_t)b->tiles.size();
-        k_tokenize<<<(nt + 7) / 8, 256, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_tiles.as<TokTile>(), nt,
+        k_tokenize<<<(nt + kTokWarps - 1) / kTokWarps, kTokWarps * 32, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_tiles.as<TokTile>(), nt,
                                                b->d_desc.as<uint32_t>(), b->d_slots.as<uint8_t>(),
                                                b->d_tile_lens.as<uint32_t>(), b->err_word());
         CK(cudaGetLastError());

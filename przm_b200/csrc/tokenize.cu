@@ -29,78 +29,6 @@ __host__ __device__ inline uint32_t slot_cap(int s) { return s == S_OFF ? kSlotO
 
 struct TokTile { uint32_t job; uint32_t tile; };
 
-// Warp-uniform emitter for one tile: all lanes keep the same lengths, lane 0
-// stores the bytes.
-struct Emit {
-    uint8_t* base;  // this tile's slot block
-    uint32_t len[S_COUNT];
-    bool ok;
-    uint32_t lane;
-    __device__ void put(int s, uint8_t b) {
-        if (len[s] >= slot_cap(s)) { ok = false; return; }
-        if (lane == 0) base[slot_base(s) + len[s]] = b;
-        len[s]++;
-    }
-    __device__ void cmd_op(uint8_t b) { put(S_CMD, b); put(S_OP, b); }   // opcode byte
-    __device__ void cmd_meta(uint8_t b) { put(S_CMD, b); put(S_META, b); }
-    __device__ void cmd_varint(uint32_t v) {                              // przm_tokenizer.cuh:33-55
-        while (v >= 0x80) { put(S_CMD, (uint8_t)(v | 0x80)); put(S_VAR, (uint8_t)(v | 0x80)); v >>= 7; }
-        put(S_CMD, (uint8_t)v);
-        put(S_VAR, (uint8_t)v);
-    }
-    __device__ void off_varint(uint32_t v) {
-        while (v >= 0x80) { put(S_OFF, (uint8_t)(v | 0x80)); v >>= 7; }
-        put(S_OFF, (uint8_t)v);
-    }
-    __device__ void lit_op(uint32_t count) {                              // przm_tokenizer.cuh:57-76
-        if (count == 0) return;
-        if (count <= 8) { cmd_op((uint8_t)(0xF2 + count)); return; }
-        cmd_op(0xF0);
-        cmd_varint(count);
-    }
-    // Literal bytes go to the literal slot in walk order.  Runs of up to 256
-    // bytes are copied one token late: each lane loads its 8 bytes now (two
-    // aligned words) and stores them at the next copy or at flush(), so the
-    // loads overlap the next token's descriptor search.  Longer runs are
-    // copied at once by the whole warp.  Source buffers are padded by 64
-    // bytes, so the aligned word loads never leave the input buffer.
-    uint32_t p_w0, p_w1, p_w2, p_sh, p_n;  // this lane's pending bytes: aligned words, byte shift, count
-    uint8_t* p_dst;
-    __device__ void flush() {
-        if (p_n) {
-            const uint32_t lo = p_sh ? __funnelshift_r(p_w0, p_w1, p_sh) : p_w0;
-            const uint32_t hi = p_sh ? __funnelshift_r(p_w1, p_w2, p_sh) : p_w1;
-            const uint64_t x = ((uint64_t)hi << 32) | lo;
-            for (uint32_t i = 0; i < p_n; i++) p_dst[i] = (uint8_t)(x >> (8 * i));
-        }
-        p_n = 0;
-    }
-    __device__ void lits(const uint8_t* src, uint32_t count) {
-        if (count == 0) return;
-        if (len[S_LIT] + count > kSlotLit) { ok = false; return; }
-        uint8_t* d = base + slot_base(S_LIT) + len[S_LIT];
-        flush();
-        if (count <= 256) {
-            const uint32_t o = 8 * lane;
-            if (o < count) {
-                const uintptr_t a = reinterpret_cast<uintptr_t>(src + o);
-                const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
-                const uint32_t sh = (uint32_t)(a & 3) * 8;
-                // the 8 bytes at src + o; nothing here waits for the loads
-                p_w0 = __ldg(w);
-                p_w1 = __ldg(w + 1);
-                p_w2 = __ldg(w + 2);
-                p_sh = sh;
-                p_n = count - o < 8 ? count - o : 8;
-                p_dst = d + o;
-            }
-        } else {
-            for (uint32_t i = lane; i < count; i += 32) d[i] = src[i];
-        }
-        len[S_LIT] += count;
-    }
-};
-
 // First index i in [from, lim) with src[i] != b (or lim), lanes in parallel.
 __device__ uint32_t warp_run_end(const uint8_t* src, uint32_t from, uint32_t lim, uint8_t b, uint32_t lane) {
     const uint64_t rep = 0x0101010101010101ull * b;
@@ -139,13 +67,182 @@ __device__ uint32_t warp_match_end(const uint8_t* src, uint32_t a, uint32_t b, u
     return lim;
 }
 
-__global__ void __launch_bounds__(256) k_tokenize(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
-                                                  const TokTile* __restrict__ tiles, uint32_t ntiles,
-                                                  const uint32_t* __restrict__ desc, uint8_t* __restrict__ slots,
-                                                  uint32_t* __restrict__ tile_lens, uint32_t* __restrict__ err) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+// ---------------------------------------------------------------------------
+// Tokenizer, in two phases per tile (one warp per 32 KiB tile).
+//
+// Walk.  The greedy parse is serial: each decision fixes where the next one
+// starts.  It runs over a shared window of kTokWin match descriptors
+// (radix frames: 8-aligned candidates; small frames: every position), with
+// two bitmaps of the window in registers -- lane l holds the bits of entries
+// [32l, 32l + 32) -- one marking non-zero descriptors, one marking positions
+// whose 4 bytes are equal (the run-length test).  Finding the next
+// descriptor is a ballot over those registers; only run-length scans and
+// the extension of 4095-byte matches read global memory.  Every decision
+// becomes a 12-byte record in shared memory:
+//   r0 = q - tile start | literals before q << 16
+//   r1 = match or run length | kind << 16 | repeat slot << 18
+//   r2 = offset
+// kinds: 0 explicit match, 1 repeat match, 2 run-length, 3 trailing literals.
+// Emit.  Every kTokRec records (and at the end of the tile) the warp writes
+// them out, 32 at a time: each lane turns one record into its bytes for the
+// command, op, meta, var and offset streams (encodings of
+// przm_tokenizer.cuh:57-76,329-426; Mode 8 split of commands.go:18-202),
+// warp prefix sums give every lane its offsets, and the records' literal
+// runs are copied by all lanes together.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kTokWin = 1024;   // descriptor window entries
+constexpr uint32_t kTokRec = 256;    // records buffered before emission
+constexpr uint32_t kTokWarps = 4;    // warps (tiles) per block
+
+struct TokSmem {
+    uint32_t desc[kTokWin];
+    uint32_t rec[kTokRec][3];
+};
+
+__device__ __forceinline__ uint32_t vlen(uint32_t v) { return v < 0x80u ? 1u : v < 0x4000u ? 2u : v < 0x200000u ? 3u : v < 0x10000000u ? 4u : 5u; }
+
+__device__ __forceinline__ uint32_t put_varint(uint8_t* d, uint32_t v) {  // przm_tokenizer.cuh:33-55
+    uint32_t k = 0;
+    while (v >= 0x80u) { d[k++] = (uint8_t)(v | 0x80u); v >>= 7; }
+    d[k++] = (uint8_t)v;
+    return k;
+}
+
+// Inclusive warp prefix sum.
+__device__ __forceinline__ uint32_t warp_incl(uint32_t v, uint32_t lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, v, o);
+        if (lane >= (uint32_t)o) v += y;
+    }
+    return v;
+}
+
+struct TokTileOut {
+    uint8_t* base;          // the tile's slot block
+    uint32_t len[S_COUNT];  // bytes written per stream (warp-uniform)
+    bool ok;
+};
+
+// Writes records [0, nrec) of the warp's buffer.
+__device__ void tok_emit(const uint32_t (*rec)[3], uint32_t nrec, const uint8_t* tile_src, TokTileOut& o,
+                         uint32_t lane) {
+    for (uint32_t g = 0; g < nrec; g += 32) {
+        const uint32_t i = g + lane;
+        const bool v = i < nrec;
+        uint32_t r0 = 0, r1 = 0, r2 = 0;
+        if (v) { r0 = rec[i][0]; r1 = rec[i][1]; r2 = rec[i][2]; }
+        const uint32_t q = r0 & 0xFFFFu, lit = r0 >> 16, len = r1 & 0xFFFFu, kind = (r1 >> 16) & 3u, k = r1 >> 18;
+        // literal-op count, op byte and the rest, per record kind
+        uint32_t flush = 0, litLen = 0, base = 0;
+        if (kind <= 1) {
+            const uint32_t keep = kind == 1 ? (len <= 7 ? 7u : 15u) : 3u;
+            flush = lit > keep ? lit - keep : 0u;
+            litLen = lit - flush;
+            base = len - 4 > 14 ? 15u : len - 4;
+        } else {
+            flush = lit;
+        }
+        const uint32_t lop = flush == 0 ? 0u : (flush <= 8 ? 1u : 1u + vlen(flush));  // literal-op bytes
+        const uint32_t lvar = flush > 8 ? vlen(flush) : 0u;
+        const bool rep_long = kind == 1 && len > 7;
+        const bool tail_var = (kind == 0 || rep_long) && base == 15;
+        uint32_t c[S_COUNT] = {0, 0, 0, 0, 0, 0};
+        if (v) {
+            c[S_OP] = (flush ? 1u : 0u) + (kind <= 2 ? 1u : 0u);
+            c[S_META] = rep_long ? 1u : 0u;
+            c[S_VAR] = lvar + (tail_var ? vlen(len - 19) : 0u) + (kind == 2 ? vlen(len) : 0u);
+            c[S_CMD] = lop + (kind <= 2 ? 1u : 0u) + c[S_META] + (c[S_VAR] - lvar);
+            c[S_OFF] = kind == 0 ? vlen(r2) : 0u;
+            c[S_LIT] = lit + (kind == 2 ? 1u : 0u);
+        }
+        uint32_t off[S_COUNT], tot[S_COUNT];
+#pragma unroll
+        for (int s = 0; s < S_COUNT; s++) {
+            const uint32_t inc = warp_incl(c[s], lane);
+            tot[s] = __shfl_sync(0xFFFFFFFFu, inc, 31);
+            off[s] = o.len[s] + inc - c[s];
+        }
+        bool fits = o.ok;
+#pragma unroll
+        for (int s = 0; s < S_COUNT; s++) fits = fits && o.len[s] + tot[s] <= slot_cap(s);
+        if (!fits) {
+            o.ok = false;
+            return;
+        }
+        if (v) {
+            uint8_t* cmd = o.base + slot_base(S_CMD) + off[S_CMD];
+            uint8_t* op = o.base + slot_base(S_OP) + off[S_OP];
+            uint8_t* var = o.base + slot_base(S_VAR) + off[S_VAR];
+            if (flush) {
+                const uint8_t b = flush <= 8 ? (uint8_t)(0xF2u + flush) : (uint8_t)0xF0u;
+                *cmd++ = b;
+                *op++ = b;
+                if (flush > 8) {
+                    const uint32_t n = put_varint(cmd, flush);
+                    put_varint(var, flush);
+                    cmd += n;
+                    var += n;
+                }
+            }
+            if (kind == 2) {
+                *cmd++ = 0xF1u;
+                *op = 0xF1u;
+                put_varint(cmd, len);
+                put_varint(var, len);
+            } else if (kind == 1 && len <= 7) {
+                const uint8_t b = (uint8_t)((litLen << 4) | ((len - 4) << 2) | k);
+                *cmd = b;
+                *op = b;
+            } else if (kind <= 1) {
+                const uint8_t b = kind == 1 ? (uint8_t)(0xC0u | k) : (uint8_t)(0x80u | (litLen << 4) | base);
+                *cmd++ = b;
+                *op = b;
+                if (kind == 1) {
+                    const uint8_t t = (uint8_t)((litLen << 4) | base);
+                    *cmd++ = t;
+                    o.base[slot_base(S_META) + off[S_META]] = t;
+                }
+                if (base == 15) {
+                    put_varint(cmd, len - 19);
+                    put_varint(var, len - 19);
+                }
+                if (kind == 0) put_varint(o.base + slot_base(S_OFF) + off[S_OFF], r2);
+            }
+        }
+        // literal runs of these records, all lanes over the concatenated bytes
+        {
+            const uint32_t incl = warp_incl(c[S_LIT], lane), tl = tot[S_LIT];
+            const uint32_t from = q - lit;  // first literal of this record, tile-relative
+            uint8_t* dl = o.base + slot_base(S_LIT) + o.len[S_LIT];
+            for (uint32_t b0 = 0; b0 < tl; b0 += 32) {  // warp-uniform trip count: every lane shuffles
+                const uint32_t b = b0 + lane;
+                // record j with incl[j-1] <= b < incl[j]
+                uint32_t j = 0;
+#pragma unroll
+                for (int st = 16; st >= 1; st >>= 1) {
+                    const uint32_t x = __shfl_sync(0xFFFFFFFFu, incl, j + st - 1);
+                    if (x <= b) j += st;
+                }
+                const uint32_t ex = __shfl_sync(0xFFFFFFFFu, incl, j ? j - 1 : 0);
+                const uint32_t f = __shfl_sync(0xFFFFFFFFu, from, j & 31);
+                if (b < tl) dl[b] = tile_src[f + (b - (j ? ex : 0u))];
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < S_COUNT; s++) o.len[s] += tot[s];
+    }
+}
+
+__global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
+                                                            const TokTile* __restrict__ tiles, uint32_t ntiles,
+                                                            const uint32_t* __restrict__ desc, uint8_t* __restrict__ slots,
+                                                            uint32_t* __restrict__ tile_lens, uint32_t* __restrict__ err) {
+    __shared__ TokSmem s_tok[kTokWarps];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    TokSmem& sm = s_tok[warp];
+    const uint32_t wid = blockIdx.x * kTokWarps + warp;
+    const uint32_t nw = gridDim.x * kTokWarps;
     for (uint32_t T = wid; T < ntiles; T += nw) {
         const TokTile tt = tiles[T];
         const Job job = jobs[tt.job];
@@ -155,84 +252,111 @@ __global__ void __launch_bounds__(256) k_tokenize(const uint8_t* __restrict__ in
         const uint32_t end = min(start + kTile, job.n);
         const bool radix = job.kind != 0;
         const uint32_t ncand = job.n >= 8 ? (job.n - 8) / 8 + 1 : 0;
-        const uint64_t S = (uint64_t)job.tile0 + tt.tile;  // slot of this tile
-        Emit e;
-        e.base = slots + S * kSlotStride;
-        for (int s = 0; s < S_COUNT; s++) e.len[s] = 0;
-        e.ok = true;
-        e.lane = lane;
-        e.p_n = 0;
+        // descriptor index space of this tile ends at e_hi
+        const uint32_t e_hi = radix ? min(ncand, (end + 7) >> 3) : end;
+        const uint64_t S = (uint64_t)job.tile0 + tt.tile;
+        TokTileOut o;
+        o.base = slots + S * kSlotStride;
+        for (int s = 0; s < S_COUNT; s++) o.len[s] = 0;
+        o.ok = true;
         int rep0 = tt.tile == 0 ? 1 : -1, rep1 = tt.tile == 0 ? 4 : -1, rep2 = tt.tile == 0 ? 8 : -1;
-        uint32_t pos = start, litStart = start;
-        auto dsc = [&](uint32_t q) -> uint32_t {
-            if (q >= end) return 0u;
-            if (!radix) return dj[q];
-            return ((q & 7) == 0 && (q >> 3) < ncand) ? dj[q >> 3] : 0u;
-        };
-        while (pos < end && e.ok) {
-            // next position q >= pos holding a match descriptor (przm_tokenizer.cuh:170-194)
-            // Each lane that sees a descriptor also loads the 4 source bytes
-            // at its position, so the run-length test below needs no second
-            // round trip to memory.
-            uint32_t q = 0xFFFFFFFFu, qd = 0, qw = 0, nd = 0;
-            if (!radix) {
-                for (uint32_t w = pos; w < end; w += 32) {
-                    uint32_t i = w + lane;
-                    uint32_t v = i < end ? dj[i] : 0u;
-                    const uint32_t sw = v ? ld32_global_u(src + i) : 0u;
-                    uint32_t m = __ballot_sync(0xFFFFFFFFu, v != 0);
-                    if (m) {
-                        int l = __ffs(m) - 1;
-                        q = w + l;
-                        qd = __shfl_sync(0xFFFFFFFFu, v, l);
-                        qw = __shfl_sync(0xFFFFFFFFu, sw, l);
-                        nd = __shfl_sync(0xFFFFFFFFu, v, (l + 1) & 31);  // descriptor at q + 1
-                        if (l == 31) nd = dsc(q + 1);
-                        break;
-                    }
-                }
-            } else {
-                const uint32_t cend = min(ncand, (end + 7) >> 3);
-                for (uint32_t c = (pos + 7) >> 3; c < cend; c += 32) {
-                    uint32_t i = c + lane;
-                    uint32_t v = i < cend ? dj[i] : 0u;
-                    const uint32_t sw = v ? __ldg(reinterpret_cast<const uint32_t*>(src) + 2 * i) : 0u;
-                    uint32_t m = __ballot_sync(0xFFFFFFFFu, v != 0);
-                    if (m) {
-                        int l = __ffs(m) - 1;
-                        q = (c + l) * 8;
-                        qd = __shfl_sync(0xFFFFFFFFu, v, l);
-                        qw = __shfl_sync(0xFFFFFFFFu, sw, l);
-                        break;
-                    }
-                }
-                // nd stays 0: q + 1 is never 8-aligned, so it has no descriptor
+        uint32_t pos = start, litStart = start, nrec = 0;
+        uint32_t wb = 0xFFFFFFFFu, nzw = 0, eqw = 0;  // window base entry, this lane's bitmap words
+        auto refill = [&](uint32_t base) {
+            // entries [base, base + kTokWin): descriptors to shared memory, bitmaps to registers
+            __syncwarp();
+            wb = base;
+            const uint32_t e0 = base + 32 * lane;
+            uint32_t nz = 0, eq = 0;
+#pragma unroll 4
+            for (uint32_t k = 0; k < 32; k++) {
+                const uint32_t e = e0 + k;
+                const uint32_t v = e < e_hi ? __ldg(dj + e) : 0u;
+                sm.desc[32 * lane + k] = v;
+                nz |= (v != 0 ? 1u : 0u) << k;
             }
+            if (nz) {  // equal-4-byte bits of the lane's 32 entries, from vector loads
+                if (radix) {
+                    // candidate e0 + k starts at byte 8(e0 + k); uint4 i covers candidates
+                    // e0 + 2i and e0 + 2i + 1 (loaded only below e_hi, so 8 e_hi + 8 <= n + 8)
+                    const uint4* s4 = reinterpret_cast<const uint4*>(src + 8ull * e0);
+#pragma unroll
+                    for (uint32_t i = 0; i < 16; i++) {
+                        if (e0 + 2 * i >= e_hi) break;
+                        const uint4 v = __ldg(s4 + i);
+                        eq |= (v.x == 0x01010101u * (v.x & 0xFFu) ? 1u : 0u) << (2 * i);
+                        eq |= (v.z == 0x01010101u * (v.z & 0xFFu) ? 1u : 0u) << (2 * i + 1);
+                    }
+                } else {
+                    // positions e0 .. e0 + 31 (e0 is 32-aligned, inputs are 16-aligned
+                    // and padded by 64 bytes past n)
+                    const uint4* s4 = reinterpret_cast<const uint4*>(src + e0);
+                    const uint4 a = __ldg(s4), b = __ldg(s4 + 1), c = __ldg(s4 + 2);
+                    const uint32_t w[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+#pragma unroll
+                    for (uint32_t k = 0; k < 32; k++) {
+                        const uint32_t x = (k & 3) ? __funnelshift_r(w[k >> 2], w[(k >> 2) + 1], 8 * (k & 3)) : w[k >> 2];
+                        eq |= (x == 0x01010101u * (x & 0xFFu) ? 1u : 0u) << k;
+                    }
+                }
+                eq &= nz;
+            }
+            nzw = nz;
+            eqw = eq;
+            __syncwarp();
+        };
+        while (pos < end && o.ok) {
+            const uint32_t e0 = radix ? (pos + 7) >> 3 : pos;
+            if (e0 >= e_hi) break;
+            if (wb == 0xFFFFFFFFu || e0 >= wb + kTokWin || e0 < wb) refill(e0 & ~31u);
+            const uint32_t rel = e0 - wb;
+            uint32_t word = nzw;
+            if (32 * lane + 31 < rel) word = 0;
+            else if (32 * lane < rel) word &= ~0u << (rel - 32 * lane);
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, word != 0);
+            if (!m) {  // nothing more in this window: continue after it
+                const uint32_t nb = wb + kTokWin;
+                if (nb >= e_hi) break;
+                pos = radix ? max(pos, 8 * nb) : max(pos, nb);
+                continue;
+            }
+            const uint32_t l = __ffs(m) - 1;
+            const uint32_t wl = __shfl_sync(0xFFFFFFFFu, word, l);
+            const uint32_t eql = __shfl_sync(0xFFFFFFFFu, eqw, l);
+            const uint32_t bit = __ffs(wl) - 1;
+            const uint32_t ent = wb + 32 * l + bit;
+            const uint32_t q = radix ? 8 * ent : ent;
             if (q >= end) break;
+            const uint32_t qd = sm.desc[ent - wb];
             uint32_t mLen = qd >> 20;
             const uint32_t d = qd & 0xFFFFFu;
-            // lookahead (:196-216)
-            if (q + 1 < end && nd != 0 && (nd >> 20) > mLen + 1) { pos = q + 1; continue; }
+            // lookahead (przm_tokenizer.cuh:196-216): radix frames have no
+            // descriptor at q + 1
+            if (!radix && q + 1 < end) {
+                const uint32_t nd = ent + 1 - wb < kTokWin ? sm.desc[ent + 1 - wb] : __ldg(dj + ent + 1);
+                if (nd != 0 && (nd >> 20) > mLen + 1) { pos = q + 1; continue; }
+            }
             // run-length token (:218-286)
-            if (q + 12 <= end) {
-                const uint8_t b0 = (uint8_t)qw;
-                if (qw == 0x01010101u * b0) {
-                    const uint32_t lim = q + min(end - q, 65535u);
-                    const uint32_t r = warp_run_end(src, q + 4, lim, b0, lane) - q;
-                    if (r >= 12 && r >= mLen) {
-                        if (q > litStart) e.lit_op(q - litStart);
-                        e.cmd_op(0xF1);
-                        e.cmd_varint(r);
-                        e.lits(src + litStart, q + 1 - litStart);  // pending literals, then the run byte
-                        pos = q + r;
-                        litStart = pos;
-                        continue;
+            if (q + 12 <= end && ((eql >> bit) & 1u)) {
+                const uint8_t b0 = src[q];
+                const uint32_t lim = q + min(end - q, 65535u);
+                const uint32_t r = warp_run_end(src, q + 4, lim, b0, lane) - q;
+                if (r >= 12 && r >= mLen) {
+                    if (lane == 0) {
+                        sm.rec[nrec][0] = (q - start) | ((q - litStart) << 16);
+                        sm.rec[nrec][1] = r | (2u << 16);
+                        sm.rec[nrec][2] = 0;
                     }
+                    nrec++;
+                    pos = q + r;
+                    litStart = pos;
+                    if (nrec == kTokRec) { __syncwarp(); tok_emit(sm.rec, nrec, src + start, o, lane); nrec = 0; __syncwarp(); }
+                    continue;
                 }
             }
             // match (:289-320).  The reference re-checks d <= q, mLen >= 4 and
             // the first 4 bytes here; every non-zero descriptor of both finders
-            // (k_tile_find, k_rx_resolve) already satisfies them.  Both finders
+            // (k_tile_find, k_rx_verify) already satisfies them.  Both finders
             // also stop a match at its first mismatch unless it reached 4095
             // bytes or the end of the data, so the forward extension can only
             // continue a 4095-byte descriptor.
@@ -242,32 +366,17 @@ __global__ void __launch_bounds__(256) k_tokenize(const uint8_t* __restrict__ in
                 if (mLen < lim && src[q + mLen] == src[q - d + mLen])
                     mLen = warp_match_end(src, q, q - d, mLen, lim, lane);
             }
-            // encode (:328-427)
             int k = -1;
             if ((int)d == rep0 && rep0 > 0) k = 0;
             else if ((int)d == rep1 && rep1 > 0) k = 1;
             else if ((int)d == rep2 && rep2 > 0) k = 2;
-            uint32_t litLen = q - litStart;
-            const uint32_t litAll = litLen;
-            const uint32_t keep = k >= 0 ? (mLen <= 7 ? 7u : 15u) : 3u;
-            if (litLen > keep) {
-                e.lit_op(litLen - keep);  // flushed literal op; its bytes go out with the rest below
-                litLen = keep;
+            if (lane == 0) {
+                sm.rec[nrec][0] = (q - start) | ((q - litStart) << 16);
+                sm.rec[nrec][1] = mLen | ((k >= 0 ? 1u : 0u) << 16) | ((uint32_t)(k >= 0 ? k : 0) << 18);
+                sm.rec[nrec][2] = d;
             }
-            const uint32_t base = mLen - 4 > 14 ? 15u : mLen - 4;
-            if (k >= 0 && mLen <= 7) {
-                e.cmd_op((uint8_t)((litLen << 4) | ((mLen - 4) << 2) | (uint32_t)k));
-            } else if (k >= 0) {
-                e.cmd_op((uint8_t)(0xC0 | k));
-                e.cmd_meta((uint8_t)((litLen << 4) | base));
-                if (base == 15) e.cmd_varint(mLen - 19);
-            } else {
-                e.cmd_op((uint8_t)(0x80 | (litLen << 4) | base));
-                if (base == 15) e.cmd_varint(mLen - 19);
-            }
-            e.lits(src + litStart, litAll);
+            nrec++;
             if (k < 0) {
-                e.off_varint(d);
                 rep2 = rep1; rep1 = rep0; rep0 = (int)d;
             } else if (k == 1) {
                 rep1 = rep0; rep0 = (int)d;
@@ -276,15 +385,22 @@ __global__ void __launch_bounds__(256) k_tokenize(const uint8_t* __restrict__ in
             }
             pos = q + mLen;
             litStart = pos;
+            if (nrec == kTokRec) { __syncwarp(); tok_emit(sm.rec, nrec, src + start, o, lane); nrec = 0; __syncwarp(); }
         }
-        if (e.ok && litStart < end) {  // trailing literals (:440-464)
-            e.lit_op(end - litStart);
-            e.lits(src + litStart, end - litStart);
+        if (o.ok && litStart < end) {  // trailing literals (:440-464)
+            if (lane == 0) {
+                sm.rec[nrec][0] = (end - start) | ((end - litStart) << 16);
+                sm.rec[nrec][1] = 3u << 16;
+                sm.rec[nrec][2] = 0;
+            }
+            nrec++;
         }
-        e.flush();
+        __syncwarp();
+        if (o.ok && nrec) tok_emit(sm.rec, nrec, src + start, o, lane);
+        __syncwarp();
         if (lane == 0) {
-            for (int s = 0; s < S_COUNT; s++) tile_lens[S * S_COUNT + s] = e.len[s];
-            if (!e.ok) atomicOr(err, (uint32_t)E_SLOT_OVERFLOW);
+            for (int s = 0; s < S_COUNT; s++) tile_lens[S * S_COUNT + s] = o.len[s];
+            if (!o.ok) atomicOr(err, (uint32_t)E_SLOT_OVERFLOW);
         }
     }
 }
