@@ -554,7 +554,7 @@ class Server:
 
     def poll(self, rid: int, cap: int, wait: bool = True):
         """(frame, t_submit_ns, t_done_ns), or None while pending (wait=False)."""
-        out = np.zeros(max(cap, 1), np.uint8)
+        out = np.empty(max(cap, 1), np.uint8)
         n, t0, t1 = C.c_uint64(), C.c_uint64(), C.c_uint64()
         r = L().przmg_serve_poll(self._h, rid, 1 if wait else 0, C.c_void_p(out.ctypes.data), cap, C.byref(n),
                                  C.byref(t0), C.byref(t1))
