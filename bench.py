@@ -211,6 +211,73 @@ def link_gbs(hin, nbytes: int, dev_buf: int, stream) -> dict:
     return out
 
 
+def uneven_measure(comp, count: int, sample: int) -> dict:
+    """The uneven-batch workload: `count` inputs with sizes log-uniform in
+    [1 KiB, 4 MiB] and mixed contents.  All of them as one device-resident
+    batch (graph replays, CUDA events), and a sample of `sample` inputs (every
+    count/sample-th) through the host API twice: batched (one launch sequence
+    for the sample) and plain (one launch sequence and one synchronisation per
+    input), both timed end to end with host buffers, frames compared."""
+    import numpy as np
+    import torch
+    from przm_b200 import gpu
+    from przm_b200 import workloads as W
+    xs = W.config3(count)
+    total = int(sum(len(a) for a in xs))
+    out = {"inputs": count, "bytes": total}
+    b = gpu.DeviceBatch(comp, [len(a) for a in xs], gpu.PROFILE_ANS)
+    try:
+        b.upload(np.concatenate(xs))
+        st = torch.cuda.Stream()
+        for _ in range(3):
+            b.enqueue(st.cuda_stream, graph=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(3):
+            b.enqueue(st.cuda_stream, graph=True)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        out["batched_device"] = {"gbps": round(total / ms / 1e6, 3), "ms": round(ms, 3)}
+    finally:
+        b.close()
+    # the sample, through the packed host API with pinned buffers: batched =
+    # one call for all inputs, plain = one call (launch sequence + sync) each
+    sub = xs[:: max(1, count // sample)][:sample]
+    sz = np.array([len(a) for a in sub], np.uint64)
+    sb = int(sz.sum())
+    cap = int(sum(gpu.FrameBound(int(s)) for s in sz)) + 64
+    p_in, p_out = gpu.AllocPinnedHost(sb + 64), gpu.AllocPinnedHost(cap)
+    try:
+        hin = np.ctypeslib.as_array((np.ctypeslib.ctypes.c_uint8 * (sb + 64)).from_address(p_in))
+        hout = np.ctypeslib.as_array((np.ctypeslib.ctypes.c_uint8 * cap).from_address(p_out))
+        offs = np.concatenate([[0], np.cumsum(sz)]).astype(np.int64)
+        for a, o in zip(sub, offs):
+            hin[o:o + len(a)] = a
+        comp.CompressPacked(hin, sz[:8], host_out=hout)  # warm
+        t0 = time.perf_counter()
+        fr, fs = comp.CompressPacked(hin, sz, host_out=hout)
+        tb = time.perf_counter() - t0
+        fb = bytes(fr)
+        t0 = time.perf_counter()
+        o_out = 0
+        same = True
+        for i in range(len(sub)):
+            f1, s1 = comp.CompressPacked(hin[offs[i]:], sz[i:i + 1], host_out=hout[o_out:])
+            same = same and int(s1[0]) == int(fs[i])
+            o_out += int(s1[0])
+        tp = time.perf_counter() - t0
+        same = same and bytes(hout[:o_out]) == fb
+    finally:
+        gpu.FreePinnedHost(p_in)
+        gpu.FreePinnedHost(p_out)
+    out["sample"] = {"inputs": len(sub), "bytes": sb, "api": "przmg_compress_packed, pinned host buffers",
+                     "batched_e2e_gbps": round(sb / tb / 1e9, 3), "plain_e2e_gbps": round(sb / tp / 1e9, 3),
+                     "batched_over_plain": round(tp / tb, 2), "identical_bytes": same}
+    return out
+
+
 def serve_measure(comp, count: int, fractions=(0.5,), seed: int = 0x50525A4D + 4) -> dict:
     """Serving workload: `count` requests with log-normal sizes (median 64 KiB,
     sigma 1.5, capped below 16 MiB) and mixed contents, through the
@@ -252,6 +319,8 @@ def main() -> None:
     ap.add_argument("--frames", type=int, default=256, help="frames per GPU (smaller cases for profiling)")
     ap.add_argument("--inflight", type=int, default=3, help="batches in flight on separate streams")
     ap.add_argument("--serve-requests", type=int, default=2000, help="requests of the serving measurement (0: skip)")
+    ap.add_argument("--uneven-inputs", type=int, default=4096, help="inputs of the uneven-batch measurement (0: skip)")
+    ap.add_argument("--uneven-sample", type=int, default=256, help="inputs timed batched vs plain")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -422,7 +491,12 @@ def main() -> None:
         plain = {"frames": len(sub), "gbps_e2e": round(sum(len(a) for a in sub) / dt / 1e9, 3),
                  "identical_bytes": all(bytes(f) == O.compress_p1(a) for f, a in zip(fb[:2], sub[:2]))}
 
+    for bt in batches[1:]:  # free the extra in-flight batches before the other workloads
+        bt.close()
+    batches = batches[:1]
     serve = serve_measure(comp, args.serve_requests) if args.serve_requests > 0 and rank == 0 else None
+    uneven = (uneven_measure(comp, args.uneven_inputs, args.uneven_sample)
+              if args.uneven_inputs > 0 and rank == 0 else None)
 
     # roofline of the dominant kernel
     peak, peak_kind = measured_peaks()
@@ -475,7 +549,7 @@ def main() -> None:
                     "ms_per_step": round(e2e_step, 3), "link_gbs": link, "host": numa},
             "roofline": roofline, "pipeline_roofline": pipeline, "stage_ms": {k: round(v, 3) for k, v in stages.items()},
             "cpu_baseline": cpu_base, "plain_per_frame": plain, "clocks": clk, "gpu_launches": gl,
-            "serving": serve,
+            "serving": serve, "uneven_batch": uneven,
         }
         print(json.dumps(line), flush=True)
     for bt in batches:
