@@ -20,7 +20,7 @@ Ours (default):
   reference's Go compressor cannot be built on this machine (no Go
   toolchain), so the oracle port of the path runs instead on all host cores.
 
-Steps are pipelined: --inflight D (default 3) batches, each with its own
+Steps are pipelined: --inflight D (default 5) batches, each with its own
 device buffers, take steps k = 0, 1, ... in turn on D streams, so one
 step's match/tokenize kernels overlap the previous steps' rANS chains
 (which use one warp on ~100 SMs for ~9 ms).  The timed region still spans
@@ -291,17 +291,20 @@ def serve_measure(comp, count: int, fractions=(0.5,), seed: int = 0x50525A4D + 4
     inputs = [W.mixture(seed + 31 * i, int(s))[0] for i, s in enumerate(sizes)]
     srv = gpu.Server(comp, gpu.PROFILE_ANS, mem_budget=64 << 30, max_inflight=3)
     try:
-        serving.run_open_loop(srv, inputs[: min(200, count)], None)  # warm the slots' buffers
+        serving.run_open_loop(srv, inputs, None)  # warm: slot buffers and the pinned chunk pool
+        t_before = srv.timing()
         sat = serving.run_open_loop(srv, inputs, None)
+        t_sat = {k: round(v - t_before[k], 3) if not k.startswith("max") else v for k, v in srv.timing().items()}
         rate_sat = count / sat["span_s"]
         out = {"requests": count, "bytes": sat["bytes"], "budget_gib": 64, "inflight": 3,
                "saturation": {"gbps": round(sat["gbps"], 3), "p50_ms": round(sat["p50_ms"], 3),
-                              "p99_ms": round(sat["p99_ms"], 3)}, "open_loop": []}
+                              "p99_ms": round(sat["p99_ms"], 3), "engine_timing": t_sat}, "open_loop": []}
         for f in fractions:
             r = serving.run_open_loop(srv, inputs, f * rate_sat, seed=seed + int(1000 * f))
             out["open_loop"].append({"load": f, "offered_gbps": round(r["offered_gbps"], 3), "gbps": round(r["gbps"], 3),
                                      "p50_ms": round(r["p50_ms"], 3), "p99_ms": round(r["p99_ms"], 3)})
         out["engine"] = srv.stats()
+        out["engine_timing"] = srv.timing()
     finally:
         srv.close()
     return out
@@ -310,14 +313,14 @@ def serve_measure(comp, count: int, fractions=(0.5,), seed: int = 0x50525A4D + 4
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--e2e-steps", type=int, default=16)
     ap.add_argument("--plain-frames", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--frames", type=int, default=256, help="frames per GPU (smaller cases for profiling)")
-    ap.add_argument("--inflight", type=int, default=3, help="batches in flight on separate streams")
+    ap.add_argument("--inflight", type=int, default=5, help="batches in flight on separate streams")
     ap.add_argument("--serve-requests", type=int, default=2000, help="requests of the serving measurement (0: skip)")
     ap.add_argument("--uneven-inputs", type=int, default=4096, help="inputs of the uneven-batch measurement (0: skip)")
     ap.add_argument("--uneven-sample", type=int, default=256, help="inputs timed batched vs plain")

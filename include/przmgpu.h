@@ -232,6 +232,11 @@ int32_t przmg_serve_poll(przmg_server* s, uint64_t id, int32_t wait, uint8_t* ds
  * largest batch (requests), most batches in flight at once, requests pending,
  * requests not yet polled */
 int32_t przmg_serve_stats(przmg_server* s, uint64_t stats[8]);
+/* t[6]: per-batch host times in ms, summed and largest: {sum launch, sum
+ * wait, sum out, max launch, max wait, max out}; launch = lay out, stage,
+ * upload and enqueue; wait = launched -> complete on the device; out =
+ * download and hand the frames to their requests */
+int32_t przmg_serve_timing(przmg_server* s, double t[6]);
 /* finishes the batches in flight, then frees the engine */
 int32_t przmg_serve_destroy(przmg_server* s);
 

@@ -98,6 +98,7 @@ SIGNATURES: dict[str, tuple] = {
     "przmg_serve_submit": (i32, [vp, vp, u64, vp]),
     "przmg_serve_poll": (i32, [vp, u64, i32, vp, u64, vp, vp, vp]),
     "przmg_serve_stats": (i32, [vp, vp]),
+    "przmg_serve_timing": (i32, [vp, vp]),
     "przmg_serve_destroy": (i32, [vp]),
     "przmg_normalize_freq": (None, [vp, u32, vp]),
     "przmg_normalize_frequencies": (None, [vp, vp]),

@@ -570,6 +570,13 @@ class Server:
         _check(L().przmg_serve_stats(self._h, _ptr(s)))
         return {k: int(v) for k, v in zip(self.STAT_KEYS, s)}
 
+    TIMING_KEYS = ("launch_ms", "wait_ms", "out_ms", "max_launch_ms", "max_wait_ms", "max_out_ms")
+
+    def timing(self) -> dict[str, float]:
+        t = np.zeros(6, np.float64)
+        _check(L().przmg_serve_timing(self._h, _ptr(t)))
+        return {k: round(float(v), 3) for k, v in zip(self.TIMING_KEYS, t)}
+
     def close(self) -> None:
         if self._h:
             _check(L().przmg_serve_destroy(self._h))

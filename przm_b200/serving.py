@@ -1,10 +1,11 @@
 """Open-loop load generation for the serving engine (gpu.Server): requests
-arrive as a Poisson process, a submitter thread sends each at its arrival
-time and a collector thread polls completions; latencies come from the
-engine's own submit/complete stamps (steady clock, frame on the host)."""
+arrive as a Poisson process and are submitted at their arrival times; the
+frames are collected afterwards.  Latencies come from the engine's own
+submit / complete stamps (steady clock, frame on the host), so collecting
+late does not change them, and one thread keeps the submission schedule
+free of interpreter-lock contention."""
 from __future__ import annotations
 
-import threading
 import time
 
 import numpy as np
@@ -17,44 +18,20 @@ def run_open_loop(server, inputs, rate_hz: float | None, seed: int = 7, cap_of=N
     rng = np.random.default_rng(seed)
     gaps = np.zeros(n) if rate_hz is None else rng.exponential(1.0 / rate_hz, n)
     arrive = np.cumsum(gaps)
-    ids = [None] * n
-    ready = [threading.Event() for _ in range(n)]
+    ids = []
+    t0 = time.perf_counter()
+    for i in range(n):
+        d = t0 + arrive[i] - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        ids.append(server.submit(inputs[i]))
     frames = [None] * n
-    lat = np.zeros(n)
     t_sub = np.zeros(n, np.int64)
     t_done = np.zeros(n, np.int64)
-    err = []
-
-    def submitter():
-        t0 = time.perf_counter()
-        for i in range(n):
-            d = t0 + arrive[i] - time.perf_counter()
-            if d > 0:
-                time.sleep(d)
-            ids[i] = server.submit(inputs[i])
-            ready[i].set()
-
-    def collector():
-        try:
-            for i in range(n):
-                ready[i].wait()
-                cap = cap_of(len(inputs[i])) if cap_of else 2 * len(inputs[i]) + 4096
-                f, ts, td = server.poll(ids[i], cap, wait=True)
-                frames[i] = f
-                t_sub[i], t_done[i] = ts, td
-                lat[i] = (td - ts) / 1e6
-        except Exception as e:  # reported to the caller
-            err.append(e)
-            for j in range(n):
-                ready[j].set()
-
-    ts, tc = threading.Thread(target=submitter), threading.Thread(target=collector)
-    ts.start()
-    tc.start()
-    ts.join()
-    tc.join()
-    if err:
-        raise err[0]
+    for i in range(n):
+        cap = cap_of(len(inputs[i])) if cap_of else 2 * len(inputs[i]) + 4096
+        frames[i], t_sub[i], t_done[i] = server.poll(ids[i], cap, wait=True)
+    lat = (t_done - t_sub) / 1e6
     span = (t_done.max() - t_sub.min()) / 1e9
     nbytes = int(sum(len(a) for a in inputs))
     offered = None if rate_hz is None else nbytes / max(arrive[-1], 1e-9) / 1e9
