@@ -519,6 +519,16 @@ def main() -> None:
                 "frac": round(achieved / peak, 5), "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
                 "traffic": traffic, "algorithmic_bytes_per_launch": int(alg),
                 "kernel_ms": round(stages[dom], 3)}
+    if dom == "rans":
+        # the bound that applies: the longest lane chain (ceil(symbols / 4)
+        # dependent steps) at the 42.6-cycle register-only step of a one-warp
+        # microbenchmark, at the sampled SM clock
+        lens = batch.stream_lens()
+        rounds = int(max(int(lens[:, 5].max(initial=0)), int(lens[:, 1:4].max(initial=0))) + 3) // 4
+        mhz = clk.get("sm_mhz") or 1965.0
+        floor_ms = rounds * 42.6 / (mhz * 1e3)
+        roofline["chain"] = {"longest_lane_rounds": rounds, "cycles_per_round_floor": 42.6, "sm_mhz": mhz,
+                             "floor_ms": round(floor_ms, 3), "frac": round(floor_ms / stages[dom], 3)}
     pipeline = {"alg_bytes": stats["input_bytes"] + stats["frame_bytes"],
                 "achieved_gbs": round((stats["input_bytes"] + stats["frame_bytes"]) / (ms / 1e3) / 1e9, 2),
                 "frac_of_hbm": round((stats["input_bytes"] + stats["frame_bytes"]) / (ms / 1e3) / 1e9 / peak, 5)}

@@ -205,6 +205,9 @@ const char* przmg_stage_name(int32_t k);
 /* totals of the last run (synchronises): input, frame, literal, command and
  * offset bytes, rANS symbols and emitted bytes, uncompressed frames */
 int32_t przmg_batch_stats(przmg_batch* b, uint64_t stats[8]);
+/* per-input stream lengths of the last run (synchronises): lens[6 i + s] for
+ * s = commands, op, meta, var substreams, offsets, literals; cap = entries */
+int32_t przmg_batch_stream_lens(przmg_batch* b, uint32_t* lens, uint64_t cap);
 int32_t przmg_batch_destroy(przmg_batch* b);
 
 /* ---- serving: continuous batching (no reference counterpart; the reference

@@ -85,6 +85,7 @@ SIGNATURES: dict[str, tuple] = {
     "przmg_batch_stage_times": (i32, [vp, vp, i32, vp]),
     "przmg_stage_name": (C.c_char_p, [i32]),
     "przmg_batch_stats": (i32, [vp, vp]),
+    "przmg_batch_stream_lens": (i32, [vp, vp, u64]),
     "przmg_compress_packed": (i32, [vp, vp, vp, u64, i32, vp, u64, vp, vp]),
     "przmg_compute_histogram_gpu": (i32, [vp, u64, u64, u64, vp, vp, vp]),
     "przmg_compute_histogram_host": (i32, [vp, vp, u64, vp, vp]),

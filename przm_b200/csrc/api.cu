@@ -1122,6 +1122,18 @@ extern "C" int32_t przmg_compress_packed(przmg_ctx* h, const uint8_t* host_in, c
 }
 
 
+extern "C" int32_t przmg_batch_stream_lens(przmg_batch* b, uint32_t* lens, uint64_t cap) {
+    if (!b || (!lens && b->njobs)) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    if (cap < (uint64_t)b->njobs * S_COUNT) return fail(PRZMG_ERR_BUFFER_TOO_SMALL, "lens needs 6 entries per input");
+    Ctx* c = b->ctx;
+    LOCKED(c);
+    if (b->njobs) {
+        CK(cudaMemcpyAsync(lens, b->d_job_lens.p, 4ull * b->njobs * S_COUNT, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return PRZMG_OK;
+}
+
 extern "C" int32_t przmg_batch_destroy(przmg_batch* b) {
     if (!b) return PRZMG_OK;
     Ctx* c = b->ctx;

@@ -522,6 +522,13 @@ class DeviceBatch:
         _check(L().przmg_batch_stats(self._h, _ptr(s)))
         return {k: int(v) for k, v in zip(self.STAT_KEYS, s)}
 
+    def stream_lens(self) -> np.ndarray:
+        """(inputs, 6) stream lengths of the last run: commands, op, meta, var,
+        offsets, literals."""
+        out = np.zeros(max(len(self.sizes), 1) * 6, np.uint32)
+        _check(L().przmg_batch_stream_lens(self._h, _ptr(out), len(out)))
+        return out[: 6 * len(self.sizes)].reshape(-1, 6)
+
     def stage_times(self) -> dict[str, float]:
         """One enqueue with events between stages: {stage: device ms}."""
         ms = (C.c_float * 16)()
