@@ -413,6 +413,53 @@ __global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __re
 // ---------------------------------------------------------------------------
 constexpr uint32_t kGatherThreads = 512;
 
+__device__ __forceinline__ void hist4(uint32_t* h, uint32_t w) {
+    atomicAdd(&h[w & 0xFFu], 1u);
+    atomicAdd(&h[(w >> 8) & 0xFFu], 1u);
+    atomicAdd(&h[(w >> 16) & 0xFFu], 1u);
+    atomicAdd(&h[w >> 24], 1u);
+}
+
+// Copies n bytes s -> d with the warp and counts them into h (shared, may be
+// null): bytes up to d's first 16-byte boundary, then one aligned 16-byte
+// store per lane per step (source words loaded aligned and funnel-shifted,
+// so reading up to 3 bytes past s + n: the slot blocks have room), then the
+// tail bytes.
+__device__ void warp_copy_hist(uint8_t* __restrict__ d, const uint8_t* __restrict__ s, uint32_t n,
+                               uint32_t* __restrict__ h, uint32_t lane) {
+    const uint32_t head = min(n, (uint32_t)((16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15));
+    if (lane < head) {
+        const uint8_t b = s[lane];
+        d[lane] = b;
+        if (h) atomicAdd(&h[b], 1u);
+    }
+    d += head;
+    s += head;
+    n -= head;
+    const uint32_t nv = n / 16;
+    const uint32_t sh = 8 * (uint32_t)(reinterpret_cast<uintptr_t>(s) & 3);
+    const uint32_t* sw = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(s) & ~uintptr_t(3));
+    uint4* d4 = reinterpret_cast<uint4*>(d);
+    for (uint32_t v = lane; v < nv; v += 32) {
+        const uint32_t* q = sw + 4 * v;
+        uint4 o;
+        if (sh == 0) {
+            o = make_uint4(q[0], q[1], q[2], q[3]);
+        } else {
+            const uint32_t w4 = q[4];
+            o = make_uint4(__funnelshift_r(q[0], q[1], sh), __funnelshift_r(q[1], q[2], sh),
+                           __funnelshift_r(q[2], q[3], sh), __funnelshift_r(q[3], w4, sh));
+        }
+        d4[v] = o;
+        if (h) { hist4(h, o.x); hist4(h, o.y); hist4(h, o.z); hist4(h, o.w); }
+    }
+    for (uint32_t i = 16 * nv + lane; i < n; i += 32) {
+        const uint8_t b = s[i];
+        d[i] = b;
+        if (h) atomicAdd(&h[b], 1u);
+    }
+}
+
 __global__ void __launch_bounds__(kGatherThreads) k_gather(const Job* __restrict__ jobs, uint32_t njobs,
                                                           const uint8_t* __restrict__ slots,
                                                           const uint32_t* __restrict__ tile_lens,
@@ -454,15 +501,11 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather(const Job* __restrict
             }
             uint8_t* dst = sreg + stream_base(job, s);
             const int hs = s == S_LIT ? 0 : (s == S_OP ? 1 : (s == S_META ? 2 : (s == S_VAR ? 3 : -1)));
-            // one warp per tile, bytes in order
+            // one warp per tile
             for (uint32_t t = warp; t < job.ntiles; t += kGatherThreads / 32) {
                 const uint32_t o = s_off[t], l = s_off[t + 1] - o;
                 const uint8_t* sp = slots + (uint64_t)(job.tile0 + t) * kSlotStride + slot_base(s);
-                for (uint32_t i = lane; i < l; i += 32) {
-                    uint8_t b = sp[i];
-                    dst[o + i] = b;
-                    if (hs >= 0) atomicAdd(&s_hist[hs][warp & 3][b], 1u);
-                }
+                warp_copy_hist(dst + o, sp, l, hs >= 0 ? s_hist[hs][warp & 3] : nullptr, lane);
             }
             if (tid == 0) job_lens[(uint64_t)j * S_COUNT + s] = total;
         }
