@@ -963,10 +963,10 @@ extern "C" int32_t przmg_batch_launch_count(przmg_batch* b) { return b ? b->laun
 __global__ void k_scatter_inputs(const uint8_t* __restrict__ packed, const uint64_t* __restrict__ src_off,
                                  const Job* __restrict__ jobs, uint32_t njobs, uint8_t* __restrict__ in) {
     for (uint32_t j = blockIdx.y; j < njobs; j += gridDim.y) {
-        const uint8_t* s = packed + src_off[j];
-        uint8_t* d = in + jobs[j].in_off;
         const uint32_t n = jobs[j].n;
-        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d[i] = s[i];
+        const uint32_t chunk = ((n + gridDim.x - 1) / gridDim.x + 15) & ~15u;  // 16-byte aligned slice per block
+        const uint32_t lo = min(n, blockIdx.x * chunk), hi = min(n, lo + chunk);
+        if (lo < hi) block_copy(in + jobs[j].in_off + lo, packed + src_off[j] + lo, hi - lo);
     }
 }
 
@@ -974,10 +974,10 @@ __global__ void k_gather_frames(const uint8_t* __restrict__ out, const Job* __re
                                 const uint32_t* __restrict__ sizes, const uint64_t* __restrict__ dst_off, uint32_t njobs,
                                 uint8_t* __restrict__ packed) {
     for (uint32_t j = blockIdx.y; j < njobs; j += gridDim.y) {
-        const uint8_t* s = out + jobs[j].out_off;
-        uint8_t* d = packed + dst_off[j];
         const uint32_t n = sizes[j];
-        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d[i] = s[i];
+        const uint32_t chunk = ((n + gridDim.x - 1) / gridDim.x + 15) & ~15u;
+        const uint32_t lo = min(n, blockIdx.x * chunk), hi = min(n, lo + chunk);
+        if (lo < hi) block_copy(packed + dst_off[j] + lo, out + jobs[j].out_off + lo, hi - lo);
     }
 }
 
