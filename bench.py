@@ -208,6 +208,24 @@ def link_gbs(hin, nbytes: int, dev_buf: int, stream) -> dict:
         e1.record(stream)
         e1.synchronize()
         out[name] = round(nbytes / (e0.elapsed_time(e1) / 1e3) / 1e9, 2)
+    # both directions at once (two streams, halves of the buffers): what an
+    # end-to-end step that uploads and downloads concurrently can use
+    half = nbytes // 2
+    s2 = torch.cuda.Stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    s2.wait_event(e0)
+    rt.cudaMemcpyAsync(ctypes.c_void_p(dev_buf), ctypes.c_void_p(hin.ctypes.data), half, 1,
+                       ctypes.c_void_p(stream.cuda_stream))
+    rt.cudaMemcpyAsync(ctypes.c_void_p(hin.ctypes.data + half), ctypes.c_void_p(dev_buf + half), half, 2,
+                       ctypes.c_void_p(s2.cuda_stream))
+    ev = torch.cuda.Event()
+    ev.record(s2)
+    stream.wait_event(ev)
+    e1.record(stream)
+    e1.synchronize()
+    out["both_each_way"] = round(half / (e0.elapsed_time(e1) / 1e3) / 1e9, 2)
     return out
 
 
