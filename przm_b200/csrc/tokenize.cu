@@ -73,11 +73,11 @@ __device__ uint32_t warp_match_end(const uint8_t* src, uint32_t a, uint32_t b, u
 // Walk.  The greedy parse is serial: each decision fixes where the next one
 // starts.  It runs over a shared window of kTokWin match descriptors
 // (radix frames: 8-aligned candidates; small frames: every position), with
-// two bitmaps of the window in registers -- lane l holds the bits of entries
-// [32l, 32l + 32) -- one marking non-zero descriptors, one marking positions
-// whose 4 bytes are equal (the run-length test).  Finding the next
-// descriptor is a ballot over those registers; only run-length scans and
-// the extension of 4095-byte matches read global memory.  Every decision
+// two shared bitmaps of the window -- non-zero descriptors, and positions
+// whose 4 bytes are equal (the run-length test) -- and a register summary of
+// the non-empty bitmap words.  Finding the next descriptor is a warp-uniform
+// lookup in those; only run-length scans and the extension of 4095-byte
+// matches read global memory.  Every decision
 // becomes a 12-byte record in shared memory:
 //   r0 = q - tile start | literals before q << 16
 //   r1 = match or run length | kind << 16 | repeat slot << 18
@@ -96,7 +96,9 @@ constexpr uint32_t kTokWarps = 4;    // warps (tiles) per block
 
 struct TokSmem {
     uint32_t desc[kTokWin];
-    uint32_t rec[kTokRec][3];
+    uint32_t nz[kTokWin / 32];  // non-zero descriptors of the window, word per 32 entries
+    uint32_t eq[kTokWin / 32];  // ... whose 4 bytes are equal
+    uint4 rec[kTokRec];         // records (x, y, z; w unused): one 16-byte store each
 };
 
 __device__ __forceinline__ uint32_t vlen(uint32_t v) { return v < 0x80u ? 1u : v < 0x4000u ? 2u : v < 0x200000u ? 3u : v < 0x10000000u ? 4u : 5u; }
@@ -125,13 +127,12 @@ struct TokTileOut {
 };
 
 // Writes records [0, nrec) of the warp's buffer.
-__device__ void tok_emit(const uint32_t (*rec)[3], uint32_t nrec, const uint8_t* tile_src, TokTileOut& o,
-                         uint32_t lane) {
+__device__ void tok_emit(const uint4* rec, uint32_t nrec, const uint8_t* tile_src, TokTileOut& o, uint32_t lane) {
     for (uint32_t g = 0; g < nrec; g += 32) {
         const uint32_t i = g + lane;
         const bool v = i < nrec;
         uint32_t r0 = 0, r1 = 0, r2 = 0;
-        if (v) { r0 = rec[i][0]; r1 = rec[i][1]; r2 = rec[i][2]; }
+        if (v) { const uint4 x = rec[i]; r0 = x.x; r1 = x.y; r2 = x.z; }
         const uint32_t q = r0 & 0xFFFFu, lit = r0 >> 16, len = r1 & 0xFFFFu, kind = (r1 >> 16) & 3u, k = r1 >> 18;
         // literal-op count, op byte and the rest, per record kind
         uint32_t flush = 0, litLen = 0, base = 0;
@@ -261,7 +262,7 @@ __global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __re
         o.ok = true;
         int rep0 = tt.tile == 0 ? 1 : -1, rep1 = tt.tile == 0 ? 4 : -1, rep2 = tt.tile == 0 ? 8 : -1;
         uint32_t pos = start, litStart = start, nrec = 0;
-        uint32_t wb = 0xFFFFFFFFu, nzw = 0, eqw = 0;  // window base entry, this lane's bitmap words
+        uint32_t wb = 0xFFFFFFFFu, wsum = 0;  // window base entry; bit k: word k of the window has a descriptor
         auto refill = [&](uint32_t base) {
             // entries [base, base + kTokWin): descriptors to shared memory, bitmaps to registers
             __syncwarp();
@@ -301,28 +302,32 @@ __global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __re
                 }
                 eq &= nz;
             }
-            nzw = nz;
-            eqw = eq;
+            sm.nz[lane] = nz;
+            sm.eq[lane] = eq;
+            wsum = __ballot_sync(0xFFFFFFFFu, nz != 0);
             __syncwarp();
         };
         while (pos < end && o.ok) {
             const uint32_t e0 = radix ? (pos + 7) >> 3 : pos;
             if (e0 >= e_hi) break;
             if (wb == 0xFFFFFFFFu || e0 >= wb + kTokWin || e0 < wb) refill(e0 & ~31u);
+            // next descriptor at or after e0: the rest of e0's word, else the
+            // first non-empty word after it (warp-uniform, no shuffles)
             const uint32_t rel = e0 - wb;
-            uint32_t word = nzw;
-            if (32 * lane + 31 < rel) word = 0;
-            else if (32 * lane < rel) word &= ~0u << (rel - 32 * lane);
-            const uint32_t m = __ballot_sync(0xFFFFFFFFu, word != 0);
-            if (!m) {  // nothing more in this window: continue after it
-                const uint32_t nb = wb + kTokWin;
-                if (nb >= e_hi) break;
-                pos = radix ? max(pos, 8 * nb) : max(pos, nb);
-                continue;
+            uint32_t l = rel >> 5;
+            uint32_t wl = sm.nz[l] & (0xFFFFFFFFu << (rel & 31));
+            if (!wl) {
+                const uint32_t rest = l < 31 ? wsum & (0xFFFFFFFEu << l) : 0u;
+                if (!rest) {  // nothing more in this window: continue after it
+                    const uint32_t nb = wb + kTokWin;
+                    if (nb >= e_hi) break;
+                    pos = radix ? max(pos, 8 * nb) : max(pos, nb);
+                    continue;
+                }
+                l = __ffs(rest) - 1;
+                wl = sm.nz[l];
             }
-            const uint32_t l = __ffs(m) - 1;
-            const uint32_t wl = __shfl_sync(0xFFFFFFFFu, word, l);
-            const uint32_t eql = __shfl_sync(0xFFFFFFFFu, eqw, l);
+            const uint32_t eql = sm.eq[l];
             const uint32_t bit = __ffs(wl) - 1;
             const uint32_t ent = wb + 32 * l + bit;
             const uint32_t q = radix ? 8 * ent : ent;
@@ -342,11 +347,7 @@ __global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __re
                 const uint32_t lim = q + min(end - q, 65535u);
                 const uint32_t r = warp_run_end(src, q + 4, lim, b0, lane) - q;
                 if (r >= 12 && r >= mLen) {
-                    if (lane == 0) {
-                        sm.rec[nrec][0] = (q - start) | ((q - litStart) << 16);
-                        sm.rec[nrec][1] = r | (2u << 16);
-                        sm.rec[nrec][2] = 0;
-                    }
+                    if (lane == 0) sm.rec[nrec] = make_uint4((q - start) | ((q - litStart) << 16), r | (2u << 16), 0u, 0u);
                     nrec++;
                     pos = q + r;
                     litStart = pos;
@@ -370,11 +371,9 @@ __global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __re
             if ((int)d == rep0 && rep0 > 0) k = 0;
             else if ((int)d == rep1 && rep1 > 0) k = 1;
             else if ((int)d == rep2 && rep2 > 0) k = 2;
-            if (lane == 0) {
-                sm.rec[nrec][0] = (q - start) | ((q - litStart) << 16);
-                sm.rec[nrec][1] = mLen | ((k >= 0 ? 1u : 0u) << 16) | ((uint32_t)(k >= 0 ? k : 0) << 18);
-                sm.rec[nrec][2] = d;
-            }
+            if (lane == 0)
+                sm.rec[nrec] = make_uint4((q - start) | ((q - litStart) << 16),
+                                          mLen | ((k >= 0 ? 1u : 0u) << 16) | ((uint32_t)(k >= 0 ? k : 0) << 18), d, 0u);
             nrec++;
             if (k < 0) {
                 rep2 = rep1; rep1 = rep0; rep0 = (int)d;
@@ -388,11 +387,7 @@ __global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __re
             if (nrec == kTokRec) { __syncwarp(); tok_emit(sm.rec, nrec, src + start, o, lane); nrec = 0; __syncwarp(); }
         }
         if (o.ok && litStart < end) {  // trailing literals (:440-464)
-            if (lane == 0) {
-                sm.rec[nrec][0] = (end - start) | ((end - litStart) << 16);
-                sm.rec[nrec][1] = 3u << 16;
-                sm.rec[nrec][2] = 0;
-            }
+            if (lane == 0) sm.rec[nrec] = make_uint4((end - start) | ((end - litStart) << 16), 3u << 16, 0u, 0u);
             nrec++;
         }
         __syncwarp();
