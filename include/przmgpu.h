@@ -119,7 +119,10 @@ int32_t przmg_is_available(void);                              /* IsAvailable, g
 int32_t przmg_init(int32_t device, przmg_ctx** out);            /* NewGPUCompressor, gpu/bridge.go:291 */
 int32_t przmg_get_global(przmg_ctx** out);                      /* GetGlobalCompressor, gpu/bridge.go:96 */
 void przmg_reset_global_for_test(void);                         /* ResetGlobalCompressorForTest, :117 */
-int32_t przmg_close(przmg_ctx* ctx);                            /* (*GPUCompressor).Close, :513 */
+/* (*GPUCompressor).Close, :513.  Batches (przmg_batch_create) and serving
+ * engines (przmg_serve_create) use their context until they are destroyed:
+ * destroy them first. */
+int32_t przmg_close(przmg_ctx* ctx);
 void przmg_set_mock_unavailable(int32_t unavailable);           /* SetMockUnavailableForTest, :45 */
 void przmg_set_mock_match_error(int32_t code);                  /* SetMockMatchErrorForTest, :50 (0 clears) */
 /* ComputeMajor/ComputeMinor/DeviceName/SMCount/TotalVRAMBytes fields, :283-287 */
