@@ -214,13 +214,16 @@ __global__ void __launch_bounds__(256) k_rx_scatter(const uint8_t* __restrict__ 
         __syncthreads();
         for (uint32_t i = tid; i < 8 * kRxParts; i += 256) (&s_w[0][0])[i] = 0;
         __syncthreads();
-        uint32_t h[16];
+        uint32_t h[16], peers[16];  // hash and same-partition lanes of each round
 #pragma unroll
         for (int r = 0; r < 16; r++) {
             const uint32_t c = c0 + 512 * warp + 32 * r + lane;
             h[r] = c < c1 ? kmer_hash(__ldg(src + c)) : 0xFFFFFFFFu;
-            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, h[r] >> kRxKeyBits);
-            if (h[r] != 0xFFFFFFFFu && (peers & lt) == 0) s_w[warp][h[r] >> kRxKeyBits] += __popc(peers);
+        }
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+            peers[r] = __match_any_sync(0xFFFFFFFFu, h[r] >> kRxKeyBits);
+            if (h[r] != 0xFFFFFFFFu && (peers[r] & lt) == 0) s_w[warp][h[r] >> kRxKeyBits] += __popc(peers[r]);
             __syncwarp();
         }
         __syncthreads();
@@ -238,12 +241,11 @@ __global__ void __launch_bounds__(256) k_rx_scatter(const uint8_t* __restrict__ 
 #pragma unroll
         for (int r = 0; r < 16; r++) {
             const uint32_t c = c0 + 512 * warp + 32 * r + lane;
-            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, h[r] >> kRxKeyBits);
             uint32_t slot = 0;
-            if (h[r] != 0xFFFFFFFFu) slot = s_w[warp][h[r] >> kRxKeyBits] + __popc(peers & lt);
+            if (h[r] != 0xFFFFFFFFu) slot = s_w[warp][h[r] >> kRxKeyBits] + __popc(peers[r] & lt);
             __syncwarp();
             if (h[r] != 0xFFFFFFFFu) {
-                if ((peers & lt) == 0) s_w[warp][h[r] >> kRxKeyBits] += __popc(peers);
+                if ((peers[r] & lt) == 0) s_w[warp][h[r] >> kRxKeyBits] += __popc(peers[r]);
                 ej[slot] = c;
                 kj[slot] = (uint16_t)(h[r] & (kRxKeys - 1));
             }
