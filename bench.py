@@ -519,9 +519,10 @@ def main() -> None:
     for bt in batches[1:]:  # free the extra in-flight batches before the other workloads
         bt.close()
     batches = batches[:1]
-    serve = serve_measure(comp, args.serve_requests) if args.serve_requests > 0 and rank == 0 else None
+    # single-GPU runs only (under torchrun the other ranks would wait for them)
+    serve = serve_measure(comp, args.serve_requests) if args.serve_requests > 0 and world == 1 else None
     uneven = (uneven_measure(comp, args.uneven_inputs, args.uneven_sample)
-              if args.uneven_inputs > 0 and rank == 0 else None)
+              if args.uneven_inputs > 0 and world == 1 else None)
 
     # roofline of the dominant kernel
     peak, peak_kind = measured_peaks()
