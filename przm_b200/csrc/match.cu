@@ -309,26 +309,32 @@ __global__ void __launch_bounds__(kRxResolveWarps * 32) k_rx_resolve(const Job* 
         const uint32_t* ej = ent + job.desc_off + pr.x;
         const uint16_t* kj = key + job.desc_off + pr.x;
         uint32_t* pj = pred + job.desc_off + pr.x;
-        // the next chunk's entries are loaded while this one resolves
-        uint32_t c = lane < pr.y ? ej[lane] : 0u;
-        uint32_t k = lane < pr.y ? kj[lane] : 0xFFFFu;
-        for (uint32_t i0 = 0; i0 < pr.y; i0 += 32) {
-            const uint32_t i = i0 + lane, inext = i + 32;
-            const uint32_t cn = inext < pr.y ? ej[inext] : 0u;
-            const uint32_t kn = inext < pr.y ? kj[inext] : 0xFFFFu;
-            const bool v = i < pr.y;
-            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, k);
-            const uint32_t lower = peers & lt;
-            const uint32_t from = lower ? 31u - __clz(lower) : lane;
-            const uint32_t cl = __shfl_sync(0xFFFFFFFFu, c, from);
-            uint32_t pv = 0;  // predecessor + 1
-            if (v) pv = lower ? cl + 1 : table[k];
-            __syncwarp();
-            if (v && (peers >> lane) == 1u) table[k] = c + 1;
-            __syncwarp();
-            if (v) pj[i] = pv;
-            c = cn;
-            k = kn;
+        // 256 entries per round trip: each lane loads 8 (one per chunk of 32)
+        // together, then the 8 chunks resolve in order from registers
+        for (uint32_t b0 = 0; b0 < pr.y; b0 += 256) {
+            uint32_t cc[8], kk[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const uint32_t i = b0 + 32 * u + lane;
+                cc[u] = i < pr.y ? ej[i] : 0u;
+                kk[u] = i < pr.y ? kj[i] : 0xFFFFu;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const uint32_t i = b0 + 32 * u + lane;
+                const bool v = i < pr.y;
+                const uint32_t c = cc[u], k = kk[u];
+                const uint32_t peers = __match_any_sync(0xFFFFFFFFu, k);
+                const uint32_t lower = peers & lt;
+                const uint32_t from = lower ? 31u - __clz(lower) : lane;
+                const uint32_t cl = __shfl_sync(0xFFFFFFFFu, c, from);
+                uint32_t pv = 0;  // predecessor + 1
+                if (v) pv = lower ? cl + 1 : table[k];
+                __syncwarp();
+                if (v && (peers >> lane) == 1u) table[k] = c + 1;
+                __syncwarp();
+                if (v) pj[i] = pv;
+            }
         }
         __syncwarp();
     }
