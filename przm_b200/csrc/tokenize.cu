@@ -93,6 +93,7 @@ __device__ uint32_t warp_match_end(const uint8_t* src, uint32_t a, uint32_t b, u
 constexpr uint32_t kTokWin = 1024;   // descriptor window entries
 constexpr uint32_t kTokRec = 256;    // records buffered before emission
 constexpr uint32_t kTokWarps = 4;    // warps (tiles) per block
+constexpr uint32_t kLongLit = 128;   // literal runs copied 16 bytes per lane
 
 struct TokSmem {
     uint32_t desc[kTokWin];
@@ -125,6 +126,66 @@ struct TokTileOut {
     uint32_t len[S_COUNT];  // bytes written per stream (warp-uniform)
     bool ok;
 };
+
+__device__ __forceinline__ void hist4(uint32_t* h, uint32_t w) {
+    atomicAdd(&h[w & 0xFFu], 1u);
+    atomicAdd(&h[(w >> 8) & 0xFFu], 1u);
+    atomicAdd(&h[(w >> 16) & 0xFFu], 1u);
+    atomicAdd(&h[w >> 24], 1u);
+}
+
+// 16 source bytes at sw + 4v, shifted right by sh bits (sh = 8 x the
+// source's offset from its 4-byte boundary).
+__device__ __forceinline__ uint4 ld16_shifted(const uint32_t* __restrict__ sw, uint32_t v, uint32_t sh) {
+    const uint32_t* q = sw + 4 * v;
+    if (sh == 0) return make_uint4(q[0], q[1], q[2], q[3]);
+    const uint32_t w4 = q[4];
+    return make_uint4(__funnelshift_r(q[0], q[1], sh), __funnelshift_r(q[1], q[2], sh),
+                      __funnelshift_r(q[2], q[3], sh), __funnelshift_r(q[3], w4, sh));
+}
+
+// Copies n bytes s -> d with the warp and counts them into h (shared, may be
+// null): bytes up to d's first 16-byte boundary, then aligned 16-byte stores,
+// four per lane in flight (source words loaded aligned and funnel-shifted, so
+// reading up to 3 bytes past s + n: slot blocks and inputs have room), then
+// the tail bytes.
+__device__ void warp_copy_hist(uint8_t* __restrict__ d, const uint8_t* __restrict__ s, uint32_t n,
+                               uint32_t* __restrict__ h, uint32_t lane) {
+    const uint32_t head = min(n, (uint32_t)((16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15));
+    if (lane < head) {
+        const uint8_t b = s[lane];
+        d[lane] = b;
+        if (h) atomicAdd(&h[b], 1u);
+    }
+    d += head;
+    s += head;
+    n -= head;
+    const uint32_t nv = n / 16;
+    const uint32_t sh = 8 * (uint32_t)(reinterpret_cast<uintptr_t>(s) & 3);
+    const uint32_t* sw = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(s) & ~uintptr_t(3));
+    uint4* d4 = reinterpret_cast<uint4*>(d);
+    uint32_t v = lane;
+    for (; v + 96 < nv; v += 128) {
+        uint4 o[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) o[u] = ld16_shifted(sw, v + 32 * u, sh);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            d4[v + 32 * u] = o[u];
+            if (h) { hist4(h, o[u].x); hist4(h, o[u].y); hist4(h, o[u].z); hist4(h, o[u].w); }
+        }
+    }
+    for (; v < nv; v += 32) {
+        const uint4 o = ld16_shifted(sw, v, sh);
+        d4[v] = o;
+        if (h) { hist4(h, o.x); hist4(h, o.y); hist4(h, o.z); hist4(h, o.w); }
+    }
+    for (uint32_t i = 16 * nv + lane; i < n; i += 32) {
+        const uint8_t b = s[i];
+        d[i] = b;
+        if (h) atomicAdd(&h[b], 1u);
+    }
+}
 
 // Writes records [0, nrec) of the warp's buffer.
 __device__ void tok_emit(const uint4* rec, uint32_t nrec, const uint8_t* tile_src, TokTileOut& o, uint32_t lane) {
@@ -211,23 +272,49 @@ __device__ void tok_emit(const uint4* rec, uint32_t nrec, const uint8_t* tile_sr
                 if (kind == 0) put_varint(o.base + slot_base(S_OFF) + off[S_OFF], r2);
             }
         }
-        // literal runs of these records, all lanes over the concatenated bytes
+        // literal runs of these records: runs of kLongLit bytes or more one at a
+        // time with the warp's 16-byte copy, the shorter ones all lanes over
+        // their concatenated bytes, four bytes per lane in flight
         {
-            const uint32_t incl = warp_incl(c[S_LIT], lane), tl = tot[S_LIT];
-            const uint32_t from = q - lit;  // first literal of this record, tile-relative
+            const uint32_t cl = c[S_LIT];
+            const bool lng = cl >= kLongLit;
+            const uint32_t cs = lng ? 0u : cl;
+            const uint32_t incl = warp_incl(cs, lane), ts = __shfl_sync(0xFFFFFFFFu, incl, 31);
+            const uint32_t from = q - lit;                     // first literal of this record, tile-relative
+            const uint32_t dx = off[S_LIT] - o.len[S_LIT];     // its place in this group's literal bytes
             uint8_t* dl = o.base + slot_base(S_LIT) + o.len[S_LIT];
-            for (uint32_t b0 = 0; b0 < tl; b0 += 32) {  // warp-uniform trip count: every lane shuffles
-                const uint32_t b = b0 + lane;
-                // record j with incl[j-1] <= b < incl[j]
-                uint32_t j = 0;
+            for (uint32_t b0 = 0; b0 < ts; b0 += 128) {  // warp-uniform trip count: every lane shuffles
+                uint32_t si[4], di[4];
 #pragma unroll
-                for (int st = 16; st >= 1; st >>= 1) {
-                    const uint32_t x = __shfl_sync(0xFFFFFFFFu, incl, j + st - 1);
-                    if (x <= b) j += st;
+                for (int u = 0; u < 4; u++) {
+                    const uint32_t b = b0 + 32 * u + lane;
+                    // record j with incl[j-1] <= b < incl[j]
+                    uint32_t j = 0;
+#pragma unroll
+                    for (int st = 16; st >= 1; st >>= 1) {
+                        const uint32_t x = __shfl_sync(0xFFFFFFFFu, incl, j + st - 1);
+                        if (x <= b) j += st;
+                    }
+                    const uint32_t ex = __shfl_sync(0xFFFFFFFFu, incl, j ? j - 1 : 0);
+                    const uint32_t f = __shfl_sync(0xFFFFFFFFu, from, j & 31);
+                    const uint32_t dj = __shfl_sync(0xFFFFFFFFu, dx, j & 31);
+                    const uint32_t k = b - (j ? ex : 0u);
+                    si[u] = f + k;
+                    di[u] = dj + k;
                 }
-                const uint32_t ex = __shfl_sync(0xFFFFFFFFu, incl, j ? j - 1 : 0);
-                const uint32_t f = __shfl_sync(0xFFFFFFFFu, from, j & 31);
-                if (b < tl) dl[b] = tile_src[f + (b - (j ? ex : 0u))];
+                uint8_t vb[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) vb[u] = b0 + 32 * u + lane < ts ? tile_src[si[u]] : 0;
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (b0 + 32 * u + lane < ts) dl[di[u]] = vb[u];
+            }
+            uint32_t lm = __ballot_sync(0xFFFFFFFFu, lng);
+            while (lm) {
+                const uint32_t j = __ffs(lm) - 1;
+                lm &= lm - 1;
+                warp_copy_hist(dl + __shfl_sync(0xFFFFFFFFu, dx, j), tile_src + __shfl_sync(0xFFFFFFFFu, from, j),
+                               __shfl_sync(0xFFFFFFFFu, cl, j), nullptr, lane);
             }
         }
 #pragma unroll
@@ -407,53 +494,6 @@ __global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __re
 // privatised per warp in shared memory.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kGatherThreads = 512;
-
-__device__ __forceinline__ void hist4(uint32_t* h, uint32_t w) {
-    atomicAdd(&h[w & 0xFFu], 1u);
-    atomicAdd(&h[(w >> 8) & 0xFFu], 1u);
-    atomicAdd(&h[(w >> 16) & 0xFFu], 1u);
-    atomicAdd(&h[w >> 24], 1u);
-}
-
-// Copies n bytes s -> d with the warp and counts them into h (shared, may be
-// null): bytes up to d's first 16-byte boundary, then one aligned 16-byte
-// store per lane per step (source words loaded aligned and funnel-shifted,
-// so reading up to 3 bytes past s + n: the slot blocks have room), then the
-// tail bytes.
-__device__ void warp_copy_hist(uint8_t* __restrict__ d, const uint8_t* __restrict__ s, uint32_t n,
-                               uint32_t* __restrict__ h, uint32_t lane) {
-    const uint32_t head = min(n, (uint32_t)((16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15));
-    if (lane < head) {
-        const uint8_t b = s[lane];
-        d[lane] = b;
-        if (h) atomicAdd(&h[b], 1u);
-    }
-    d += head;
-    s += head;
-    n -= head;
-    const uint32_t nv = n / 16;
-    const uint32_t sh = 8 * (uint32_t)(reinterpret_cast<uintptr_t>(s) & 3);
-    const uint32_t* sw = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(s) & ~uintptr_t(3));
-    uint4* d4 = reinterpret_cast<uint4*>(d);
-    for (uint32_t v = lane; v < nv; v += 32) {
-        const uint32_t* q = sw + 4 * v;
-        uint4 o;
-        if (sh == 0) {
-            o = make_uint4(q[0], q[1], q[2], q[3]);
-        } else {
-            const uint32_t w4 = q[4];
-            o = make_uint4(__funnelshift_r(q[0], q[1], sh), __funnelshift_r(q[1], q[2], sh),
-                           __funnelshift_r(q[2], q[3], sh), __funnelshift_r(q[3], w4, sh));
-        }
-        d4[v] = o;
-        if (h) { hist4(h, o.x); hist4(h, o.y); hist4(h, o.z); hist4(h, o.w); }
-    }
-    for (uint32_t i = 16 * nv + lane; i < n; i += 32) {
-        const uint8_t b = s[i];
-        d[i] = b;
-        if (h) atomicAdd(&h[b], 1u);
-    }
-}
 
 __global__ void __launch_bounds__(kGatherThreads) k_gather(const Job* __restrict__ jobs, uint32_t njobs,
                                                           const uint8_t* __restrict__ slots,
