@@ -124,6 +124,7 @@ struct przmg_batch {
     // staging belong to the batch, so batches on different streams never
     // share scratch
     DevBuf d_rtiles, d_rx_cnt, d_rx_parts, d_rx_ent, d_rx_key, d_rx_pred, d_stage_in, d_stage_out, d_stage_offs, d_up_offs;
+    DevBuf d_tile_sched;  // tokenizer tile weights [0, ntiles) and walk order [ntiles, 2 ntiles)
     HostBuf h_offs;
     std::vector<RxTile> rtiles;
     uint64_t max_big_cand = 0;  // most radix candidates of one frame
@@ -141,7 +142,7 @@ struct przmg_batch {
         DevBuf* all[] = {&d_in, &d_jobs, &d_small, &d_big, &d_tiles, &d_desc, &d_slots, &d_tile_lens, &d_streams,
                          &d_job_lens, &d_hist, &d_tabs, &d_infos, &d_ans, &d_outs, &d_plans, &d_sizes, &d_out, &d_misc,
                          &d_lists, &d_rtiles, &d_rx_cnt, &d_rx_parts, &d_rx_ent, &d_rx_key, &d_rx_pred, &d_stage_in,
-                         &d_stage_out, &d_stage_offs, &d_up_offs};
+                         &d_stage_out, &d_stage_offs, &d_up_offs, &d_tile_sched};
         for (DevBuf* b : all) b->release();
         h_offs.release();
     }
@@ -231,6 +232,7 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     CK(b->d_small.ensure(sizeof(TileRef) * std::max<uint32_t>(b->nsmall, 1)));
     CK(b->d_big.ensure(sizeof(uint32_t) * std::max<uint32_t>(b->nbig, 1)));
     CK(b->d_tiles.ensure(sizeof(TokTile) * std::max<size_t>(b->tiles.size(), 1)));
+    CK(b->d_tile_sched.ensure(2 * sizeof(uint32_t) * std::max<size_t>(b->tiles.size(), 1)));
     CK(b->d_desc.ensure(b->desc_words * 4));
     CK(b->d_slots.ensure((size_t)b->ntiles * kSlotStride));
     CK(b->d_tile_lens.ensure((size_t)b->ntiles * S_COUNT * 4));
@@ -324,8 +326,15 @@ static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cuda
     CK(mark(2));
     if (stop_after >= 1 && !b->tiles.empty()) {
         const uint32_t nt = (uint32_t)b->tiles.size();
+        uint32_t* tile_w = b->d_tile_sched.as<uint32_t>();
+        uint32_t* tile_order = tile_w + nt;
+        k_tile_weight<<<std::min<uint32_t>(nt, 16u * c->sms), 256, 0, s>>>(b->d_jobs.as<Job>(), b->d_tiles.as<TokTile>(), nt,
+                                                                          b->d_desc.as<uint32_t>(), tile_w);
+        CK(cudaGetLastError());
+        k_tile_order<<<1, 1024, 0, s>>>(tile_w, nt, tile_order);
+        CK(cudaGetLastError());
         k_tokenize<<<(nt + kTokWarps - 1) / kTokWarps, kTokWarps * 32, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_tiles.as<TokTile>(), nt,
-                                               b->d_desc.as<uint32_t>(), b->d_slots.as<uint8_t>(),
+                                               tile_order, b->d_desc.as<uint32_t>(), b->d_slots.as<uint8_t>(),
                                                b->d_tile_lens.as<uint32_t>(), b->err_word());
         CK(cudaGetLastError());
         CK(mark(3));
@@ -335,7 +344,7 @@ static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cuda
             b->d_jobs.as<Job>(), b->njobs, b->d_slots.as<uint8_t>(), b->d_tile_lens.as<uint32_t>(),
             b->d_streams.as<uint8_t>(), b->d_job_lens.as<uint32_t>(), b->d_hist.as<uint32_t>(), b->err_word());
         CK(cudaGetLastError());
-        launches += 2;
+        launches += 4;
     } else {
         CK(mark(3));
     }

@@ -150,4 +150,22 @@ __device__ __forceinline__ uint32_t pack_match32(uint32_t len, uint32_t off) {
     return ((len > kMaxLen32 ? kMaxLen32 : len) << 20) | (off & 0xFFFFFu);
 }
 
+// Spreads the 16 bits of v to the even bit positions of a 32-bit word.
+__device__ __forceinline__ uint32_t spread16(uint32_t v) {
+    v = (v | (v << 8)) & 0x00FF00FFu;
+    v = (v | (v << 4)) & 0x0F0F0F0Fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+// Spreads the low 8 bits of v to bit positions 0, 4, 8, ..., 28.
+__device__ __forceinline__ uint32_t spread8_4(uint32_t v) {
+    v &= 0xFFu;
+    v = (v | (v << 12)) & 0x000F000Fu;
+    v = (v | (v << 6)) & 0x03030303u;
+    v = (v | (v << 3)) & 0x11111111u;
+    return v;
+}
+
 }  // namespace pz

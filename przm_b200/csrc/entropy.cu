@@ -381,15 +381,6 @@ __device__ __forceinline__ void words16(const uint4* c, uint32_t* w) {
     for (int v = 0; v < 4; v++) { w[4 * v] = c[v].x; w[4 * v + 1] = c[v].y; w[4 * v + 2] = c[v].z; w[4 * v + 3] = c[v].w; }
 }
 
-// Spreads the 16 bits of v to the even bit positions of a 32-bit word.
-__device__ __forceinline__ uint32_t spread16(uint32_t v) {
-    v = (v | (v << 8)) & 0x00FF00FFu;
-    v = (v | (v << 4)) & 0x0F0F0F0Fu;
-    v = (v | (v << 2)) & 0x33333333u;
-    v = (v | (v << 1)) & 0x55555555u;
-    return v;
-}
-
 // The 16 chain steps of one full group with the entries already in
 // registers; writes the group's records and its 2-bit count word.
 __device__ __forceinline__ void encode_group(uint32_t& x, uint32_t& cnt, const EncSym* e, int32_t g, uint4* r4,

@@ -324,6 +324,7 @@ __device__ void tok_emit(const uint4* rec, uint32_t nrec, const uint8_t* tile_sr
 
 __global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
                                                             const TokTile* __restrict__ tiles, uint32_t ntiles,
+                                                            const uint32_t* __restrict__ order,
                                                             const uint32_t* __restrict__ desc, uint8_t* __restrict__ slots,
                                                             uint32_t* __restrict__ tile_lens, uint32_t* __restrict__ err) {
     __shared__ TokSmem s_tok[kTokWarps];
@@ -332,7 +333,7 @@ __global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __re
     const uint32_t wid = blockIdx.x * kTokWarps + warp;
     const uint32_t nw = gridDim.x * kTokWarps;
     for (uint32_t T = wid; T < ntiles; T += nw) {
-        const TokTile tt = tiles[T];
+        const TokTile tt = tiles[order[T]];
         const Job job = jobs[tt.job];
         const uint8_t* src = in + job.in_off;
         const uint32_t* dj = desc + job.desc_off;
@@ -351,47 +352,78 @@ __global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __re
         uint32_t pos = start, litStart = start, nrec = 0;
         uint32_t wb = 0xFFFFFFFFu, wsum = 0;  // window base entry; bit k: word k of the window has a descriptor
         auto refill = [&](uint32_t base) {
-            // entries [base, base + kTokWin): descriptors to shared memory, bitmaps to registers
+            // entries [base, base + kTokWin): descriptors to shared memory, one
+            // bitmap word per lane.  Every load instruction of the warp reads
+            // 512 contiguous bytes; the bitmaps are put together from ballots.
             __syncwarp();
             wb = base;
-            const uint32_t e0 = base + 32 * lane;
-            uint32_t nz = 0, eq = 0;
-#pragma unroll 4
-            for (uint32_t k = 0; k < 32; k++) {
-                const uint32_t e = e0 + k;
-                const uint32_t v = e < e_hi ? __ldg(dj + e) : 0u;
-                sm.desc[32 * lane + k] = v;
-                nz |= (v != 0 ? 1u : 0u) << k;
-            }
-            if (nz) {  // equal-4-byte bits of the lane's 32 entries, from vector loads
-                if (radix) {
-                    // candidate e0 + k starts at byte 8(e0 + k); uint4 i covers candidates
-                    // e0 + 2i and e0 + 2i + 1 (loaded only below e_hi, so 8 e_hi + 8 <= n + 8)
-                    const uint4* s4 = reinterpret_cast<const uint4*>(src + 8ull * e0);
+            // descriptors: round i, lane t holds entries 128 i + 4 t .. + 3, so
+            // bit 4u + b of word k is component b of lane 8 (k & 3) + u in
+            // round k >> 2
+            uint32_t cap0 = 0, cap1 = 0, cap2 = 0, cap3 = 0;
 #pragma unroll
-                    for (uint32_t i = 0; i < 16; i++) {
-                        if (e0 + 2 * i >= e_hi) break;
-                        const uint4 v = __ldg(s4 + i);
-                        eq |= (v.x == 0x01010101u * (v.x & 0xFFu) ? 1u : 0u) << (2 * i);
-                        eq |= (v.z == 0x01010101u * (v.z & 0xFFu) ? 1u : 0u) << (2 * i + 1);
-                    }
-                } else {
-                    // positions e0 .. e0 + 31 (e0 is 32-aligned, inputs are 16-aligned
-                    // and padded by 64 bytes past n)
-                    const uint4* s4 = reinterpret_cast<const uint4*>(src + e0);
-                    const uint4 a = __ldg(s4), b = __ldg(s4 + 1), c = __ldg(s4 + 2);
-                    const uint32_t w[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+            for (uint32_t h = 0; h < 8; h += 4) {
+                uint4 v[4];
 #pragma unroll
-                    for (uint32_t k = 0; k < 32; k++) {
-                        const uint32_t x = (k & 3) ? __funnelshift_r(w[k >> 2], w[(k >> 2) + 1], 8 * (k & 3)) : w[k >> 2];
-                        eq |= (x == 0x01010101u * (x & 0xFFu) ? 1u : 0u) << k;
+                for (uint32_t u = 0; u < 4; u++) {
+                    const uint32_t e = base + 128 * (h + u) + 4 * lane;
+                    v[u] = make_uint4(0u, 0u, 0u, 0u);
+                    if (e < e_hi) {  // dj + e is 16-byte aligned; the array holds whole uint4s below e_hi
+                        v[u] = __ldg(reinterpret_cast<const uint4*>(dj + e));
+                        if (e + 1 >= e_hi) v[u].y = 0;
+                        if (e + 2 >= e_hi) v[u].z = 0;
+                        if (e + 3 >= e_hi) v[u].w = 0;
                     }
                 }
-                eq &= nz;
+#pragma unroll
+                for (uint32_t u = 0; u < 4; u++) {
+                    *reinterpret_cast<uint4*>(&sm.desc[128 * (h + u) + 4 * lane]) = v[u];
+                    const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, v[u].x != 0), b1 = __ballot_sync(0xFFFFFFFFu, v[u].y != 0);
+                    const uint32_t b2 = __ballot_sync(0xFFFFFFFFu, v[u].z != 0), b3 = __ballot_sync(0xFFFFFFFFu, v[u].w != 0);
+                    if ((lane >> 2) == h + u) { cap0 = b0; cap1 = b1; cap2 = b2; cap3 = b3; }
+                }
+            }
+            const uint32_t s8 = 8 * (lane & 3);
+            const uint32_t nz = spread8_4(cap0 >> s8) | (spread8_4(cap1 >> s8) << 1) | (spread8_4(cap2 >> s8) << 2) |
+                                (spread8_4(cap3 >> s8) << 3);
+            wsum = __ballot_sync(0xFFFFFFFFu, nz != 0);
+            uint32_t eq = 0;
+            if (radix) {
+                // candidate base + r starts at byte 8 (base + r); uint4 u = 32 i + t
+                // covers candidates 2u and 2u + 1, so bits 2v and 2v + 1 of word k
+                // are lane 16 (k & 1) + v of round k >> 1 (rounds whose two words
+                // hold no descriptor are skipped)
+                const uint4* s4 = reinterpret_cast<const uint4*>(src + 8ull * base);
+                uint32_t capa = 0, capb = 0;
+#pragma unroll 4
+                for (uint32_t i = 0; i < 16; i++) {
+                    if (((wsum >> (2 * i)) & 3u) == 0) continue;
+                    const uint32_t u = 32 * i + lane;
+                    bool ea = false, eb = false;
+                    if (base + 2 * u < e_hi) {  // bytes below 8 e_hi + 8 <= n + 8
+                        const uint4 v = __ldg(s4 + u);
+                        ea = v.x == 0x01010101u * (v.x & 0xFFu);
+                        eb = v.z == 0x01010101u * (v.z & 0xFFu);
+                    }
+                    const uint32_t ba = __ballot_sync(0xFFFFFFFFu, ea), bb = __ballot_sync(0xFFFFFFFFu, eb);
+                    if ((lane >> 1) == i) { capa = ba; capb = bb; }
+                }
+                const uint32_t s16 = 16 * (lane & 1);
+                eq = spread16((capa >> s16) & 0xFFFFu) | (spread16((capb >> s16) & 0xFFFFu) << 1);
+            } else if (nz) {
+                // positions base + 32 lane .. + 31 (32-aligned, inputs are 16-aligned
+                // and padded by 64 bytes past n)
+                const uint4* s4 = reinterpret_cast<const uint4*>(src + base + 32 * lane);
+                const uint4 a = __ldg(s4), b = __ldg(s4 + 1), c = __ldg(s4 + 2);
+                const uint32_t w[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+#pragma unroll
+                for (uint32_t k = 0; k < 32; k++) {
+                    const uint32_t x = (k & 3) ? __funnelshift_r(w[k >> 2], w[(k >> 2) + 1], 8 * (k & 3)) : w[k >> 2];
+                    eq |= (x == 0x01010101u * (x & 0xFFu) ? 1u : 0u) << k;
+                }
             }
             sm.nz[lane] = nz;
-            sm.eq[lane] = eq;
-            wsum = __ballot_sync(0xFFFFFFFFu, nz != 0);
+            sm.eq[lane] = eq & nz;
             __syncwarp();
         };
         while (pos < end && o.ok) {
@@ -484,6 +516,84 @@ __global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __re
             for (int s = 0; s < S_COUNT; s++) tile_lens[S * S_COUNT + s] = o.len[s];
             if (!o.ok) atomicOr(err, (uint32_t)E_SLOT_OVERFLOW);
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tokenizer schedule.  A tile's walk costs about one step per match it takes,
+// and tiles of one batch differ by 10x or more (a tile of short repeats
+// against one of long copies or of no matches at all); walked in list order,
+// heavy tiles that start late would set the kernel's length.  So the tiles
+// are walked heaviest first: the weight of a tile is its number of non-zero
+// match descriptors, and the order buckets tiles by the bit length of that
+// weight.  The order changes no output byte (every tile is parsed alone).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_tile_weight(const Job* __restrict__ jobs, const TokTile* __restrict__ tiles,
+                                                     uint32_t ntiles, const uint32_t* __restrict__ desc,
+                                                     uint32_t* __restrict__ weight) {
+    __shared__ uint32_t s_w[8];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t T = blockIdx.x; T < ntiles; T += gridDim.x) {
+        const TokTile tt = tiles[T];
+        const Job job = jobs[tt.job];
+        const uint32_t start = tt.tile * kTile, end = min(start + kTile, job.n);
+        const uint32_t ncand = job.n >= 8 ? (job.n - 8) / 8 + 1 : 0;
+        // the tile's descriptor entries [e_lo, e_hi), as the walk indexes them;
+        // e_lo is a multiple of 4, so the uint4 loads are aligned, and whole
+        // uint4s below e_hi lie inside the frame's descriptor array
+        const uint32_t e_lo = job.kind != 0 ? min(ncand, start >> 3) : start;
+        const uint32_t e_hi = job.kind != 0 ? min(ncand, (end + 7) >> 3) : end;
+        const uint32_t* dj = desc + job.desc_off;
+        uint32_t c = 0;
+        for (uint32_t e = e_lo + 4 * threadIdx.x; e < e_hi; e += 1024) {
+            const uint4 v = __ldg(reinterpret_cast<const uint4*>(dj + e));
+            c += (v.x != 0 ? 1u : 0u) + (e + 1 < e_hi && v.y != 0 ? 1u : 0u) + (e + 2 < e_hi && v.z != 0 ? 1u : 0u) +
+                 (e + 3 < e_hi && v.w != 0 ? 1u : 0u);
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+        if (lane == 0) s_w[warp] = c;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t t = 0;
+            for (int w = 0; w < 8; w++) t += s_w[w];
+            weight[T] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// order[0, ntiles): tile list indices, heaviest bit-length bucket first.  One
+// block; the warps rank equal buckets together (one shared atomic per bucket
+// and warp).
+__global__ void __launch_bounds__(1024) k_tile_order(const uint32_t* __restrict__ weight, uint32_t ntiles,
+                                                     uint32_t* __restrict__ order) {
+    __shared__ uint32_t s_cnt[33], s_pos[33];
+    const uint32_t tid = threadIdx.x, lane = tid & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    if (tid < 33) s_cnt[tid] = 0;
+    __syncthreads();
+    for (uint32_t b0 = 0; b0 < ntiles; b0 += 1024) {  // uniform trip count: every lane takes part in the match
+        const uint32_t T = b0 + tid;
+        const uint32_t k = T < ntiles ? 32u - __clz(weight[T]) : 33u;
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, k);
+        if (k < 33 && (peers & lt) == 0) atomicAdd(&s_cnt[k], __popc(peers));
+    }
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t a = 0;
+        for (int k = 32; k >= 0; k--) { s_pos[k] = a; a += s_cnt[k]; }
+    }
+    __syncthreads();
+    for (uint32_t b0 = 0; b0 < ntiles; b0 += 1024) {
+        const uint32_t T = b0 + tid;
+        const uint32_t k = T < ntiles ? 32u - __clz(weight[T]) : 33u;
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, k);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (k < 33 && lane == leader) base = atomicAdd(&s_pos[k], __popc(peers));
+        base = __shfl_sync(0xFFFFFFFFu, base, leader);
+        if (k < 33) order[base + __popc(peers & lt)] = T;
     }
 }
 
