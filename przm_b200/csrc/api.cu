@@ -116,6 +116,7 @@ struct przmg_batch {
     std::vector<TileRef> small;
     std::vector<uint32_t> big;
     std::vector<TokTile> tiles;
+    std::vector<uint2> asm_items;  // every frame's part 0 first, then the literal parts
     std::vector<uint64_t> in_offs, out_offs, up_offs;
     uint64_t in_bytes = 0, desc_words = 0, stream_bytes = 0, ans_bytes = 0, out_bytes = 0;
     DevBuf d_in, d_jobs, d_small, d_big, d_tiles, d_desc, d_slots, d_tile_lens, d_streams, d_job_lens, d_hist, d_tabs,
@@ -125,6 +126,7 @@ struct przmg_batch {
     // share scratch
     DevBuf d_rtiles, d_rx_cnt, d_rx_parts, d_rx_ent, d_rx_key, d_rx_pred, d_stage_in, d_stage_out, d_stage_offs, d_up_offs;
     DevBuf d_tile_sched;  // tokenizer tile weights [0, ntiles) and walk order [ntiles, 2 ntiles)
+    DevBuf d_asm;         // assembly work items (frame, part)
     HostBuf h_offs;
     std::vector<RxTile> rtiles;
     uint64_t max_big_cand = 0;  // most radix candidates of one frame
@@ -142,7 +144,7 @@ struct przmg_batch {
         DevBuf* all[] = {&d_in, &d_jobs, &d_small, &d_big, &d_tiles, &d_desc, &d_slots, &d_tile_lens, &d_streams,
                          &d_job_lens, &d_hist, &d_tabs, &d_infos, &d_ans, &d_outs, &d_plans, &d_sizes, &d_out, &d_misc,
                          &d_lists, &d_rtiles, &d_rx_cnt, &d_rx_parts, &d_rx_ent, &d_rx_key, &d_rx_pred, &d_stage_in,
-                         &d_stage_out, &d_stage_offs, &d_up_offs, &d_tile_sched};
+                         &d_stage_out, &d_stage_offs, &d_up_offs, &d_tile_sched, &d_asm};
         for (DevBuf* b : all) b->release();
         h_offs.release();
     }
@@ -223,6 +225,10 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     b->nsmall = (uint32_t)b->small.size();
     b->nbig = (uint32_t)b->big.size();
     b->in_bytes = in + 64;
+    b->asm_items.clear();
+    for (uint32_t i = 0; i < njobs; i++) b->asm_items.push_back(make_uint2(i, 0));
+    for (uint32_t i = 0; i < njobs; i++)
+        for (uint32_t k = 0, np = asm_lit_parts(b->jobs[i]); k < np; k++) b->asm_items.push_back(make_uint2(i, k + 1));
     b->desc_words = desc + 16;
     b->stream_bytes = str + 64;
     b->ans_bytes = ans + 64;
@@ -233,6 +239,7 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     CK(b->d_big.ensure(sizeof(uint32_t) * std::max<uint32_t>(b->nbig, 1)));
     CK(b->d_tiles.ensure(sizeof(TokTile) * std::max<size_t>(b->tiles.size(), 1)));
     CK(b->d_tile_sched.ensure(2 * sizeof(uint32_t) * std::max<size_t>(b->tiles.size(), 1)));
+    CK(b->d_asm.ensure(sizeof(uint2) * std::max<size_t>(b->asm_items.size(), 1)));
     CK(b->d_desc.ensure(b->desc_words * 4));
     CK(b->d_slots.ensure((size_t)b->ntiles * kSlotStride));
     CK(b->d_tile_lens.ensure((size_t)b->ntiles * S_COUNT * 4));
@@ -268,6 +275,8 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     if (b->nbig) CK(cudaMemcpyAsync(b->d_big.p, b->big.data(), sizeof(uint32_t) * b->nbig, cudaMemcpyHostToDevice, s));
     if (!b->tiles.empty())
         CK(cudaMemcpyAsync(b->d_tiles.p, b->tiles.data(), sizeof(TokTile) * b->tiles.size(), cudaMemcpyHostToDevice, s));
+    if (!b->asm_items.empty())
+        CK(cudaMemcpyAsync(b->d_asm.p, b->asm_items.data(), sizeof(uint2) * b->asm_items.size(), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(b->d_sizes.p, 0, (size_t)njobs * 4 + 16, s));
     CK(cudaMemsetAsync(b->d_job_lens.p, 0, (size_t)njobs * S_COUNT * 4 + 16, s));
     // the host-side vectors above must stay alive until the copies ran
@@ -380,8 +389,9 @@ static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cuda
                                                       b->d_sizes.as<uint32_t>());
         CK(cudaGetLastError());
         CK(mark(7));
-        k_assemble<<<std::min<uint32_t>(b->njobs, 16u * c->sms), kAsmThreads, 0, s>>>(
-            b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->njobs, b->d_job_lens.as<uint32_t>(), b->d_plans.as<Plan>(),
+        const uint32_t nitems = (uint32_t)b->asm_items.size();
+        k_assemble<<<std::max<uint32_t>(1, std::min<uint32_t>(nitems, 1u << 20)), kAsmThreads, 0, s>>>(
+            b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_asm.as<uint2>(), nitems, b->d_job_lens.as<uint32_t>(), b->d_plans.as<Plan>(),
             b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(), b->d_streams.as<uint8_t>(), b->d_ans.as<uint8_t>(),
             b->d_out.as<uint8_t>());
         CK(cudaGetLastError());

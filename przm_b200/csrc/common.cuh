@@ -71,12 +71,18 @@ __host__ __device__ inline uint64_t stream_region_bytes(const Job& j) {
     return 4ull * j.cmd_cap + j.off_cap + j.lit_cap;
 }
 
-// ANS scratch of one task: four lane byte streams then four lane count
-// words (2 bits per round).  L = symbol capacity of the task's stream.
-// lane streams are written in 64-byte chunks (64-byte aligned), so every lane
-// region is a multiple of 64 with room for the last partial chunk
+// ANS scratch of one task: four lane byte streams, then per lane its count
+// words (2 bits per round) followed by its running byte count at every
+// kStitchRounds-th round (the bytes of rounds >= 4096 k, k = 0, 1, ...), from
+// which a stitch pass finds its output offset without the passes before it.
+// L = symbol capacity of the task's stream.  Lane streams are written in
+// 64-byte chunks (64-byte aligned), so every lane region is a multiple of 64
+// with room for the last partial chunk.
+constexpr uint32_t kStitchRounds = 4096;  // rounds of one stitch pass (256 threads x 16)
 __host__ __device__ inline uint64_t ans_lane_cap(uint32_t L) { return ((2ull * ((L + 3) / 4) + 128) + 63) & ~63ull; }
-__host__ __device__ inline uint64_t ans_nbw_cap(uint32_t L) { return (((L + 3) / 4) + 15) / 16 + 1; }  // u32 words
+__host__ __device__ inline uint64_t ans_nbw_words(uint32_t L) { return (((L + 3) / 4) + 15) / 16 + 1; }
+__host__ __device__ inline uint64_t ans_cum_words(uint32_t L) { return ((L + 3) / 4 + kStitchRounds - 1) / kStitchRounds + 1; }
+__host__ __device__ inline uint64_t ans_nbw_cap(uint32_t L) { return ans_nbw_words(L) + ans_cum_words(L); }  // u32 words
 __host__ __device__ inline uint64_t ans_task_bytes(uint32_t L) {
     uint64_t b = 4 * ans_lane_cap(L) + 4 * 4 * ans_nbw_cap(L);
     return (b + 63) & ~63ull;

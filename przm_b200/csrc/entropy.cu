@@ -330,12 +330,14 @@ __global__ void k_normalize(const Job* __restrict__ jobs, uint32_t njobs, const 
 struct LaneIO {
     uint8_t* bytes;     // lane byte stream
     uint32_t* nbw;      // 2-bit emitted-byte counts, 16 rounds per word (round j -> word j/16)
+    uint32_t* cum;      // cum[k]: bytes of rounds >= kStitchRounds k (written where the lane has round kStitchRounds k)
 };
 
 __device__ __forceinline__ LaneIO lane_io(uint8_t* task_base, uint32_t cap, uint32_t l) {
     LaneIO io;
     io.bytes = task_base + (uint64_t)l * ans_lane_cap(cap);
     io.nbw = reinterpret_cast<uint32_t*>(task_base + 4 * ans_lane_cap(cap)) + (uint64_t)l * ans_nbw_cap(cap);
+    io.cum = io.nbw + ans_nbw_words(cap);
     return io;
 }
 
@@ -461,6 +463,7 @@ __device__ __forceinline__ void rans_lane(const uint8_t* __restrict__ src, uint3
                     io.nbw[j >> 4] = acc;
                     acc = 0;
                 }
+                if ((j & (kStitchRounds - 1)) == 0) io.cum[j / kStitchRounds] = cnt;
             }
         }
         if (G > 0) {
@@ -489,6 +492,7 @@ __device__ __forceinline__ void rans_lane(const uint8_t* __restrict__ src, uint3
                 // the slot of group g is free once its words are in registers
                 ring_fetch(ring, t, g, s4, max(g - kRing, 0));
                 encode_group(x, cnt, e, g, r4, io.nbw);
+                if ((g & (kStitchRounds / 16 - 1)) == 0) io.cum[g / (kStitchRounds / 16)] = cnt;
 #pragma unroll
                 for (int v = 0; v < 4; v++) cur[v] = nxt[v];
             }
@@ -692,81 +696,98 @@ struct StitchStage {
     static constexpr uint32_t kBytes = NT * 16 * 8 + 16;
 };
 
-// Every pass: thread t takes rounds [r0 + 16t, r0 + 16t + 16) of the four
-// lanes (two 16-byte loads of records and one count word per lane), one
-// block scan gives its byte offset, it writes its bytes into a shared
-// staging buffer placed at the output's 16-byte phase, and the block then
-// stores the staged run with aligned 16-byte stores (byte stores only for
-// the partial first and last 16 bytes of the run).
+// One stitch pass: thread t takes rounds [r0 + 16t, r0 + 16t + 16) of the
+// four lanes (two 16-byte loads of records and one count word per lane), one
+// block scan gives its byte offset, it writes its bytes into a shared staging
+// buffer placed at the output's 16-byte phase, and the block then stores the
+// staged run at dst with aligned 16-byte stores (byte stores only for the
+// partial first and last 16 bytes of the run).  Returns the run's length.
 template <int NT>
-__device__ void block_stitch(const uint8_t* task_base, uint32_t cap, uint32_t n, uint8_t* __restrict__ out) {
+__device__ uint32_t stitch_pass(const uint8_t* task_base, uint32_t cap, uint32_t n, uint32_t r0, uint8_t* __restrict__ dst) {
     __shared__ uint32_t s_warp[32];
     __shared__ __align__(16) uint8_t s_stage[StitchStage<NT>::kBytes];
     const uint32_t tid = threadIdx.x;
     const uint32_t rounds = (n + 3) / 4;
-    const uint16_t* raw[4];
-    const uint32_t* nw[4];
+    const uint32_t rb = r0 + 16 * tid;  // first round of this thread (multiple of 16)
+    uint32_t w[4] = {0, 0, 0, 0}, c = 0;
+    uint4 rv[4][2];
+#pragma unroll
     for (uint32_t l = 0; l < 4; l++) {
-        raw[l] = reinterpret_cast<const uint16_t*>(task_base + (uint64_t)l * ans_lane_cap(cap));
-        nw[l] = reinterpret_cast<const uint32_t*>(task_base + 4 * ans_lane_cap(cap)) + (uint64_t)l * ans_nbw_cap(cap);
+        rv[l][0] = rv[l][1] = make_uint4(0, 0, 0, 0);
+        if (rb >= rounds || n <= l) continue;
+        const uint32_t jmax = (n - 1 - l) / 4;
+        if (rb > jmax) continue;
+        const uint16_t* raw = reinterpret_cast<const uint16_t*>(task_base + (uint64_t)l * ans_lane_cap(cap));
+        const uint32_t* nw = reinterpret_cast<const uint32_t*>(task_base + 4 * ans_lane_cap(cap)) + (uint64_t)l * ans_nbw_cap(cap);
+        uint32_t v = nw[rb >> 4];
+        const uint32_t top = jmax - rb;  // rounds of this word the lane has
+        if (top < 15) v &= (1u << (2 * (top + 1))) - 1u;
+        w[l] = v;
+        c += sum2(v);
+        // rounds past jmax are in the lane region (it holds ceil(cap/4) + 64 records) and masked by w
+        const uint4* rp = reinterpret_cast<const uint4*>(raw + rb);
+        rv[l][0] = rp[0];
+        rv[l][1] = rp[1];
     }
-    uint32_t carry = 0;
-    for (uint32_t r0 = 0; r0 < rounds; r0 += 16 * NT) {
-        const uint32_t rb = r0 + 16 * tid;  // first round of this thread (multiple of 16)
-        uint32_t w[4] = {0, 0, 0, 0}, c = 0;
-        uint4 rv[4][2];
+    uint32_t total;
+    const uint32_t excl = block_exclusive_scan<NT>(c, s_warp, total);
+    const uint32_t a = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15);
+    uint32_t q = a + excl;
 #pragma unroll
-        for (uint32_t l = 0; l < 4; l++) {
-            rv[l][0] = rv[l][1] = make_uint4(0, 0, 0, 0);
-            if (rb >= rounds || n <= l) continue;
-            const uint32_t jmax = (n - 1 - l) / 4;
-            if (rb > jmax) continue;
-            uint32_t v = nw[l][rb >> 4];
-            const uint32_t top = jmax - rb;  // rounds of this word the lane has
-            if (top < 15) v &= (1u << (2 * (top + 1))) - 1u;
-            w[l] = v;
-            c += sum2(v);
-            // rounds past jmax are in the lane region (it holds ceil(cap/4) + 64 records) and masked by w
-            const uint4* rp = reinterpret_cast<const uint4*>(raw[l] + rb);
-            rv[l][0] = rp[0];
-            rv[l][1] = rp[1];
-        }
-        uint32_t total;
-        const uint32_t excl = block_exclusive_scan<NT>(c, s_warp, total);
-        uint8_t* dst = out + carry;
-        const uint32_t a = (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15);
-        uint32_t q = a + excl;
+    for (int r = 0; r < 16; r++) {
 #pragma unroll
-        for (int r = 0; r < 16; r++) {
-#pragma unroll
-            for (int l = 0; l < 4; l++) {
-                const uint32_t k = (w[l] >> (2 * r)) & 3u;
-                if (!k) continue;
-                const uint32_t v = rec16(rv[l], r);
-                if (k == 2) {
-                    s_stage[q] = (uint8_t)(v >> 8);
-                    s_stage[q + 1] = (uint8_t)v;
-                    q += 2;
-                } else {
-                    s_stage[q] = (uint8_t)v;
-                    q += 1;
-                }
-            }
-        }
-        __syncthreads();
-        uint8_t* g0 = dst - a;  // 16-byte aligned; only bytes [a, a + total) are written
-        const uint32_t end = a + total, nch = (end + 15) / 16;
-        for (uint32_t ch = tid; ch < nch; ch += NT) {
-            const uint32_t lo = ch * 16, hi = lo + 16;
-            if (lo >= a && hi <= end) {
-                *reinterpret_cast<uint4*>(g0 + lo) = *reinterpret_cast<const uint4*>(s_stage + lo);
+        for (int l = 0; l < 4; l++) {
+            const uint32_t k = (w[l] >> (2 * r)) & 3u;
+            if (!k) continue;
+            const uint32_t v = rec16(rv[l], r);
+            if (k == 2) {
+                s_stage[q] = (uint8_t)(v >> 8);
+                s_stage[q + 1] = (uint8_t)v;
+                q += 2;
             } else {
-                for (uint32_t b = lo > a ? lo : a; b < (hi < end ? hi : end); b++) g0[b] = s_stage[b];
+                s_stage[q] = (uint8_t)v;
+                q += 1;
             }
         }
-        __syncthreads();  // the staging buffer is reused by the next pass
-        carry += total;
     }
+    __syncthreads();
+    uint8_t* g0 = dst - a;  // 16-byte aligned; only bytes [a, a + total) are written
+    const uint32_t end = a + total, nch = (end + 15) / 16;
+    for (uint32_t ch = tid; ch < nch; ch += NT) {
+        const uint32_t lo = ch * 16, hi = lo + 16;
+        if (lo >= a && hi <= end) {
+            *reinterpret_cast<uint4*>(g0 + lo) = *reinterpret_cast<const uint4*>(s_stage + lo);
+        } else {
+            for (uint32_t b = lo > a ? lo : a; b < (hi < end ? hi : end); b++) g0[b] = s_stage[b];
+        }
+    }
+    __syncthreads();  // the staging buffer is reused by the next pass
+    return total;
+}
+
+// The whole stream, pass after pass, by one block.
+template <int NT>
+__device__ void block_stitch(const uint8_t* task_base, uint32_t cap, uint32_t n, uint8_t* __restrict__ out) {
+    const uint32_t rounds = (n + 3) / 4;
+    uint32_t carry = 0;
+    for (uint32_t r0 = 0; r0 < rounds; r0 += 16 * NT) carry += stitch_pass<NT>(task_base, cap, n, r0, out + carry);
+}
+
+// Output offset of the stitch pass starting at round r0 (a multiple of
+// kStitchRounds): the bytes of all rounds below r0, from each lane's total
+// and its recorded count of the rounds from r0 up.
+__device__ __forceinline__ uint32_t stitch_offset(const uint8_t* task_base, uint32_t cap, uint32_t n, const TaskOut& o,
+                                                  uint32_t r0) {
+    uint32_t off = 0;
+#pragma unroll
+    for (uint32_t l = 0; l < 4; l++) {
+        if (n <= l) continue;
+        const uint32_t jmax = (n - 1 - l) / 4;
+        const uint32_t* cum = reinterpret_cast<const uint32_t*>(task_base + 4 * ans_lane_cap(cap)) +
+                              (uint64_t)l * ans_nbw_cap(cap) + ans_nbw_words(cap);
+        off += o.count[l] - (r0 <= jmax ? cum[r0 / kStitchRounds] : 0u);
+    }
+    return off;
 }
 
 }  // namespace pz

@@ -132,27 +132,45 @@ __device__ inline void put32(uint8_t* p, uint32_t v) {
     p[0] = (uint8_t)v; p[1] = (uint8_t)(v >> 8); p[2] = (uint8_t)(v >> 16); p[3] = (uint8_t)(v >> 24);
 }
 
-// container: 'V','A',01,flags | LE32 n | [matrix] | 4 x LE32 state | stream
-__device__ uint32_t write_container(uint8_t* dst, uint8_t flags, uint32_t n, const TableInfo* info, const TaskOut& o,
-                                    const uint8_t* task_base, uint32_t cap) {
-    uint32_t h = 8 + (info ? info->mat_len : 0);
+// container: 'V','A',01,flags | LE32 n | [matrix] | 4 x LE32 state | stream.
+// Writes everything but the stream; returns the stream's offset.
+__device__ uint32_t container_head(uint8_t* dst, uint8_t flags, uint32_t n, const TableInfo* info, const TaskOut& o) {
+    const uint32_t h = 8 + (info ? info->mat_len : 0);
     if (threadIdx.x == 0) {
         dst[0] = 'V'; dst[1] = 'A'; dst[2] = 0x01; dst[3] = flags;
         put32(dst + 4, n);
         for (int k = 0; k < 4; k++) put32(dst + h + 4 * k, o.state[k]);
     }
     if (info) block_copy(dst + 8, info->mat, info->mat_len);
-    block_stitch<kAsmThreads>(task_base, cap, n, dst + h + 16);
-    return h + 16 + tsum(o);
+    return h + 16;
 }
 
+__device__ void write_container(uint8_t* dst, uint8_t flags, uint32_t n, const TableInfo* info, const TaskOut& o,
+                                const uint8_t* task_base, uint32_t cap) {
+    block_stitch<kAsmThreads>(task_base, cap, n, dst + container_head(dst, flags, n, info, o));
+}
+
+// Frame assembly as independent parts, one block each: part 0 of a frame
+// writes its header and Sections 2 and 3 and the head of Section 4; part
+// k + 1 writes bytes [k kAsmChunk, (k + 1) kAsmChunk) of the Section 4
+// literals (raw) or the k-th stitch pass of their V-ANS stream, at the
+// offset recorded by the rANS lanes, or that slice of an uncompressed frame.
+// So a frame's literals are written by many blocks at once, and every part
+// writes bytes no other part writes.
+constexpr uint32_t kAsmChunk = 4 * kStitchRounds;  // literal bytes (symbols) per part
+static_assert(16 * kAsmThreads == kStitchRounds, "a literal part is one stitch pass");
+
+__host__ __device__ inline uint32_t asm_lit_parts(const Job& j) { return j.n == 0 ? 0u : (j.lit_cap + kAsmChunk - 1) / kAsmChunk; }
+
 __global__ void __launch_bounds__(kAsmThreads) k_assemble(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
-                                                          uint32_t njobs, const uint32_t* __restrict__ job_lens,
+                                                          const uint2* __restrict__ items, uint32_t nitems,
+                                                          const uint32_t* __restrict__ job_lens,
                                                           const Plan* __restrict__ plans, const TableInfo* __restrict__ infos,
                                                           const TaskOut* __restrict__ outs,
                                                           const uint8_t* __restrict__ streams,
                                                           const uint8_t* __restrict__ ans, uint8_t* __restrict__ out) {
-    for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
+    for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const uint32_t j = items[it].x, part = items[it].y;
         const Job job = jobs[j];
         const Plan p = plans[j];
         const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
@@ -161,15 +179,39 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(const uint8_t* __restr
         __syncthreads();
         if (n == 0) continue;
         if (p.uncompressed) {
-            if (threadIdx.x == 0) {
-                f[0] = 'P'; f[1] = 'R'; f[2] = 'Z'; f[3] = 'M'; f[4] = 0x04;
-                f[5] = (uint8_t)n; f[6] = (uint8_t)(n >> 8); f[7] = (uint8_t)(n >> 16);
+            if (part == 0) {
+                if (threadIdx.x == 0) {
+                    f[0] = 'P'; f[1] = 'R'; f[2] = 'Z'; f[3] = 'M'; f[4] = 0x04;
+                    f[5] = (uint8_t)n; f[6] = (uint8_t)(n >> 8); f[7] = (uint8_t)(n >> 16);
+                }
+            } else {
+                const uint32_t lo = (part - 1) * kAsmChunk;
+                if (lo < n) block_copy(f + 8 + lo, in + job.in_off + lo, min(kAsmChunk, n - lo));
             }
-            block_copy(f + 8, in + job.in_off, n);
             continue;
         }
         const bool ext = (p.flags & 0x08) != 0;
         uint32_t w = 8 + (ext ? 6 : 4);
+        const uint8_t* sreg = streams + job.str_off;
+        const uint8_t* abase = ans + job.ans_off;
+        uint8_t* s4 = f + w + 8 + p.l2 + p.l3;
+        if (part > 0) {  // Section 4 literals, part - 1
+            const uint32_t k = part - 1, len = lens[S_LIT];
+            if (p.s4_mode == 1) {
+                const uint32_t r0 = k * kStitchRounds;
+                if (r0 < (len + 3) / 4) {
+                    const TaskOut to = outs[(uint64_t)j * T_COUNT + T_LIT];
+                    const uint8_t* tb = abase + ans_task_off(job, T_LIT);
+                    const uint32_t cap = task_cap(job, T_LIT);
+                    const uint32_t h = 8 + infos[(uint64_t)j * 4].mat_len + 16;
+                    stitch_pass<kAsmThreads>(tb, cap, len, r0, s4 + h + stitch_offset(tb, cap, len, to, r0));
+                }
+            } else {
+                const uint32_t lo = k * kAsmChunk;
+                if (lo < len) block_copy(s4 + lo, sreg + stream_base(job, S_LIT) + lo, min(kAsmChunk, len - lo));
+            }
+            continue;
+        }
         if (threadIdx.x == 0) {
             f[0] = 'P'; f[1] = 'R'; f[2] = 'Z'; f[3] = 'M'; f[4] = (uint8_t)p.flags;
             f[5] = (uint8_t)n; f[6] = (uint8_t)(n >> 8); f[7] = (uint8_t)(n >> 16);
@@ -184,8 +226,6 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(const uint8_t* __restr
             f[w + 1] = (uint8_t)p.wlog;
         }
         w += 8;
-        const uint8_t* sreg = streams + job.str_off;
-        const uint8_t* abase = ans + job.ans_off;
         // Section 2
         uint8_t* s2 = f + w;
         if (job.profile == 0) {
@@ -225,16 +265,9 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(const uint8_t* __restr
         uint8_t* s3 = f + w;
         if (threadIdx.x == 0) { s3[0] = 0x00; put32(s3 + 1, lens[S_OFF]); }
         block_copy(s3 + 5, sreg + stream_base(job, S_OFF), lens[S_OFF]);
-        w += p.l3;
-        // Section 4
-        uint8_t* s4 = f + w;
-        if (p.s4_mode == 1) {
-            const TaskOut to = outs[(uint64_t)j * T_COUNT + T_LIT];
-            write_container(s4, 0x00, lens[S_LIT], infos + (uint64_t)j * 4, to, abase + ans_task_off(job, T_LIT),
-                            task_cap(job, T_LIT));
-        } else {
-            block_copy(s4, sreg + stream_base(job, S_LIT), lens[S_LIT]);
-        }
+        // Section 4: the container head here, the literals in parts 1, 2, ...
+        if (p.s4_mode == 1)
+            container_head(s4, 0x00, lens[S_LIT], infos + (uint64_t)j * 4, outs[(uint64_t)j * T_COUNT + T_LIT]);
     }
 }
 
