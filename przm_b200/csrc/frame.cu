@@ -162,7 +162,8 @@ static_assert(16 * kAsmThreads == kStitchRounds, "a literal part is one stitch p
 
 __host__ __device__ inline uint32_t asm_lit_parts(const Job& j) { return j.n == 0 ? 0u : (j.lit_cap + kAsmChunk - 1) / kAsmChunk; }
 
-__global__ void __launch_bounds__(kAsmThreads) k_assemble(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
+// Four blocks per SM (64 registers): the parts are short and latency-bound.
+__global__ void __launch_bounds__(kAsmThreads, 4) k_assemble(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
                                                           const uint2* __restrict__ items, uint32_t nitems,
                                                           const uint32_t* __restrict__ job_lens,
                                                           const Plan* __restrict__ plans, const TableInfo* __restrict__ infos,

@@ -259,16 +259,24 @@ __global__ void __launch_bounds__(256) k_rx_scatter(const uint8_t* __restrict__ 
 // p + L + 8 <= n and L + 8 <= 4095, then byte by byte below 4095.  Four steps
 // are loaded per round trip (all loads 8-aligned; the input is padded by 64
 // bytes, so words past n are readable and only used where a step allows).
-__device__ __forceinline__ uint32_t rx_match(const uint8_t* src, uint32_t n, uint32_t c, uint32_t q) {
+// rx_first is the first round trip: the XOR of the 32 bytes at the candidate
+// and at its predecessor (loaded whatever the distance; both lie in the
+// frame's padded input).
+__device__ __forceinline__ void rx_first(const uint8_t* src, uint32_t c, uint32_t q, uint64_t* x) {
+    const uint64_t* a = reinterpret_cast<const uint64_t*>(src + 8 * c);
+    const uint64_t* b = reinterpret_cast<const uint64_t*>(src + 8 * q);
+#pragma unroll
+    for (int k = 0; k < 4; k++) x[k] = __ldg(a + k) ^ __ldg(b + k);
+}
+
+// The descriptor of candidate c against predecessor q, given rx_first's words.
+__device__ __forceinline__ uint32_t rx_finish(const uint8_t* src, uint32_t n, uint32_t c, uint32_t q, uint64_t* x) {
     const uint32_t p = c * 8, pq = q * 8;
     const uint32_t dist = p - pq;
     if (dist > kWindow || dist > kMaxOff32) return 0;
+    if (x[0]) return 0;
     const uint64_t* a = reinterpret_cast<const uint64_t*>(src + p);
     const uint64_t* b = reinterpret_cast<const uint64_t*>(src + pq);
-    uint64_t x[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) x[k] = __ldg(a + k) ^ __ldg(b + k);
-    if (x[0]) return 0;
     uint32_t L = 8;
     int k0 = 1;
     for (;;) {
@@ -353,9 +361,18 @@ __global__ void __launch_bounds__(256) k_rx_verify(const uint8_t* __restrict__ i
         const uint32_t* ej = ent + job.desc_off;
         const uint32_t* pj = pred + job.desc_off;
         uint32_t* d8 = desc + job.desc_off;
-        for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < C; i += gridDim.x * 256) {
-            const uint32_t c = ej[i], pv = pj[i];
-            d8[c] = pv ? rx_match(src, job.n, c, pv - 1) : 0u;
+        // two entries per thread per step, their first loads in flight together
+        const uint32_t stride = gridDim.x * 256;
+        for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < C; i += 2 * stride) {
+            const uint32_t i2 = i + stride;
+            const bool two = i2 < C;
+            const uint32_t c1 = ej[i], p1 = pj[i];
+            const uint32_t c2 = two ? ej[i2] : 0u, p2 = two ? pj[i2] : 0u;
+            uint64_t x1[4], x2[4];
+            if (p1) rx_first(src, c1, p1 - 1, x1);
+            if (p2) rx_first(src, c2, p2 - 1, x2);
+            d8[c1] = p1 ? rx_finish(src, job.n, c1, p1 - 1, x1) : 0u;
+            if (two) d8[c2] = p2 ? rx_finish(src, job.n, c2, p2 - 1, x2) : 0u;
         }
     }
 }
