@@ -20,12 +20,13 @@ Ours (default):
   reference's Go compressor cannot be built on this machine (no Go
   toolchain), so the oracle port of the path runs instead on all host cores.
 
-Steps are pipelined: --inflight D (default 5) batches, each with its own
-device buffers, take steps k = 0, 1, ... in turn on D streams, so one
-step's match/tokenize kernels overlap the previous steps' rANS chains
-(which use one warp on ~100 SMs for ~9 ms).  The timed region still spans
-exactly K steps (events joined across the streams); step_latency_ms in
-config is one step alone, submission to completion.
+Steps are pipelined: --inflight D (default 10) batches, each with its own
+device buffers (about 4 GB), take steps k = 0, 1, ... in turn on D streams,
+so one step's match/tokenize/assembly kernels overlap the earlier steps'
+rANS chains (one warp per block, ~8 ms of dependent rounds).  The timed
+region still spans exactly K steps (events joined across the streams), the
+last D of them draining the pipeline; step_latency_ms in config is one step
+alone, submission to completion.
 
 Multi-GPU (torchrun): every rank compresses its own 256 frames (weak
 scaling, no data-path collective); the step time is the max over ranks.
@@ -55,40 +56,66 @@ def frame_seeds_of(rank_seed: int, idx) -> list[int]:
     return [rank_seed + 7919 * i for i in idx]  # = shard.frame_seeds(rank)[i]
 
 
-def _cpu_worker(idx: list[int], rank_seed: int, barrier, q) -> None:
+def _cpu_worker(idx: list[int], rank_seed: int, barrier, cmd, q) -> None:
     sys.path.insert(0, ROOT)
     from oracle import oracle as O
     from przm_b200 import workloads as W
     frames = [W.mixture(s, FRAME)[0] for s in frame_seeds_of(rank_seed, idx)]
     O.lib()
-    barrier.wait()
-    t0 = time.perf_counter()
-    out = 0
-    for a in frames:
-        out += len(O.compress_p1(a))
-    q.put((time.perf_counter() - t0, sum(len(a) for a in frames), out))
+    while cmd.get() is not None:  # one compress of the worker's frames per step
+        barrier.wait()
+        t0 = time.perf_counter()
+        out = 0
+        for a in frames:
+            out += len(O.compress_p1(a))
+        q.put((time.perf_counter() - t0, sum(len(a) for a in frames), out))
+
+
+class CpuPool:
+    """The oracle's entropy-coded compress of `frames` frames spread over
+    `cores` worker processes (spawned: safe beside a CUDA context), kept
+    alive across steps; step() times one pass over all frames."""
+
+    def __init__(self, frames: int, rank_seed: int, cores: int):
+        import multiprocessing as mp
+        ctx = mp.get_context("spawn")
+        self.frames = frames
+        self.cores = max(1, min(cores, frames))
+        # the pool holds the barrier and queues for the workers' lifetime (a
+        # spawned worker reopens them by name after start() returns)
+        self.barrier = ctx.Barrier(self.cores)
+        self.cmd = [ctx.Queue() for _ in range(self.cores)]
+        self.res = ctx.Queue()
+        parts = [list(range(k, frames, self.cores)) for k in range(self.cores)]
+        self.procs = [ctx.Process(target=_cpu_worker, args=(p, rank_seed, self.barrier, c, self.res))
+                      for p, c in zip(parts, self.cmd)]
+        for p in self.procs:
+            p.start()
+
+    def step(self) -> dict:
+        for c in self.cmd:
+            c.put(1)
+        res = [self.res.get() for _ in self.procs]
+        t = max(r[0] for r in res)
+        n = sum(r[1] for r in res)
+        return {"value": round(n / t / 1e9, 4), "unit": "GB/s", "cores": self.cores, "kind": "port",
+                "sample": f"{self.frames} x 1 MiB frames of the mixed workload, entropy-coded frame profile "
+                          f"(oracle/przm_oracle.c), one process per core", "seconds": round(t, 3)}
+
+    def close(self) -> None:
+        for c in self.cmd:
+            c.put(None)
+        for p in self.procs:
+            p.join()
 
 
 def cpu_throughput(frames: int, rank_seed: int, cores: int) -> dict:
-    """Input GB/s of the oracle's entropy-coded compress over `frames` frames
-    spread over `cores` processes (spawned: safe beside a CUDA context)."""
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    cores = max(1, min(cores, frames))
-    barrier = ctx.Barrier(cores)
-    q = ctx.Queue()
-    parts = [list(range(k, frames, cores)) for k in range(cores)]
-    procs = [ctx.Process(target=_cpu_worker, args=(p, rank_seed, barrier, q)) for p in parts]
-    for p in procs:
-        p.start()
-    res = [q.get() for _ in procs]
-    for p in procs:
-        p.join()
-    t = max(r[0] for r in res)
-    n = sum(r[1] for r in res)
-    return {"value": round(n / t / 1e9, 4), "unit": "GB/s", "cores": cores, "kind": "port",
-            "sample": f"{frames} x 1 MiB frames of the mixed workload, entropy-coded frame profile "
-                      f"(oracle/przm_oracle.c), one process per core", "seconds": round(t, 3)}
+    """Input GB/s of one timed pass of the oracle over `frames` frames."""
+    pool = CpuPool(frames, rank_seed, cores)
+    try:
+        return pool.step()
+    finally:
+        pool.close()
 
 
 # ---------------------------------------------------------------------------
@@ -331,14 +358,14 @@ def serve_measure(comp, count: int, fractions=(0.5,), seed: int = 0x50525A4D + 4
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=16)
     ap.add_argument("--plain-frames", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--frames", type=int, default=256, help="frames per GPU (smaller cases for profiling)")
-    ap.add_argument("--inflight", type=int, default=5, help="batches in flight on separate streams")
+    ap.add_argument("--inflight", type=int, default=10, help="batches in flight on separate streams")
     ap.add_argument("--serve-requests", type=int, default=2000, help="requests of the serving measurement (0: skip)")
     ap.add_argument("--uneven-inputs", type=int, default=4096, help="inputs of the uneven-batch measurement (0: skip)")
     ap.add_argument("--uneven-sample", type=int, default=256, help="inputs timed batched vs plain")
@@ -356,10 +383,12 @@ def main() -> None:
         if rank != 0:
             return
         steps = []
+        pool = CpuPool(args.frames, rank_seed, ncores)
         for s in range(args.warmup + args.steps):
-            r = cpu_throughput(args.frames, rank_seed, ncores)
+            r = pool.step()
             if s >= args.warmup:
                 steps.append(r)
+        pool.close()
         v = sorted(x["value"] for x in steps)[len(steps) // 2]
         base = dict(steps[0])
         base["value"] = v
