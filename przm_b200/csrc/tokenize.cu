@@ -78,7 +78,7 @@ __device__ uint32_t warp_match_end(const uint8_t* src, uint32_t a, uint32_t b, u
 // the non-empty bitmap words.  Finding the next descriptor is a warp-uniform
 // lookup in those; only run-length scans and the extension of 4095-byte
 // matches read global memory.  Every decision
-// becomes a 12-byte record in shared memory:
+// becomes a record in shared memory (16 bytes, the fourth word unused):
 //   r0 = q - tile start | literals before q << 16
 //   r1 = match or run length | kind << 16 | repeat slot << 18
 //   r2 = offset
