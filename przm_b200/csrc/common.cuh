@@ -174,4 +174,22 @@ __device__ __forceinline__ uint32_t spread8_4(uint32_t v) {
     return v;
 }
 
+// Lanes of the warp whose key equals this lane's, for keys below 2^kBits
+// (all 32 lanes take part): the AND over the key's bits of the ballot of that
+// bit, or of its complement where the bit is clear.  __match_any_sync gives
+// the same mask in one instruction, but on sm_100 that instruction costs
+// about 380 cycles of latency and one issue per ~63 SM cycles, while these
+// kBits ballots are independent and cheap.
+template <int kBits>
+__device__ __forceinline__ uint32_t warp_match(uint32_t key) {
+    uint32_t m = 0xFFFFFFFFu;
+#pragma unroll
+    for (int b = 0; b < kBits; b++) {
+        const bool x = ((key >> b) & 1u) != 0;
+        const uint32_t bb = __ballot_sync(0xFFFFFFFFu, x);
+        m &= x ? bb : ~bb;
+    }
+    return m;
+}
+
 }  // namespace pz

@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(256) k_tile_find(const uint8_t* __restrict__ i
 //   k_rx_resolve one warp per (frame, partition): walks the partition's
 //                candidates in position order 32 at a time with a 2048-entry
 //                shared table of the latest candidate per low-11-bit key
-//                (ties inside the 32 resolved with __match_any_sync) and
+//                (ties inside the 32 resolved with warp_match) and
 //                stores each candidate's predecessor next to it;
 //   k_rx_verify  one thread per candidate: verifies and extends the match
 //                against the predecessor and writes the descriptor.
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(256) k_rx_scatter(const uint8_t* __restrict__ 
         }
 #pragma unroll
         for (int r = 0; r < 16; r++) {
-            peers[r] = __match_any_sync(0xFFFFFFFFu, h[r] >> kRxKeyBits);
+            peers[r] = warp_match<9>(h[r] != 0xFFFFFFFFu ? h[r] >> kRxKeyBits : kRxParts);  // 256: no candidate
             if (h[r] != 0xFFFFFFFFu && (peers[r] & lt) == 0) s_w[warp][h[r] >> kRxKeyBits] += __popc(peers[r]);
             __syncwarp();
         }
@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(kRxResolveWarps * 32) k_rx_resolve(const Job* 
                 const uint32_t i = b0 + 32 * u + lane;
                 const bool v = i < pr.y;
                 const uint32_t c = cc[u], k = kk[u];
-                const uint32_t peers = __match_any_sync(0xFFFFFFFFu, k);
+                const uint32_t peers = warp_match<12>(v ? k : kRxKeys);  // 2048: no entry
                 const uint32_t lower = peers & lt;
                 const uint32_t from = lower ? 31u - __clz(lower) : lane;
                 const uint32_t cl = __shfl_sync(0xFFFFFFFFu, c, from);

@@ -576,7 +576,7 @@ __global__ void __launch_bounds__(1024) k_tile_order(const uint32_t* __restrict_
     for (uint32_t b0 = 0; b0 < ntiles; b0 += 1024) {  // uniform trip count: every lane takes part in the match
         const uint32_t T = b0 + tid;
         const uint32_t k = T < ntiles ? 32u - __clz(weight[T]) : 33u;
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, k);
+        const uint32_t peers = warp_match<6>(k);  // buckets 0..33
         if (k < 33 && (peers & lt) == 0) atomicAdd(&s_cnt[k], __popc(peers));
     }
     __syncthreads();
@@ -588,7 +588,7 @@ __global__ void __launch_bounds__(1024) k_tile_order(const uint32_t* __restrict_
     for (uint32_t b0 = 0; b0 < ntiles; b0 += 1024) {
         const uint32_t T = b0 + tid;
         const uint32_t k = T < ntiles ? 32u - __clz(weight[T]) : 33u;
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, k);
+        const uint32_t peers = warp_match<6>(k);  // buckets 0..33
         const uint32_t leader = __ffs(peers) - 1;
         uint32_t base = 0;
         if (k < 33 && lane == leader) base = atomicAdd(&s_pos[k], __popc(peers));
