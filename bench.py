@@ -361,7 +361,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--e2e-steps", type=int, default=16)
+    ap.add_argument("--e2e-steps", type=int, default=60)
     ap.add_argument("--plain-frames", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--frames", type=int, default=256, help="frames per GPU (smaller cases for profiling)")
