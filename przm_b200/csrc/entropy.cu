@@ -346,16 +346,15 @@ __device__ __forceinline__ LaneIO lane_io(uint8_t* task_base, uint32_t cap, uint
 // again when x >= 2^20 f), and advances x.  The caller keeps the low 16 bits
 // of x from before the step; its first k bytes (low byte first) are what the
 // reference writes.  x < 2^24 throughout, so x >= t2 can only hold for f < 16.
-// The three candidate states (0, 1 or 2 bytes shifted out) are computed side
-// by side and selected last, which keeps the compares off the multiply's
-// dependency chain.
+// The renormalised state is selected first and divided once: computing the
+// three candidates (0, 1 or 2 bytes shifted out) side by side and selecting
+// last keeps the compares off the multiply's chain, but its extra
+// instructions made the kernel slower (7.68 vs 7.45 ms on the 256 x 1 MiB
+// mixed batch).
 __device__ __forceinline__ uint32_t rans_next(uint32_t x, const EncSym& e) {
     const uint32_t s = e.w >> 25, cf = (e.w >> 13) & 0xFFFu, cb = e.w & 0x1FFFu;
-    const uint32_t x8 = x >> 8, x16 = x >> 16;
-    const uint32_t a0 = x + cb + (__umulhi(x, e.m) >> s) * cf;
-    const uint32_t a1 = x8 + cb + (__umulhi(x8, e.m) >> s) * cf;
-    const uint32_t a2 = x16 + cb + (__umulhi(x16, e.m) >> s) * cf;
-    return x >= e.t2 ? a2 : (x >= e.t1 ? a1 : a0);
+    const uint32_t xs = x >= e.t2 ? (x >> 16) : (x >= e.t1 ? (x >> 8) : x);
+    return xs + cb + (__umulhi(xs, e.m) >> s) * cf;
 }
 __device__ __forceinline__ uint32_t rans_step(uint32_t& x, const EncSym& e) {
     const uint32_t k = (uint32_t)(x >= e.t1) + (uint32_t)(x >= e.t2);
