@@ -77,6 +77,16 @@ def lib() -> C.CDLL:
         L.or_raw_literals_misparse.restype = C.c_int
         L.or_raw_literals_misparse.argtypes = [u8p, C.c_uint64]
         L.or_tokenize_input.argtypes = [u8p, C.c_uint64, u8p, u64p, u8p, u64p, u8p, u64p]
+        L.or_distance_to_code.restype = C.c_uint8
+        L.or_distance_to_code.argtypes = [C.c_uint32, u32p, u32p]
+        L.or_dist_mode12.restype = C.c_uint64
+        L.or_dist_mode12.argtypes = [u8p, C.c_uint64, u8p, C.c_uint64]
+        L.or_pack_distance_prefix.restype = C.c_uint64
+        L.or_pack_distance_prefix.argtypes = [u32p, C.c_uint64, u8p, C.c_uint64]
+        L.or_package_offsets.restype = C.c_uint64
+        L.or_package_offsets.argtypes = [u32p, C.c_uint64, u8p]
+        L.or_compress_p2.restype = C.c_uint64
+        L.or_compress_p2.argtypes = [u8p, C.c_uint64, u8p]
         _LIB = L
     return _LIB
 
@@ -264,6 +274,45 @@ def compress_p1(data) -> bytes:
     return bytes(out[:n])
 
 
+def compress_p2(data) -> bytes:
+    """P1 with Section 3 distance-coded (PackageOffsetsSection)."""
+    a = _u8(data)
+    out = np.zeros(frame_bound(len(a)), np.uint8)
+    n = lib().or_compress_p2(_p(a), len(a), _p(out))
+    return bytes(out[:n])
+
+
+def distance_to_code(d: int) -> tuple[int, int, int]:
+    """(code, extra, extra bit count) of distance d (DistanceToCode)."""
+    ex, nb = C.c_uint32(), C.c_uint32()
+    c = lib().or_distance_to_code(d, C.byref(ex), C.byref(nb))
+    return c, ex.value, nb.value
+
+
+def dist_mode12(codes) -> bytes | None:
+    """Mode 12 (0x0C) code stream of distance codes; None where the reference fails."""
+    a = _u8(codes)
+    out = np.zeros(4 << 20, np.uint8)
+    n = lib().or_dist_mode12(_p(a), len(a), _p(out), len(out))
+    return None if n == UINT64_MAX else bytes(out[:n])
+
+
+def pack_distance_prefix(dists, cap: int = 2 << 20) -> bytes | None:
+    """PackDistancePrefix (auto mode, V-ANS codes) into a cap-byte buffer; None on the reference's errors."""
+    d = np.ascontiguousarray(np.asarray(dists, dtype=np.uint32))
+    out = np.zeros(max(cap, 1), np.uint8)
+    n = lib().or_pack_distance_prefix(_p(d, u32p), len(d), _p(out), cap)
+    return None if n == UINT64_MAX else bytes(out[:n])
+
+
+def package_offsets(dists) -> bytes:
+    """PackageOffsetsSection: Section 3 bytes for these distances (b'' for none)."""
+    d = np.ascontiguousarray(np.asarray(dists, dtype=np.uint32))
+    out = np.zeros(5 * len(d) + 64, np.uint8)
+    n = lib().or_package_offsets(_p(d, u32p), len(d), _p(out))
+    return bytes(out[:n])
+
+
 def raw_literals_misparse(lits) -> bool:
     a = _u8(lits)
     return bool(lib().or_raw_literals_misparse(_p(a), len(a)))
@@ -292,6 +341,14 @@ def dec() -> C.CDLL:
         D.przm_split_commands.restype = C.c_int32
         D.przm_split_commands.argtypes = [u8p, C.c_size_t, u8p, C.c_size_t, C.POINTER(C.c_size_t), u8p, C.c_size_t,
                                           C.POINTER(C.c_size_t), u8p, C.c_size_t, C.POINTER(C.c_size_t)]
+        D.przm_distance_to_code.restype = C.c_int32
+        D.przm_distance_to_code.argtypes = [C.c_uint32, u8p, u32p, u8p]
+        D.przm_code_to_distance.restype = C.c_int32
+        D.przm_code_to_distance.argtypes = [C.c_uint8, C.c_uint32, u32p]
+        D.przm_vans_decode_dist4.restype = C.c_int32
+        D.przm_vans_decode_dist4.argtypes = [u8p, C.c_size_t, u8p, C.c_size_t, C.c_size_t]
+        D.przm_distance_prefix_decode.restype = C.c_int32
+        D.przm_distance_prefix_decode.argtypes = [u8p, C.c_size_t, u8p, C.c_size_t, C.POINTER(C.c_size_t)]
         _DEC = D
     return _DEC
 
@@ -361,3 +418,42 @@ def ref_cuda() -> C.CDLL:
         R.ref_tokenize.argtypes = [vp, u64, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32, vp]
         _REFCUDA = R
     return _REFCUDA
+
+
+def ref_distance_to_code(d: int) -> tuple[int, int, int]:
+    """The reference decoder's own distance coder (przm_distance_to_code)."""
+    code, nb = C.c_uint8(), C.c_uint8()
+    ex = C.c_uint32()
+    r = dec().przm_distance_to_code(d, C.byref(code), C.byref(ex), C.byref(nb))
+    if r != 0:
+        raise ValueError(f"reference distance coder error {r}")
+    return code.value, ex.value, nb.value
+
+
+def ref_code_to_distance(code: int, extra: int) -> int:
+    d = C.c_uint32()
+    r = dec().przm_code_to_distance(code, extra, C.byref(d))
+    if r != 0:
+        raise ValueError(f"reference distance decoder error {r}")
+    return d.value
+
+
+def ref_decode_dist4(stream: bytes, n: int) -> bytes:
+    """Decode a Mode 12 (0x0C) code stream of n codes with the reference decoder."""
+    s = _u8(stream)
+    out = np.zeros(n + 64, np.uint8)
+    r = dec().przm_vans_decode_dist4(_p(s), len(s), _p(out), len(out), n)
+    if r != 0:
+        raise ValueError(f"reference Mode 12 decode error {r}")
+    return bytes(out[:n])
+
+
+def ref_distance_prefix_decode(container: bytes, cap: int) -> bytes:
+    """Decode a distance-prefix container (0x06/0x0A/0x0B) into LEB128 varints."""
+    s = _u8(container)
+    out = np.zeros(cap + 64, np.uint8)
+    n = C.c_size_t()
+    r = dec().przm_distance_prefix_decode(_p(s), len(s), _p(out), cap, C.byref(n))
+    if r != 0:
+        raise ValueError(f"reference distance-prefix decode error {r}")
+    return bytes(out[:n.value])

@@ -31,6 +31,7 @@
 #include <string.h>
 
 #include "../przm_b200/csrc/meta8_tables.h"
+#include "../przm_b200/csrc/dist_tables.h"
 
 #define OR_TILE 32768u
 #define OR_BUCKETS 2048u
@@ -823,6 +824,184 @@ uint64_t or_package_commands(const uint8_t *cmds, uint64_t n, uint8_t *dst) {
 }
 
 /* ---------------------------------------------------------------------------
+ * Section 3 distance coding (core/distance/distance.go), the offsets of a
+ * frame as a distance-prefix container: a 49-bracket code per distance, its
+ * extra bits MSB-first, the codes entropy-coded (Mode 12 static contexts or
+ * adaptive V-ANS).  Buffer limits follow the reference's scratch sizes, since
+ * running out of them changes the output (the flat fallback).
+ * ------------------------------------------------------------------------- */
+#define OR_DIST_SCRATCH (2u * 1024 * 1024) /* meta, varBuf, altBuf, s3Buf: distance.go:124-129, compress.go:76 */
+#define OR_DIST_CODEBUF (4u * 1024 * 1024) /* cmds: distance.go:127 */
+
+/* DistanceToCode, distance.go:165-180: code, extra bits and their count. */
+uint8_t or_distance_to_code(uint32_t d, uint32_t *extra, uint32_t *nb) {
+    if (d <= 4) { *extra = 0; *nb = 0; return (uint8_t)(d - 1); }
+    if (d <= 16777216u) {
+        const uint32_t u = d - 1;
+        const uint32_t b = (uint32_t)(32 - __builtin_clz(u)) - 2;  /* bits.Len32(u) - 2, u >= 4 */
+        const uint32_t half = (u >> b) & 1u;
+        *nb = b;
+        *extra = d - (((2u + half) << b) + 1u);
+        return (uint8_t)(2 * b + 2 + half);
+    }
+    *nb = 24;
+    *extra = d - 16777217u;
+    return 48;
+}
+
+/* ContextDist, distance.go:190-202 */
+static int ctx_dist(uint8_t prev) { return prev < 6 ? 0 : prev < 14 ? 1 : prev < 26 ? 2 : 3; }
+
+/* BitWriter, distance.go:204-247: MSB-first into buf of cap bytes; a
+ * write that needs a byte past cap fails (the reference's ErrBufferTooSmall). */
+typedef struct { uint8_t *buf; uint64_t cap, pos; uint64_t acc; uint32_t cnt; int err; } or_bits;
+static void bits_put(or_bits *w, uint32_t val, uint32_t nb) {
+    if (nb == 0 || w->err) return;
+    w->acc = (w->acc << nb) | ((uint64_t)val & ((1ull << nb) - 1));
+    w->cnt += nb;
+    while (w->cnt >= 8) {
+        if (w->pos >= w->cap) { w->err = 1; return; }
+        w->cnt -= 8;
+        w->buf[w->pos++] = (uint8_t)(w->acc >> w->cnt);
+    }
+}
+static void bits_flush(or_bits *w) {
+    if (w->cnt > 0 && !w->err) {
+        if (w->pos >= w->cap) { w->err = 1; return; }
+        w->buf[w->pos++] = (uint8_t)(w->acc << (8 - w->cnt));
+        w->cnt = 0;
+        w->acc = 0;
+    }
+}
+
+/* EncodeDistClusteredVans, distance.go:323-377: one rANS state (M = 4096,
+ * L = 65536, byte renormalisation) over the codes from the last to the
+ * first, each coded with the static weights of its predecessor's class;
+ * 0x0C | LE32 state | reversed stream.  UINT64_MAX where the reference runs
+ * out of its 2 MiB stream scratch or of dcap. */
+uint64_t or_dist_mode12(const uint8_t *codes, uint64_t n, uint8_t *dst, uint64_t dcap) {
+    if (n == 0) {
+        if (dcap < 5) return UINT64_MAX;
+        dst[0] = 0x0C;
+        wr32(dst + 1, 65536);
+        return 5;
+    }
+    uint16_t cdf[4][64];
+    for (int k = 0; k < 4; k++) {
+        uint16_t cum = 0;
+        for (int s = 0; s < 64; s++) { cdf[k][s] = cum; cum += przm_dist_freq4[k][s]; }
+    }
+    uint8_t *tmp = (uint8_t *)malloc(OR_DIST_SCRATCH);
+    uint64_t e = 0;
+    uint32_t x = 65536;
+    for (uint64_t i = n; i-- > 0;) {
+        const uint8_t sym = codes[i];
+        if (sym >= 64) { free(tmp); return UINT64_MAX; }
+        const int k = ctx_dist(i ? codes[i - 1] : 0);
+        const uint32_t f = przm_dist_freq4[k][sym], cf = cdf[k][sym];
+        while (x > 4096u * f - 1) {
+            if (e >= OR_DIST_SCRATCH) { free(tmp); return UINT64_MAX; }
+            tmp[e++] = (uint8_t)x;
+            x >>= 8;
+        }
+        x = (x / f) * 4096 + cf + (x % f);
+    }
+    if (5 + e > dcap) { free(tmp); return UINT64_MAX; }
+    dst[0] = 0x0C;
+    wr32(dst + 1, x);
+    for (uint64_t k = 0; k < e; k++) dst[5 + k] = tmp[e - 1 - k];
+    free(tmp);
+    return 5 + e;
+}
+
+static uint64_t leb_len(uint32_t d) { return d <= 0x7F ? 1 : d <= 0x3FFF ? 2 : d <= 0x1FFFFF ? 3 : d <= 0x0FFFFFFF ? 4 : 5; }
+
+/* PackDistancePrefix(mode auto, useVANS), distance.go:692-748, with
+ * SelectPrefixMode :750-758 and assemblePrefixContainer :777-822:
+ *   0x0B | u8 origLen | u8 count | u8 codeLen, or
+ *   0x0A | LE16 x 3, or 0x06 | LE32 x 3; then the code stream, then the extra
+ *   bits.  The code stream is Mode 12, or for 64 codes or more the adaptive
+ *   V-ANS container of the codes when that fits 2 MiB and is smaller.
+ * Returns the size, or UINT64_MAX on the reference's errors (a distance of 0
+ * or above 2^24, a scratch or dst overflow). */
+uint64_t or_pack_distance_prefix(const uint32_t *dist, uint64_t n, uint8_t *dst, uint64_t dcap) {
+    if (n == 0) return 0;
+    if (n > OR_DIST_SCRATCH) return UINT64_MAX; /* the codes' scratch (meta) */
+    uint8_t *codes = (uint8_t *)malloc(n);
+    uint8_t *extra = (uint8_t *)malloc(OR_DIST_SCRATCH);
+    or_bits w = {extra, OR_DIST_SCRATCH, 0, 0, 0, 0};
+    uint64_t orig = 0, ret = UINT64_MAX;
+    uint8_t *cs = NULL, *alt = NULL;
+    for (uint64_t i = 0; i < n; i++) {
+        const uint32_t d = dist[i];
+        if (d == 0 || d > 16777216u) goto out;
+        uint32_t ex, nb;
+        codes[i] = or_distance_to_code(d, &ex, &nb);
+        bits_put(&w, ex, nb);
+        if (w.err) goto out;
+        orig += leb_len(d);
+    }
+    bits_flush(&w);
+    if (w.err) goto out;
+    cs = (uint8_t *)malloc(OR_DIST_CODEBUF);
+    uint64_t cl = or_dist_mode12(codes, n, cs, OR_DIST_CODEBUF);
+    if (cl == UINT64_MAX) goto out;
+    if (n >= 64) {
+        alt = (uint8_t *)malloc(2 * n + 1024);
+        const uint64_t al = or_adaptive_vans(codes, n, alt);
+        if (al != UINT64_MAX && al <= OR_DIST_SCRATCH && al < cl) { memcpy(cs, alt, al); cl = al; }
+    }
+    uint64_t h;
+    if (orig <= 255 && n <= 255 && cl <= 255) h = 4;
+    else if (orig <= 65535 && n <= 65535 && cl <= 65535) h = 7;
+    else h = 13;
+    if (h + cl + w.pos > dcap) goto out;
+    if (h == 4) {
+        dst[0] = 0x0B; dst[1] = (uint8_t)orig; dst[2] = (uint8_t)n; dst[3] = (uint8_t)cl;
+    } else if (h == 7) {
+        dst[0] = 0x0A;
+        dst[1] = (uint8_t)orig; dst[2] = (uint8_t)(orig >> 8);
+        dst[3] = (uint8_t)n; dst[4] = (uint8_t)(n >> 8);
+        dst[5] = (uint8_t)cl; dst[6] = (uint8_t)(cl >> 8);
+    } else {
+        dst[0] = 0x06; wr32(dst + 1, (uint32_t)orig); wr32(dst + 5, (uint32_t)n); wr32(dst + 9, (uint32_t)cl);
+    }
+    memcpy(dst + h, cs, cl);
+    memcpy(dst + h + cl, extra, w.pos);
+    ret = h + cl + w.pos;
+out:
+    free(codes); free(extra); free(cs); free(alt);
+    return ret;
+}
+
+/* PackageOffsetsSection, distance.go:825-849 (into the compressor's 2 MiB
+ * s3Buf, compress.go:76,956): the distance-prefix container when it is
+ * smaller than the distances as LEB128 varints, else 0x09 + those varints.
+ * Returns 0 (an empty section) for no distances. dst holds 1 + 5 n bytes. */
+uint64_t or_package_offsets(const uint32_t *dist, uint64_t n, uint8_t *dst) {
+    if (n == 0) return 0;
+    uint8_t *buf = (uint8_t *)malloc(OR_DIST_SCRATCH);
+    const uint64_t pl = or_pack_distance_prefix(dist, n, buf, OR_DIST_SCRATCH);
+    uint64_t raw = 0;
+    for (uint64_t i = 0; i < n; i++) raw += leb_len(dist[i]);
+    uint64_t w;
+    if (pl != UINT64_MAX && pl < raw) {
+        memcpy(dst, buf, pl);
+        w = pl;
+    } else {
+        dst[0] = 0x09;
+        w = 1;
+        for (uint64_t i = 0; i < n; i++) {
+            uint32_t v = dist[i];
+            while (v >= 0x80) { dst[w++] = (uint8_t)(v | 0x80); v >>= 7; }
+            dst[w++] = (uint8_t)v;
+        }
+    }
+    free(buf);
+    return w;
+}
+
+/* ---------------------------------------------------------------------------
  * Frames.
  * ------------------------------------------------------------------------- */
 
@@ -888,7 +1067,8 @@ int or_raw_literals_misparse(const uint8_t *lit, uint64_t n) {
     return rd32(lit + 4) == (uint32_t)(((uint64_t)rd32(lit) + 1) / 2);
 }
 
-/* Profile P1 == match + tokenize + ANS frame (this build's compress format):
+/* Profiles P1 and P2.  P1 == match + tokenize + ANS frame (this build's
+ * compress format):
  *   header and Section 1 as P0;
  *   Section 2 = PackageCommandsSection(cmds) when cmds <= 2 MiB (every
  *     substream then fits the decoders' 2 MiB substream buffers), else
@@ -902,7 +1082,7 @@ int or_raw_literals_misparse(const uint8_t *lit, uint64_t n) {
  *     (assembleContainer, compress.go:962-985) or when neither Section 4 form
  *     is decodable.
  * n must be < 16 MiB (24-bit uSize). */
-uint64_t or_compress_p1(const uint8_t *in, uint64_t n, uint8_t *dst) {
+static uint64_t compress_p(const uint8_t *in, uint64_t n, uint8_t *dst, int s3_coded) {
     if (n == 0) return 0;
     or_tokens t;
     tokens_of(in, n, &t);
@@ -911,6 +1091,20 @@ uint64_t or_compress_p1(const uint8_t *in, uint64_t n, uint8_t *dst) {
     if (t.nc <= 2u * 1024 * 1024) l2 = or_package_commands(t.cmd, t.nc, s2);
     else { s2[0] = 0x09; memcpy(s2 + 1, t.cmd, t.nc); l2 = 1 + t.nc; }
     uint64_t l3 = t.no + 5;
+    uint8_t *s3 = NULL;
+    if (s3_coded) {  /* the offset stream holds one LEB128 varint per distance */
+        uint32_t *dist = (uint32_t *)malloc((t.no + 1) * sizeof(uint32_t));
+        uint64_t nd = 0;
+        for (uint64_t i = 0; i < t.no;) {
+            uint32_t v = 0, sh = 0;
+            while (t.off[i] & 0x80) { v |= (uint32_t)(t.off[i++] & 0x7F) << sh; sh += 7; }
+            v |= (uint32_t)t.off[i++] << sh;
+            dist[nd++] = v;
+        }
+        s3 = (uint8_t *)malloc(5 * nd + 64);
+        l3 = or_package_offsets(dist, nd, s3);
+        free(dist);
+    }
     uint8_t *s4 = NULL;
     uint64_t l4 = t.nl;
     uint8_t nib = 0;
@@ -941,12 +1135,22 @@ uint64_t or_compress_p1(const uint8_t *in, uint64_t n, uint8_t *dst) {
     } else {
         w = put_header(dst, flags, n, l2, l3, wlog);
         memcpy(dst + w, s2, l2); w += l2;
-        dst[w] = 0; wr32(dst + w + 1, (uint32_t)t.no); memcpy(dst + w + 5, t.off, t.no); w += l3;
+        if (s3) memcpy(dst + w, s3, l3);
+        else { dst[w] = 0; wr32(dst + w + 1, (uint32_t)t.no); memcpy(dst + w + 5, t.off, t.no); }
+        w += l3;
         memcpy(dst + w, s4 ? s4 : t.lit, l4); w += l4;
     }
-    free(s2); free(s4); free(t.cmd); free(t.off); free(t.lit);
+    free(s2); free(s3); free(s4); free(t.cmd); free(t.off); free(t.lit);
     return w;
 }
+
+uint64_t or_compress_p1(const uint8_t *in, uint64_t n, uint8_t *dst) { return compress_p(in, n, dst, 0); }
+
+/* Profile P2 == P1 with Section 3 as PackageOffsetsSection of the frame's
+ * distances (core/distance/distance.go:825-849, as the reference's CPU
+ * compressor writes it, compress.go:956): a distance-prefix container or
+ * 0x09 varints, and an empty Section 3 when the frame has no match. */
+uint64_t or_compress_p2(const uint8_t *in, uint64_t n, uint8_t *dst) { return compress_p(in, n, dst, 1); }
 
 /* Tokens only (Tokenize, gpu/bridge.go:1895), for tests. */
 void or_tokenize_input(const uint8_t *in, uint64_t n, uint8_t *cmd, uint64_t *nc, uint8_t *off, uint64_t *no,
