@@ -274,6 +274,19 @@ int32_t przmg_vans_encode4x_host(przmg_ctx* ctx, const uint8_t* src, uint64_t n,
 int32_t przmg_vans_encode_batch(przmg_ctx* ctx, uint64_t d_in, const uint64_t* in_offs, const uint32_t* lens,
                                 uint64_t count, int32_t norm, uint64_t d_out, const uint64_t* out_offs,
                                 uint32_t* out_lens, uint64_t stream);
+/* PackageOffsetsSection, core/distance/distance.go:825-849, for many
+ * distance arrays in one call: the Section 3 bytes the reference's CPU
+ * compressor writes for each (a distance-prefix container 0x0B/0x0A/0x06 whose
+ * code stream is Mode 12 or the codes' adaptive V-ANS container, or 0x09 +
+ * LEB128 varints; nothing for an empty array).  d_dist + 4 * dist_offs[i]
+ * holds counts[i] <= 2^21 uint32 distances; section i goes to
+ * d_out + out_offs[i], whose out_caps[i] bytes must hold 1 + 5 * counts[i]
+ * in the worst case; out_lens[i] receives its size.  Synchronises the stream.
+ * PRZMG_ERR_EXCEEDS_MAX_BLOCK for an array above 2^21 distances,
+ * PRZMG_ERR_BUFFER_TOO_SMALL when a section does not fit its capacity. */
+int32_t przmg_package_offsets_batch(przmg_ctx* ctx, uint64_t d_dist, const uint64_t* dist_offs, const uint32_t* counts,
+                                    uint64_t count, uint64_t d_out, const uint64_t* out_offs, const uint64_t* out_caps,
+                                    uint64_t* out_lens, uint64_t stream);
 
 /* ---- allocation-free V-ANS encode: no counterpart in the reference -------
  * Histogram + normalise + V-ANS of ONE device stream: the same launch

@@ -161,6 +161,7 @@ struct Ctx {
     przmg_batch single;  // reused by the one-input calls
     HostBuf h_in, h_out, h_aux;
     DevBuf d_scr_in, d_scr_out, d_scr_aux, d_scr_tab;
+    DevBuf d_s3;  // scratch of przmg_package_offsets_batch
     cudaEvent_t ev[8] = {};
 };
 
@@ -479,7 +480,7 @@ extern "C" int32_t przmg_close(przmg_ctx* h) {
         c->single.drop_graph();
         c->single.release();
         DevBuf* bufs[] = {&c->d_meta8, &c->d_ctxlut, &c->d_scr_in, &c->d_scr_out, &c->d_scr_aux,
-                          &c->d_scr_tab};
+                          &c->d_scr_tab, &c->d_s3};
         for (DevBuf* b : bufs) b->release();
         c->h_in.release();
         c->h_out.release();
@@ -1283,6 +1284,11 @@ extern "C" int32_t przmg_match_lz77_streaming(przmg_ctx* h, const uint8_t* src, 
 // histogram / flat pack / V-ANS single-stream APIs and the stream batch
 // ---------------------------------------------------------------------------
 #include "api_streams.inc"
+
+// ---------------------------------------------------------------------------
+// Section 3 distance coding of many distance arrays
+// ---------------------------------------------------------------------------
+#include "offsets.inc"
 
 // ---------------------------------------------------------------------------
 // serving: continuous batching of submitted requests

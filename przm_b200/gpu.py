@@ -454,6 +454,19 @@ class GPUCompressor:
                                            stream))
         return ol[: len(ln)]
 
+    def PackageOffsetsBatch(self, dDist: int, distOffs, counts, dOut: int, outOffs, outCaps,
+                            stream: int = 0) -> np.ndarray:
+        """PackageOffsetsSection (core/distance/distance.go:825) of many device
+        uint32 distance arrays: Section 3 sizes (bytes written at dOut + outOffs)."""
+        do = np.ascontiguousarray(distOffs, np.uint64)
+        ct = np.ascontiguousarray(counts, np.uint32)
+        oo = np.ascontiguousarray(outOffs, np.uint64)
+        oc = np.ascontiguousarray(outCaps, np.uint64)
+        ol = np.zeros(max(len(ct), 1), np.uint64)
+        _check(L().przmg_package_offsets_batch(self._h, dDist, _ptr(do), _ptr(ct), len(ct), dOut, _ptr(oo), _ptr(oc),
+                                               _ptr(ol), stream))
+        return ol[: len(ct)]
+
     # -- benchmarks --
     def BenchmarkVRAMBandwidth(self, sizeMB: int = 256, iterations: int = 10) -> float:
         g = C.c_double()
