@@ -259,6 +259,42 @@ def link_gbs(hin, nbytes: int, dev_buf: int, stream) -> dict:
     return out
 
 
+def section3_measure(comp, sections: int, per: int = 20_000, calls: int = 5) -> dict:
+    """Section 3 distance coding on the device (przmg_package_offsets_batch,
+    PackageOffsetsSection) of `sections` arrays of `per` distances each,
+    log-uniform in [2, 2^20 + 1] (the match window), seeded.  A call
+    synchronises (the host picks each section's form from the sizes), so the
+    figure is wall time per call, best of `calls` after one warm-up."""
+    import numpy as np
+    from przm_b200 import devmem
+    rng = np.random.default_rng(0x50525A4D + 5)
+    d = (np.exp(rng.uniform(0, np.log(1 << 20), sections * per)).astype(np.uint32) + 1).astype(np.uint32)
+    vb = int(np.where(d < 0x80, 1, np.where(d < 0x4000, 2, np.where(d < 0x200000, 3, 4))).sum())
+    counts = np.full(sections, per, np.uint32)
+    offs = np.arange(sections, dtype=np.uint64) * per
+    cap = 1 + 5 * per
+    caps = np.full(sections, cap, np.uint64)
+    out_offs = np.arange(sections, dtype=np.uint64) * (cap + 16)
+    d_dist = devmem.upload(d.view(np.uint8))
+    d_out = devmem.alloc(int(out_offs[-1]) + cap + 64)
+    lens = comp.PackageOffsetsBatch(d_dist.ptr, offs, counts, d_out.ptr, out_offs, caps)
+    best = float("inf")
+    for _ in range(calls):
+        t0 = time.perf_counter()
+        lens = comp.PackageOffsetsBatch(d_dist.ptr, offs, counts, d_out.ptr, out_offs, caps)
+        best = min(best, time.perf_counter() - t0)
+    modes: dict[str, int] = {}
+    for o, n in zip(out_offs, lens):
+        if n:
+            m = f"0x{devmem.download(d_out.ptr + int(o), 1)[0]:02X}"
+            modes[m] = modes.get(m, 0) + 1
+    return {"sections": sections, "distances": int(sections * per), "ms_per_call": round(best * 1e3, 3),
+            "mdistances_per_s": round(sections * per / best / 1e6, 2), "varint_bytes": vb,
+            "varint_gbps": round(vb / best / 1e9, 3), "section_bytes": int(np.sum(lens)),
+            "ratio_vs_varints": round(float(np.sum(lens)) / vb, 4), "modes": modes,
+            "timing": f"wall clock per synchronising call, best of {calls}"}
+
+
 def uneven_measure(comp, count: int, sample: int) -> dict:
     """The uneven-batch workload: `count` inputs with sizes log-uniform in
     [1 KiB, 4 MiB] and mixed contents.  All of them as one device-resident
@@ -372,6 +408,8 @@ def main() -> None:
     ap.add_argument("--serve-requests", type=int, default=2000, help="requests of the serving measurement (0: skip)")
     ap.add_argument("--uneven-inputs", type=int, default=4096, help="inputs of the uneven-batch measurement (0: skip)")
     ap.add_argument("--uneven-sample", type=int, default=256, help="inputs timed batched vs plain")
+    ap.add_argument("--section3-sections", type=int, default=256,
+                    help="sections of the Section 3 distance-coding measurement (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -555,6 +593,12 @@ def main() -> None:
     serve = serve_measure(comp, args.serve_requests) if args.serve_requests > 0 and world == 1 else None
     uneven = (uneven_measure(comp, args.uneven_inputs, args.uneven_sample)
               if args.uneven_inputs > 0 and world == 1 else None)
+    section3 = None
+    if args.section3_sections > 0 and world == 1:
+        try:
+            section3 = section3_measure(comp, args.section3_sections)
+        except Exception as e:  # an extra leg never costs the bench line
+            section3 = {"error": f"{type(e).__name__}: {e}"[:300]}
 
     # roofline of the dominant kernel
     peak, peak_kind = measured_peaks()
@@ -618,7 +662,7 @@ def main() -> None:
                     "link_gbs": link, "host": numa},
             "roofline": roofline, "pipeline_roofline": pipeline, "stage_ms": {k: round(v, 3) for k, v in stages.items()},
             "cpu_baseline": cpu_base, "plain_per_frame": plain, "clocks": clk, "gpu_launches": gl,
-            "serving": serve, "uneven_batch": uneven,
+            "serving": serve, "uneven_batch": uneven, "section3": section3,
         }
         print(json.dumps(line), flush=True)
     for bt in batches:
