@@ -87,6 +87,15 @@ def lib() -> C.CDLL:
         L.or_package_offsets.argtypes = [u32p, C.c_uint64, u8p]
         L.or_compress_p2.restype = C.c_uint64
         L.or_compress_p2.argtypes = [u8p, C.c_uint64, u8p]
+        L.or_compress_p3.restype = C.c_uint64
+        L.or_compress_p3.argtypes = [u8p, C.c_uint64, u8p]
+        L.or_sheaf_class.restype = C.c_uint8
+        L.or_sheaf_class.argtypes = [C.c_uint8, C.c_uint8, C.c_int]
+        L.or_decompose_fibers.argtypes = [u8p, C.c_uint64, C.c_int, C.POINTER(u8p), u64p]
+        L.or_pack_sheaf.restype = C.c_uint64
+        L.or_pack_sheaf.argtypes = [u8p, C.c_uint64, C.c_int, u8p]
+        L.or_package_literals.restype = C.c_uint64
+        L.or_package_literals.argtypes = [u8p, C.c_uint64, u8p, u8p]
         _LIB = L
     return _LIB
 
@@ -282,6 +291,45 @@ def compress_p2(data) -> bytes:
     return bytes(out[:n])
 
 
+def compress_p3(data) -> bytes:
+    """P2 with Section 4 as PackageLiteralsSection (V-ANS or a sheaf foliation)."""
+    a = _u8(data)
+    out = np.zeros(frame_bound(len(a)) + 4096, np.uint8)
+    n = lib().or_compress_p3(_p(a), len(a), _p(out))
+    return bytes(out[:n])
+
+
+def sheaf_class(p2: int, p1: int, mode: int) -> int:
+    return lib().or_sheaf_class(p2, p1, mode)
+
+
+def decompose_fibers(lits, mode: int) -> list[bytes]:
+    """The four fibers of a sheaf foliation (DecomposeFibers)."""
+    a = _u8(lits)
+    bufs = [np.zeros(max(len(a), 1), np.uint8) for _ in range(4)]
+    ptrs = (u8p * 4)(*[_p(b) for b in bufs])
+    l = np.zeros(4, np.uint64)
+    lib().or_decompose_fibers(_p(a), len(a), mode, ptrs, _p(l, u64p))
+    return [bytes(b[:int(k)]) for b, k in zip(bufs, l)]
+
+
+def pack_sheaf(lits, mode: int) -> bytes:
+    """PackEtaleSheaf container of the literals in one foliation mode."""
+    a = _u8(lits)
+    out = np.zeros(40 + 2 * len(a) + 4096, np.uint8)
+    n = lib().or_pack_sheaf(_p(a), len(a), mode, _p(out))
+    return bytes(out[:n])
+
+
+def package_literals(lits) -> tuple[bytes, int]:
+    """PackageLiteralsSection: (Section 4 bytes, flag nibble 0x80 or 0)."""
+    a = _u8(lits)
+    out = np.zeros(40 + 2 * len(a) + 4096, np.uint8)
+    nib = C.c_uint8()
+    n = lib().or_package_literals(_p(a), len(a), _p(out), C.byref(nib))
+    return bytes(out[:n]), nib.value
+
+
 def distance_to_code(d: int) -> tuple[int, int, int]:
     """(code, extra, extra bit count) of distance d (DistanceToCode)."""
     ex, nb = C.c_uint32(), C.c_uint32()
@@ -349,6 +397,13 @@ def dec() -> C.CDLL:
         D.przm_vans_decode_dist4.argtypes = [u8p, C.c_size_t, u8p, C.c_size_t, C.c_size_t]
         D.przm_distance_prefix_decode.restype = C.c_int32
         D.przm_distance_prefix_decode.argtypes = [u8p, C.c_size_t, u8p, C.c_size_t, C.POINTER(C.c_size_t)]
+        D.przm_context_classify.restype = C.c_uint8
+        D.przm_context_classify.argtypes = [C.c_uint8, C.c_uint8]
+        D.przm_context_classify_order2.restype = C.c_uint8
+        D.przm_context_classify_order2.argtypes = [C.c_uint8, C.c_uint8]
+        D.przm_reconstitute_fibers.restype = C.c_int32
+        D.przm_reconstitute_fibers.argtypes = [u8p, C.c_size_t, u8p, u8p, u8p, u8p, C.c_size_t, C.c_size_t,
+                                               C.c_size_t, C.c_size_t, C.c_uint8]
         _DEC = D
     return _DEC
 
@@ -457,3 +512,21 @@ def ref_distance_prefix_decode(container: bytes, cap: int) -> bytes:
     if r != 0:
         raise ValueError(f"reference distance-prefix decode error {r}")
     return bytes(out[:n.value])
+
+
+def ref_context_classify(p2: int, p1: int, mode: int) -> int:
+    """The reference decoder's fiber class of a literal after p2, p1."""
+    if mode < 3:
+        return dec().przm_context_classify(p1, mode)
+    return dec().przm_context_classify_order2(p2, p1)
+
+
+def ref_reconstitute_fibers(fibers: list[bytes], mode: int) -> bytes:
+    """Interleave four fibers back into the literals with the reference decoder."""
+    n = sum(len(f) for f in fibers)
+    out = np.zeros(n + 64, np.uint8)
+    fs = [_u8(f if f else b"\0") for f in fibers]
+    r = dec().przm_reconstitute_fibers(_p(out), n, *[_p(f) for f in fs], *[len(f) for f in fibers], mode)
+    if r != 0:
+        raise ValueError(f"reference reconstitution error {r}")
+    return bytes(out[:n])

@@ -1002,6 +1002,119 @@ uint64_t or_package_offsets(const uint32_t *dist, uint64_t n, uint8_t *dst) {
 }
 
 /* ---------------------------------------------------------------------------
+ * Section 4 selection (core/literals/literals.go:600-693, sheaf.go): the
+ * literals as the smallest of their adaptive V-ANS container and the four
+ * étale-sheaf foliations, else raw.  A foliation sends every literal to one of
+ * four fibers by the class of the literal before it (modes 0-2) or of the two
+ * before it (mode 3); each fiber is V-ANS coded when that is smaller.
+ * ------------------------------------------------------------------------- */
+static int sheaf_ws(uint8_t b) { return b == ' ' || b == '\t' || b == '\r' || b == '\n'; }
+static int sheaf_syntax(uint8_t b) {
+    static const char set[] = "{}[]()<>:;,.\"'`=+-*/%&|^!~?\\#";
+    return b != 0 && strchr(set, b) != NULL;
+}
+static int sheaf_ident(uint8_t b) { return (b >= 'a' && b <= 'z') || b == '_'; }
+static int sheaf_digit(uint8_t b) { return b >= '0' && b <= '9'; }
+
+/* ContextClassify (sheaf.go:39-88) for modes 0-2, ContextClassifyOrder2
+ * (:91-107) for mode 3. */
+uint8_t or_sheaf_class(uint8_t p2, uint8_t p1, int mode) {
+    switch (mode) {
+        case 0: return sheaf_ws(p1) ? 0 : sheaf_syntax(p1) ? 1 : sheaf_ident(p1) ? 2 : 3;
+        case 1: return (p1 == '"' || p1 == ':') ? 0 : sheaf_ident(p1) ? 1 : sheaf_digit(p1) ? 2 : 3;
+        case 2: return (sheaf_ws(p1) || sheaf_syntax(p1)) ? 0 : 1;
+        default:
+            if (sheaf_digit(p1)) return (sheaf_digit(p2) || p2 == '.' || p2 == '-') ? 0 : 1;
+            if (sheaf_ident(p1)) return sheaf_ident(p2) ? 2 : 3;
+            return sheaf_ws(p1) ? 0 : 1;
+    }
+}
+
+/* DecomposeFibers (sheaf.go:110-137): fiber k of the literals gets the
+ * literals of class k, in order; fibers[k] holds n bytes each, l[k] their
+ * counts. */
+void or_decompose_fibers(const uint8_t *src, uint64_t n, int mode, uint8_t *fibers[4], uint64_t l[4]) {
+    uint8_t p1 = 0, p2 = 0;
+    l[0] = l[1] = l[2] = l[3] = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        const uint8_t k = or_sheaf_class(p2, p1, mode);
+        fibers[k][l[k]++] = src[i];
+        p2 = p1;
+        p1 = src[i];
+    }
+}
+
+/* EncodeVANS4x body (literals.go:344-355: the container without its 8-byte
+ * header) with NormalizeFrequencies, as tryEncodeFiber (:633-643) makes it;
+ * UINT64_MAX where the reference's 8 MiB emission scratch overflows. */
+static uint64_t fiber_vans(const uint8_t *src, uint64_t n, uint8_t *dst) {
+    uint32_t counts[256];
+    uint16_t freq[256];
+    or_histogram(src, n, counts);
+    or_normalize_frequencies(counts, freq);
+    uint8_t *tmp = (uint8_t *)malloc(2 * n + 1024);
+    const uint64_t sz = or_vans_encode(src, n, freq, 0x00, tmp);
+    uint8_t mat[600];
+    const uint64_t hdr = 8 + 16 + or_serialize_matrix(freq, mat);
+    uint64_t r = UINT64_MAX;
+    if (sz - hdr <= 8u * 1024 * 1024) {
+        memcpy(dst, tmp + 8, sz - 8);
+        r = sz - 8;
+    }
+    free(tmp);
+    return r;
+}
+
+/* PackEtaleSheaf (literals.go:600-631) with assembleSheafContainer (:645-662):
+ * 'V','A',01, 0x01 | 0x04 | mode << 4, LE32 n, LE32 l[4], LE32 e[4], then the
+ * fibers, each V-ANS coded when that is smaller (e < l), else raw (e == l).
+ * dst holds 40 + 2 n + 4 x 1024 bytes. */
+uint64_t or_pack_sheaf(const uint8_t *src, uint64_t n, int mode, uint8_t *dst) {
+    uint8_t *fb[4];
+    uint64_t l[4], e[4];
+    for (int k = 0; k < 4; k++) fb[k] = (uint8_t *)malloc(n ? n : 1);
+    or_decompose_fibers(src, n, mode, fb, l);
+    dst[0] = 'V'; dst[1] = 'A'; dst[2] = 0x01; dst[3] = (uint8_t)(0x01 | 0x04 | ((mode & 0x0F) << 4));
+    wr32(dst + 4, (uint32_t)n);
+    uint64_t w = 40;
+    uint8_t *enc = (uint8_t *)malloc(2 * n + 1024);
+    for (int k = 0; k < 4; k++) {
+        e[k] = 0;
+        if (l[k] == 0) continue;
+        const uint64_t el = fiber_vans(fb[k], l[k], enc);
+        if (el != UINT64_MAX && el < l[k]) { memcpy(dst + w, enc, el); e[k] = el; }
+        else { memcpy(dst + w, fb[k], l[k]); e[k] = l[k]; }
+        w += e[k];
+    }
+    for (int k = 0; k < 4; k++) { wr32(dst + 8 + 4 * k, (uint32_t)l[k]); wr32(dst + 24 + 4 * k, (uint32_t)e[k]); }
+    free(enc);
+    for (int k = 0; k < 4; k++) free(fb[k]);
+    return w;
+}
+
+/* PackageLiteralsSection (literals.go:664-693): the smallest of the adaptive
+ * V-ANS container and the four foliations when one is smaller than the raw
+ * literals (*nibble = FlagNibble 0x80), else the raw literals (*nibble = 0).
+ * dst holds 40 + 2 n + 4 x 1024 bytes. */
+uint64_t or_package_literals(const uint8_t *lits, uint64_t n, uint8_t *dst, uint8_t *nibble) {
+    *nibble = 0;
+    if (n == 0) return 0;
+    uint8_t *cand = (uint8_t *)malloc(40 + 2 * n + 4 * 1024);
+    uint64_t best = n;
+    int have = 0;
+    const uint64_t vl = or_adaptive_vans(lits, n, cand);
+    if (vl != UINT64_MAX && vl < best) { memcpy(dst, cand, vl); best = vl; have = 1; }
+    for (int mode = 0; mode <= 3; mode++) {
+        const uint64_t sl = or_pack_sheaf(lits, n, mode, cand);
+        if (sl < best) { memcpy(dst, cand, sl); best = sl; have = 1; }
+    }
+    free(cand);
+    if (have) { *nibble = 0x80; return best; }
+    memcpy(dst, lits, n);
+    return n;
+}
+
+/* ---------------------------------------------------------------------------
  * Frames.
  * ------------------------------------------------------------------------- */
 
@@ -1082,7 +1195,7 @@ int or_raw_literals_misparse(const uint8_t *lit, uint64_t n) {
  *     (assembleContainer, compress.go:962-985) or when neither Section 4 form
  *     is decodable.
  * n must be < 16 MiB (24-bit uSize). */
-static uint64_t compress_p(const uint8_t *in, uint64_t n, uint8_t *dst, int s3_coded) {
+static uint64_t compress_p(const uint8_t *in, uint64_t n, uint8_t *dst, int s3_coded, int s4_full) {
     if (n == 0) return 0;
     or_tokens t;
     tokens_of(in, n, &t);
@@ -1110,7 +1223,16 @@ static uint64_t compress_p(const uint8_t *in, uint64_t n, uint8_t *dst, int s3_c
     uint8_t nib = 0;
     int raw_ok = !or_raw_literals_misparse(t.lit, t.nl);
     int fallback = 0;
-    if (t.nl > 0) {
+    if (t.nl > 0 && s4_full && t.nl <= 8u * 1024 * 1024) {
+        s4 = (uint8_t *)malloc(40 + 2 * t.nl + 4 * 1024);
+        l4 = or_package_literals(t.lit, t.nl, s4, &nib);
+        if (!nib) {  /* raw: the same decodability guard as P1 */
+            free(s4);
+            s4 = NULL;
+            l4 = t.nl;
+        }
+    }
+    if (t.nl > 0 && !nib && (!s4_full || !raw_ok || t.nl > 8u * 1024 * 1024)) {
         uint64_t vl = UINT64_MAX;
         uint8_t *vb = NULL;
         if (t.nl <= 8u * 1024 * 1024) {
@@ -1144,13 +1266,21 @@ static uint64_t compress_p(const uint8_t *in, uint64_t n, uint8_t *dst, int s3_c
     return w;
 }
 
-uint64_t or_compress_p1(const uint8_t *in, uint64_t n, uint8_t *dst) { return compress_p(in, n, dst, 0); }
+uint64_t or_compress_p1(const uint8_t *in, uint64_t n, uint8_t *dst) { return compress_p(in, n, dst, 0, 0); }
 
 /* Profile P2 == P1 with Section 3 as PackageOffsetsSection of the frame's
  * distances (core/distance/distance.go:825-849, as the reference's CPU
  * compressor writes it, compress.go:956): a distance-prefix container or
  * 0x09 varints, and an empty Section 3 when the frame has no match. */
-uint64_t or_compress_p2(const uint8_t *in, uint64_t n, uint8_t *dst) { return compress_p(in, n, dst, 1); }
+uint64_t or_compress_p2(const uint8_t *in, uint64_t n, uint8_t *dst) { return compress_p(in, n, dst, 1, 0); }
+
+/* Profile P3 == P2 with Section 4 as PackageLiteralsSection (literals.go:
+ * 664-693, as the reference's CPU compressor writes it): the smallest of the
+ * adaptive V-ANS container and the four étale-sheaf foliations, else raw
+ * under P1's decodability rule (the adaptive container when the raw bytes
+ * would be misread as one, else a stored frame); containers only for
+ * literals of at most 8 MiB (the decoders' literal and fiber buffers). */
+uint64_t or_compress_p3(const uint8_t *in, uint64_t n, uint8_t *dst) { return compress_p(in, n, dst, 1, 1); }
 
 /* Tokens only (Tokenize, gpu/bridge.go:1895), for tests. */
 void or_tokenize_input(const uint8_t *in, uint64_t n, uint8_t *cmd, uint64_t *nc, uint8_t *off, uint64_t *no,
