@@ -287,6 +287,18 @@ int32_t przmg_vans_encode_batch(przmg_ctx* ctx, uint64_t d_in, const uint64_t* i
 int32_t przmg_package_offsets_batch(przmg_ctx* ctx, uint64_t d_dist, const uint64_t* dist_offs, const uint32_t* counts,
                                     uint64_t count, uint64_t d_out, const uint64_t* out_offs, const uint64_t* out_caps,
                                     uint64_t* out_lens, uint64_t stream);
+/* PackageLiteralsSection, core/literals/literals.go:664-693, for many
+ * literal streams in one call: the Section 4 bytes the reference's CPU
+ * compressor writes for each -- the smallest of the adaptive V-ANS container
+ * and the four étale-sheaf foliations (literals.go:600-662, sheaf.go) when
+ * one is smaller than the literals, else the literals themselves -- and its
+ * flag nibble (nibbles[i] = 0x80 for a container, 0 for raw).  Stream i is
+ * lens[i] <= 4 MiB bytes at d_in + in_offs[i]; its section goes to
+ * d_out + out_offs[i] (out_caps[i] >= lens[i] always suffices).  At most
+ * 65535 streams per call.  Synchronises the stream. */
+int32_t przmg_package_literals_batch(przmg_ctx* ctx, uint64_t d_in, const uint64_t* in_offs, const uint32_t* lens,
+                                     uint64_t count, uint64_t d_out, const uint64_t* out_offs, const uint64_t* out_caps,
+                                     uint64_t* out_lens, uint8_t* nibbles, uint64_t stream);
 
 /* ---- allocation-free V-ANS encode: no counterpart in the reference -------
  * Histogram + normalise + V-ANS of ONE device stream: the same launch

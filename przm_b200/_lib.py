@@ -95,6 +95,7 @@ SIGNATURES: dict[str, tuple] = {
     "przmg_vans_encode4x_host": (i32, [vp, vp, u64, vp, u64, vp, vp]),
     "przmg_vans_encode_batch": (i32, [vp, u64, vp, vp, u64, i32, u64, vp, vp, u64]),
     "przmg_package_offsets_batch": (i32, [vp, u64, vp, vp, u64, u64, vp, vp, vp, u64]),
+    "przmg_package_literals_batch": (i32, [vp, u64, vp, vp, u64, u64, vp, vp, vp, vp, u64]),
     "przmg_vans_encode_noalloc": (i32, [u64, u32, i32, u64, u64, u64, u64]),
     "przmg_serve_create": (i32, [vp, i32, u64, i32, u64, vp]),
     "przmg_serve_submit": (i32, [vp, vp, u64, vp]),

@@ -161,7 +161,8 @@ struct Ctx {
     przmg_batch single;  // reused by the one-input calls
     HostBuf h_in, h_out, h_aux;
     DevBuf d_scr_in, d_scr_out, d_scr_aux, d_scr_tab;
-    DevBuf d_s3;  // scratch of przmg_package_offsets_batch
+    DevBuf d_s3;   // scratch of przmg_package_offsets_batch
+    DevBuf d_lit;  // scratch of przmg_package_literals_batch
     cudaEvent_t ev[8] = {};
 };
 
@@ -480,7 +481,7 @@ extern "C" int32_t przmg_close(przmg_ctx* h) {
         c->single.drop_graph();
         c->single.release();
         DevBuf* bufs[] = {&c->d_meta8, &c->d_ctxlut, &c->d_scr_in, &c->d_scr_out, &c->d_scr_aux,
-                          &c->d_scr_tab, &c->d_s3};
+                          &c->d_scr_tab, &c->d_s3, &c->d_lit};
         for (DevBuf* b : bufs) b->release();
         c->h_in.release();
         c->h_out.release();
@@ -1289,6 +1290,11 @@ extern "C" int32_t przmg_match_lz77_streaming(przmg_ctx* h, const uint8_t* src, 
 // Section 3 distance coding of many distance arrays
 // ---------------------------------------------------------------------------
 #include "offsets.inc"
+
+// ---------------------------------------------------------------------------
+// Section 4 selection (V-ANS or a sheaf foliation) of many literal streams
+// ---------------------------------------------------------------------------
+#include "literals.inc"
 
 // ---------------------------------------------------------------------------
 // serving: continuous batching of submitted requests

@@ -467,6 +467,20 @@ class GPUCompressor:
                                                _ptr(ol), stream))
         return ol[: len(ct)]
 
+    def PackageLiteralsBatch(self, dIn: int, inOffs, lens, dOut: int, outOffs, outCaps,
+                             stream: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        """PackageLiteralsSection (core/literals/literals.go:664) of many device
+        literal streams: (Section 4 sizes, flag nibbles 0x80 or 0)."""
+        io = np.ascontiguousarray(inOffs, np.uint64)
+        ln = np.ascontiguousarray(lens, np.uint32)
+        oo = np.ascontiguousarray(outOffs, np.uint64)
+        oc = np.ascontiguousarray(outCaps, np.uint64)
+        ol = np.zeros(max(len(ln), 1), np.uint64)
+        nb = np.zeros(max(len(ln), 1), np.uint8)
+        _check(L().przmg_package_literals_batch(self._h, dIn, _ptr(io), _ptr(ln), len(ln), dOut, _ptr(oo), _ptr(oc),
+                                                _ptr(ol), _ptr(nb), stream))
+        return ol[: len(ln)], nb[: len(ln)]
+
     # -- benchmarks --
     def BenchmarkVRAMBandwidth(self, sizeMB: int = 256, iterations: int = 10) -> float:
         g = C.c_double()
