@@ -295,6 +295,40 @@ def section3_measure(comp, sections: int, per: int = 20_000, calls: int = 5) -> 
             "timing": f"wall clock per synchronising call, best of {calls}"}
 
 
+def section4_measure(comp, streams: int, size: int = 256 << 10, calls: int = 5) -> dict:
+    """Section 4 selection on the device (przmg_package_literals_batch,
+    PackageLiteralsSection: adaptive V-ANS or one of four sheaf foliations)
+    of `streams` literal-like streams of `size` bytes (seeded order-1 Markov
+    text).  A call synchronises (the host compares the candidates), so the
+    figure is wall time per call, best of `calls` after one warm-up."""
+    import numpy as np
+    from przm_b200 import devmem
+    from przm_b200 import workloads as W
+    xs = [W.gen("markov", 0x50525A4D + 6 + i, size) for i in range(streams)]
+    lens = np.full(streams, size, np.uint32)
+    in_offs = np.arange(streams, dtype=np.uint64) * size
+    caps = np.full(streams, size, np.uint64)
+    out_offs = np.arange(streams, dtype=np.uint64) * (size + 16)
+    d_in = devmem.upload(np.concatenate(xs + [np.zeros(64, np.uint8)]))
+    d_out = devmem.alloc(int(out_offs[-1]) + size + 64)
+    ol, nb = comp.PackageLiteralsBatch(d_in.ptr, in_offs, lens, d_out.ptr, out_offs, caps)
+    best = float("inf")
+    for _ in range(calls):
+        t0 = time.perf_counter()
+        ol, nb = comp.PackageLiteralsBatch(d_in.ptr, in_offs, lens, d_out.ptr, out_offs, caps)
+        best = min(best, time.perf_counter() - t0)
+    forms: dict[str, int] = {}
+    for o, n, f in zip(out_offs, ol, nb):
+        h = devmem.download(d_out.ptr + int(o), 4) if f else b""
+        key = "raw" if not f else ("vans" if not h[3] & 0x04 else f"sheaf{h[3] >> 4}")
+        forms[key] = forms.get(key, 0) + 1
+    total = streams * size
+    return {"streams": streams, "bytes": total, "ms_per_call": round(best * 1e3, 3),
+            "gbps": round(total / best / 1e9, 3), "section_bytes": int(np.sum(ol)),
+            "ratio": round(float(np.sum(ol)) / total, 4), "forms": forms,
+            "timing": f"wall clock per synchronising call, best of {calls}"}
+
+
 def uneven_measure(comp, count: int, sample: int) -> dict:
     """The uneven-batch workload: `count` inputs with sizes log-uniform in
     [1 KiB, 4 MiB] and mixed contents.  All of them as one device-resident
@@ -410,6 +444,8 @@ def main() -> None:
     ap.add_argument("--uneven-sample", type=int, default=256, help="inputs timed batched vs plain")
     ap.add_argument("--section3-sections", type=int, default=256,
                     help="sections of the Section 3 distance-coding measurement (0: skip)")
+    ap.add_argument("--section4-streams", type=int, default=64,
+                    help="literal streams of the Section 4 selection measurement (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -599,6 +635,12 @@ def main() -> None:
             section3 = section3_measure(comp, args.section3_sections)
         except Exception as e:  # an extra leg never costs the bench line
             section3 = {"error": f"{type(e).__name__}: {e}"[:300]}
+    section4 = None
+    if args.section4_streams > 0 and world == 1:
+        try:
+            section4 = section4_measure(comp, args.section4_streams)
+        except Exception as e:  # an extra leg never costs the bench line
+            section4 = {"error": f"{type(e).__name__}: {e}"[:300]}
 
     # roofline of the dominant kernel
     peak, peak_kind = measured_peaks()
@@ -662,7 +704,7 @@ def main() -> None:
                     "link_gbs": link, "host": numa},
             "roofline": roofline, "pipeline_roofline": pipeline, "stage_ms": {k: round(v, 3) for k, v in stages.items()},
             "cpu_baseline": cpu_base, "plain_per_frame": plain, "clocks": clk, "gpu_launches": gl,
-            "serving": serve, "uneven_batch": uneven, "section3": section3,
+            "serving": serve, "uneven_batch": uneven, "section3": section3, "section4": section4,
         }
         print(json.dumps(line), flush=True)
     for bt in batches:
