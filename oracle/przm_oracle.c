@@ -1,5 +1,7 @@
 /*
- * przm_oracle.c -- CPU restatement of the PRZM GPU compression path.
+ * przm_oracle.c -- CPU restatement of the PRZM GPU compression path, and of
+ * the two section encoders it widens into (Section 3 distance coding,
+ * Section 4 selection with the sheaf foliations).
  *
  * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA product is
  * compared against; it is never linked into, called by, or used as a fallback
