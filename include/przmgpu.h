@@ -4,7 +4,7 @@
  * Drop-in boundary for the reference's Go `gpu` package (Lemon4ksan/przm,
  * gpu/bridge.go, gpu/types.go, gpu/memory.go).  Every entry point below
  * names the reference function it replaces.  A Go caller binds these through
- * cgo (see INTEGRATION.md); Python tests bind them through ctypes.
+ * cgo; Python tests bind them through ctypes.
  *
  * Conventions
  *   - status: int32, 0 = OK, negative = error (PRZMG_ERR_*); the numeric
@@ -152,6 +152,21 @@ int32_t przmg_tokenize(przmg_ctx* ctx, const uint8_t* src, uint64_t n, uint8_t* 
 /* TokenizeDevice / TokenizeDeviceZeroCopy, gpu/bridge.go:2139, 2247 */
 int32_t przmg_tokenize_device(przmg_ctx* ctx, const uint8_t* src, uint64_t n, przmg_device_streams_t* out,
                               przmg_tokenizer_profile_t* prof);
+/* TokenizeDeviceOnly, gpu/bridge.go:1915: runs only the tokenizer (parse,
+ * scan and gather) again on the input and match table the context staged in
+ * device memory for its last one-input call (przmg_tokenize,
+ * przmg_tokenize_device, przmg_match_table, przmg_compress...), and copies
+ * the streams out as przmg_tokenize does.  n must equal that input's size
+ * (the reference reads whatever its slot holds; here a call with nothing
+ * staged, or with another n, fails with PRZMG_ERR_INVALID_ARG).  n == 0
+ * succeeds with empty streams. */
+int32_t przmg_tokenize_device_only(przmg_ctx* ctx, uint64_t n, uint8_t* cmd, uint64_t cmd_cap, uint8_t* off,
+                                   uint64_t off_cap, uint8_t* lit, uint64_t lit_cap, uint64_t lens[3],
+                                   przmg_tokenizer_profile_t* prof);
+/* TokenizePointersDeviceOnly, gpu/bridge.go:2163: the same tokenizer-only
+ * run, returning borrowed device pointers like przmg_tokenize_device. */
+int32_t przmg_tokenize_pointers_device_only(przmg_ctx* ctx, uint64_t n, przmg_device_streams_t* out,
+                                            przmg_tokenizer_profile_t* prof);
 /* DownloadDeviceBytes, gpu/bridge.go:2253 */
 int32_t przmg_download_device_bytes(przmg_ctx* ctx, uint64_t d_ptr, uint64_t size, uint8_t* dst);
 
@@ -311,14 +326,23 @@ int32_t przmg_package_literals_batch(przmg_ctx* ctx, uint64_t d_in, const uint64
  * 2.3 MiB per device, so n is limited to PRZMG_NOALLOC_MAX_N symbols.
  *   n > PRZMG_NOALLOC_MAX_N           -> PRZMG_ERR_EXCEEDS_MAX_BLOCK
  *   out_cap < 1024 + 2 * n            -> PRZMG_ERR_BUFFER_TOO_SMALL
- *   unknown norm or null address      -> PRZMG_ERR_INVALID_ARG
- * (nothing is launched on an error; przmg_last_error() says why).
+ *   unknown norm, null address, or
+ *   d_out_len not 4-byte aligned      -> PRZMG_ERR_INVALID_ARG
+ * (nothing is launched on these errors; przmg_last_error() says why).  A
+ * CUDA error pending from earlier work is returned (PRZMG_ERR_CUDA) before
+ * anything is queued.  A CUDA error raised by one of the call's own launches
+ * returns PRZMG_ERR_CUDA with part of the sequence already queued; d_out and
+ * d_out_len are then undefined.
  * Runs on the CURRENT device, asynchronously on `stream` (0 = the legacy
  * default stream); the container length is written as a u32 to the device
- * address d_out_len when the stream reaches it.  The first call on each
- * device does setup (cudaGetSymbolAddress of the scratch with that device
- * current, which may load the module, and the rANS kernel's shared-memory
- * attribute): make one call on every device before capturing a stream.
+ * address d_out_len (4-byte aligned) when the stream reaches it.  The first
+ * call on each device does setup (cudaGetSymbolAddress of the scratch with
+ * that device current, which may load the module, and the rANS kernel's
+ * shared-memory attribute): make one call on every device before capturing a
+ * stream.  The scratch address is looked up once per device and process:
+ * after cudaDeviceReset of a device this entry point must not be called on
+ * that device again in the same process (the cached address belonged to the
+ * destroyed context).
  * Nothing in the scratch has to start at zero: each call clears the 1 KiB
  * histogram it counts into and overwrites the rest before reading it.
  * All calls on one device share the one scratch, so calls that overlap in
@@ -343,6 +367,27 @@ int32_t przmg_benchmark_entropy_vram(przmg_ctx* ctx, int32_t size_mb, int32_t it
 /* ---- pinned host memory (gpu/memory.go:51-165) --------------------------- */
 int32_t przmg_alloc_pinned_host(uint64_t size, void** out); /* AllocPinnedHost */
 int32_t przmg_free_pinned_host(void* p);                    /* FreePinnedHost */
+
+/* PinnedBufferPool, gpu/memory.go:91-165: thread-safe reuse of pinned host
+ * buffers of one size.  create = NewPinnedBufferPool(buf_size, initial_cap)
+ * (initial_cap buffers allocated up front; the pool keeps at most
+ * max(initial_cap, 8)); get = Get (a pooled buffer, else a new one); put =
+ * Put (len must equal the pool's buffer size, else the buffer is ignored, as
+ * in the reference; a full pool frees it); close = Close (frees the pooled
+ * buffers, then the pool, unless the pool belongs to a context -- see
+ * przmg_get_pinned -- in which case the context frees it in przmg_close). */
+typedef struct przmg_pinned_pool przmg_pinned_pool;
+int32_t przmg_pinned_pool_create(uint64_t buf_size, int32_t initial_cap, przmg_pinned_pool** out);
+int32_t przmg_pinned_pool_get(przmg_pinned_pool* pool, void** buf);
+void przmg_pinned_pool_put(przmg_pinned_pool* pool, void* buf, uint64_t len);
+int32_t przmg_pinned_pool_close(przmg_pinned_pool* pool);
+uint64_t przmg_pinned_pool_buf_size(const przmg_pinned_pool* pool);
+uint64_t przmg_pinned_pool_pooled(przmg_pinned_pool* pool); /* buffers held (for tests) */
+/* GetPinned, gpu/bridge.go:452: leases a buffer of at least size bytes from
+ * the context's pool of the next power-of-two size (created on first use,
+ * owned by the context).  *pool receives that pool: return the buffer with
+ * przmg_pinned_pool_put(pool, buf, przmg_pinned_pool_buf_size(pool)). */
+int32_t przmg_get_pinned(przmg_ctx* ctx, uint64_t size, void** buf, przmg_pinned_pool** pool);
 
 #ifdef __cplusplus
 }

@@ -448,6 +448,14 @@ def ref_decode_meta8(container: bytes, n: int) -> bytes:
 #   ref_tokenize       d_matches n x u32; per 32 KiB chunk 36864 bytes of
 #                      cmd/off/lit slot; d_lens 6 x chunks u32; d_totals 3 x
 #                      u32; all input reads stay below the tile end.
+#   cuda_lz77_match_batch        (the reference's own host wrapper,
+#                      przm_lz77.cu:458-475) tile finder over n bytes in
+#                      32 KiB tiles, <<<224, 256>>>; writes d_matches[0, n).
+#   cuda_lz77_radix_strike_batch (przm_lz77.cu:477-502) clears the 2 MiB
+#                      d_radix_table (2^19 u32) and runs the radix-strike
+#                      kernel; writes d_matches[p] only where it finds a
+#                      match, so the caller clears d_matches (n x u32) first.
+#                      All reads stay below n.
 
 _REFCUDA = None
 
@@ -471,6 +479,10 @@ def ref_cuda() -> C.CDLL:
         R.ref_vans_encode4x.argtypes = [vp, u32, vp, vp, vp, u32, vp, vp, vp, vp]
         R.ref_tokenize.restype = C.c_int
         R.ref_tokenize.argtypes = [vp, u64, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32, vp]
+        R.cuda_lz77_match_batch.restype = C.c_int
+        R.cuda_lz77_match_batch.argtypes = [vp, C.c_size_t, vp, C.c_size_t, vp]
+        R.cuda_lz77_radix_strike_batch.restype = C.c_int
+        R.cuda_lz77_radix_strike_batch.argtypes = [vp, C.c_size_t, vp, vp, C.c_size_t, vp]
         _REFCUDA = R
     return _REFCUDA
 

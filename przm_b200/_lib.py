@@ -67,6 +67,8 @@ SIGNATURES: dict[str, tuple] = {
     "przmg_match_lz77_streaming": (i32, [vp, vp, u64, i64, vp, u64, vp, vp]),
     "przmg_tokenize": (i32, [vp, vp, u64, vp, u64, vp, u64, vp, u64, vp, vp]),
     "przmg_tokenize_device": (i32, [vp, vp, u64, vp, vp]),
+    "przmg_tokenize_device_only": (i32, [vp, u64, vp, u64, vp, u64, vp, u64, vp, vp]),
+    "przmg_tokenize_pointers_device_only": (i32, [vp, u64, vp, vp]),
     "przmg_download_device_bytes": (i32, [vp, u64, u64, vp]),
     "przmg_frame_bound": (u64, [u64]),
     "przmg_encode_d2d": (i32, [vp, vp, u32, i32, vp, u64, vp, vp]),
@@ -112,6 +114,13 @@ SIGNATURES: dict[str, tuple] = {
     "przmg_benchmark_entropy_vram": (i32, [vp, i32, i32, vp]),
     "przmg_alloc_pinned_host": (i32, [u64, vp]),
     "przmg_free_pinned_host": (i32, [vp]),
+    "przmg_pinned_pool_create": (i32, [u64, i32, vp]),
+    "przmg_pinned_pool_get": (i32, [vp, vp]),
+    "przmg_pinned_pool_put": (None, [vp, vp, u64]),
+    "przmg_pinned_pool_close": (i32, [vp]),
+    "przmg_pinned_pool_buf_size": (u64, [vp]),
+    "przmg_pinned_pool_pooled": (u64, [vp]),
+    "przmg_get_pinned": (i32, [vp, u64, vp, vp]),
 }
 
 _LIB: C.CDLL | None = None

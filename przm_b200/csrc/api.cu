@@ -133,6 +133,9 @@ struct przmg_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int launches = 0;
+    // the batch holds one input and its match table from a completed
+    // one-input call (what the tokenizer-only entry points run on)
+    bool staged_single = false;
     ~przmg_batch() { drop_graph(); release(); }
     void drop_graph() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -151,10 +154,27 @@ struct przmg_batch {
     uint32_t* err_word() const { return d_misc.as<uint32_t>(); }
 };
 
+// PinnedBufferPool (gpu/memory.go:91-165): a mutex-guarded stack of pinned
+// host buffers of one size, at most max_cap of them kept.
+struct przmg_pinned_pool {
+    std::mutex mu;
+    uint64_t buf_size = 0;
+    size_t max_cap = 8;
+    std::vector<void*> free_bufs;
+    bool ctx_owned = false;  // created by GetPinned: the context frees it
+    void free_all() {
+        std::lock_guard<std::mutex> lk(mu);
+        for (void* p : free_bufs) cudaFreeHost(p);
+        free_bufs.clear();
+    }
+};
+
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::mutex mu;
+    std::mutex pools_mu;
+    std::unordered_map<uint64_t, przmg_pinned_pool*> pools;  // GetPinned pools by power-of-two size
     cudaDeviceProp prop{};
     int sms = 148;
     DevBuf d_meta8, d_ctxlut;
@@ -171,6 +191,7 @@ struct Ctx {
 static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njobs, int profile, bool force_radix,
                              cudaStream_t setup = nullptr) {
     b->drop_graph();
+    b->staged_single = false;
     b->profile = profile;
     b->force_radix = force_radix;
     b->njobs = njobs;
@@ -294,13 +315,15 @@ constexpr int kStages = 8;
 
 // ev (optional): kStages + 1 events; ev[0] before the first kernel and
 // ev[k + 1] after stage k (stages that do not run record back to back).
-static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cudaEvent_t* ev = nullptr) {
+// skip_match: the match table is already in d_desc (tokenizer-only runs).
+static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cudaEvent_t* ev = nullptr,
+                            bool skip_match = false) {
     Ctx* c = b->ctx;
     int launches = 0;
     CK(cudaMemsetAsync(b->d_misc.p, 0, 16, s));
     auto mark = [&](int k) -> cudaError_t { return ev ? cudaEventRecord(ev[k], s) : cudaSuccess; };
     CK(mark(0));
-    if (b->nsmall) {
+    if (b->nsmall && !skip_match) {
         const uint32_t grid = std::min<uint32_t>(b->nsmall, 8u * c->sms);
         k_tile_find<<<grid, 256, kTileFindSmem, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_small.as<TileRef>(),
                                                      b->nsmall, b->d_desc.as<uint32_t>());
@@ -308,7 +331,7 @@ static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cuda
         launches++;
     }
     CK(mark(1));
-    if (b->nbig && !b->rtiles.empty()) {
+    if (b->nbig && !b->rtiles.empty() && !skip_match) {
         const uint32_t nrt = (uint32_t)b->rtiles.size();
         const uint32_t gt = std::min<uint32_t>(nrt, 16u * c->sms);
         k_rx_count<<<gt, 256, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_rtiles.as<RxTile>(), nrt,
@@ -490,6 +513,14 @@ extern "C" int32_t przmg_close(przmg_ctx* h) {
         cudaStreamDestroy(c->stream);
     }
     {
+        std::lock_guard<std::mutex> lk(c->pools_mu);
+        for (auto& kv : c->pools) {
+            kv.second->free_all();
+            delete kv.second;
+        }
+        c->pools.clear();
+    }
+    {
         std::lock_guard<std::mutex> g(g_global_mu);
         if (g_global == c) g_global = nullptr;
     }
@@ -586,6 +617,7 @@ static int32_t single_run(Ctx* c, const uint8_t* src, uint64_t n, int profile, i
     CK(cudaEventRecord(c->ev[2], c->stream));
     r = batch_check(b);
     if (r) return r;
+    b->staged_single = true;
     if (prof) {
         *prof = przmg_profile_t{};
         prof->ingress_dma_bytes = n;
@@ -650,10 +682,27 @@ extern "C" int32_t przmg_compress(przmg_ctx* h, const uint8_t* src, uint64_t n, 
     return compress_one(c, src, n, profile, dst, cap, out_len, prof);
 }
 
+// src != null: stage src and run match + tokenize; src == null: tokenize
+// again the input and match table staged by the last one-input call
+// (TokenizeDeviceOnly, gpu/bridge.go:1915-1940).
 static int32_t tokenize_common(Ctx* c, const uint8_t* src, uint64_t n, przmg_tokenizer_profile_t* prof, uint32_t lens6[6]) {
-    int32_t r = single_run(c, src, n, PRZMG_PROFILE_D2D, 1, false, nullptr);
-    if (r) return r;
     przmg_batch* b = &c->single;
+    if (src) {
+        int32_t r = single_run(c, src, n, PRZMG_PROFILE_D2D, 1, false, nullptr);
+        if (r) return r;
+    } else {
+        if (!b->staged_single || b->njobs != 1 || b->jobs[0].n != n)
+            return fail(PRZMG_ERR_INVALID_ARG, "no staged input of " + std::to_string(n) +
+                                                   " bytes: the tokenizer-only calls run on the input of the last "
+                                                   "one-input call (przmg_tokenize, przmg_match_table, ...)");
+        CK(cudaEventRecord(c->ev[0], c->stream));
+        CK(cudaEventRecord(c->ev[1], c->stream));
+        int32_t r = batch_launch(b, c->stream, 1, nullptr, true);
+        if (r) return r;
+        CK(cudaEventRecord(c->ev[2], c->stream));
+        r = batch_check(b);
+        if (r) return r;
+    }
     CK(cudaMemcpyAsync(lens6, b->d_job_lens.p, 24, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (prof) {
@@ -670,6 +719,12 @@ static int32_t tokenize_common(Ctx* c, const uint8_t* src, uint64_t n, przmg_tok
     return PRZMG_OK;
 }
 
+static int32_t tokenize_to_host(Ctx* c, const uint8_t* src, uint64_t n, uint8_t* cmd, uint64_t cmd_cap, uint8_t* off,
+                                uint64_t off_cap, uint8_t* lit, uint64_t lit_cap, uint64_t lens[3],
+                                przmg_tokenizer_profile_t* prof);
+static int32_t tokenize_to_device(Ctx* c, const uint8_t* src, uint64_t n, przmg_device_streams_t* out,
+                                  przmg_tokenizer_profile_t* prof);
+
 extern "C" int32_t przmg_tokenize(przmg_ctx* h, const uint8_t* src, uint64_t n, uint8_t* cmd, uint64_t cmd_cap,
                                   uint8_t* off, uint64_t off_cap, uint8_t* lit, uint64_t lit_cap, uint64_t lens[3],
                                   przmg_tokenizer_profile_t* prof) {
@@ -681,11 +736,31 @@ extern "C" int32_t przmg_tokenize(przmg_ctx* h, const uint8_t* src, uint64_t n, 
     if (n == 0) return PRZMG_OK;
     if (!src) return fail(PRZMG_ERR_INVALID_ARG, "null source");
     LOCKED(c);
+    return tokenize_to_host(c, src, n, cmd, cmd_cap, off, off_cap, lit, lit_cap, lens, prof);
+}
+
+extern "C" int32_t przmg_tokenize_device_only(przmg_ctx* h, uint64_t n, uint8_t* cmd, uint64_t cmd_cap, uint8_t* off,
+                                              uint64_t off_cap, uint8_t* lit, uint64_t lit_cap, uint64_t lens[3],
+                                              przmg_tokenizer_profile_t* prof) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c || !lens) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    lens[0] = lens[1] = lens[2] = 0;
+    if (prof) *prof = przmg_tokenizer_profile_t{};
+    if (n == 0) return PRZMG_OK;
+    LOCKED(c);
+    return tokenize_to_host(c, nullptr, n, cmd, cmd_cap, off, off_cap, lit, lit_cap, lens, prof);
+}
+
+static int32_t tokenize_to_host(Ctx* c, const uint8_t* src, uint64_t n, uint8_t* cmd, uint64_t cmd_cap, uint8_t* off,
+                                uint64_t off_cap, uint8_t* lit, uint64_t lit_cap, uint64_t lens[3],
+                                przmg_tokenizer_profile_t* prof) {
     uint32_t l6[6];
     int32_t r = tokenize_common(c, src, n, prof, l6);
     if (r) return r;
     if (l6[S_CMD] > cmd_cap || l6[S_OFF] > off_cap || l6[S_LIT] > lit_cap)
         return fail(PRZMG_ERR_BUFFER_TOO_SMALL, "stream buffers too small");
+    if ((l6[S_CMD] && !cmd) || (l6[S_OFF] && !off) || (l6[S_LIT] && !lit))
+        return fail(PRZMG_ERR_INVALID_ARG, "null stream buffer");
     przmg_batch* b = &c->single;
     const Job& j = b->jobs[0];
     const uint8_t* base = b->d_streams.as<uint8_t>() + j.str_off;
@@ -709,6 +784,22 @@ extern "C" int32_t przmg_tokenize_device(przmg_ctx* h, const uint8_t* src, uint6
     if (n == 0) return PRZMG_OK;
     if (!src) return fail(PRZMG_ERR_INVALID_ARG, "null source");
     LOCKED(c);
+    return tokenize_to_device(c, src, n, out, prof);
+}
+
+extern "C" int32_t przmg_tokenize_pointers_device_only(przmg_ctx* h, uint64_t n, przmg_device_streams_t* out,
+                                                       przmg_tokenizer_profile_t* prof) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c || !out) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    *out = przmg_device_streams_t{};
+    if (prof) *prof = przmg_tokenizer_profile_t{};
+    if (n == 0) return PRZMG_OK;
+    LOCKED(c);
+    return tokenize_to_device(c, nullptr, n, out, prof);
+}
+
+static int32_t tokenize_to_device(Ctx* c, const uint8_t* src, uint64_t n, przmg_device_streams_t* out,
+                                  przmg_tokenizer_profile_t* prof) {
     uint32_t l6[6];
     int32_t r = tokenize_common(c, src, n, prof, l6);
     if (r) return r;
@@ -1321,4 +1412,97 @@ extern "C" int32_t przmg_free_pinned_host(void* p) {
     if (!p) return PRZMG_OK;
     CK(cudaFreeHost(p));
     return PRZMG_OK;
+}
+
+// NewPinnedBufferPool, gpu/memory.go:108-124
+extern "C" int32_t przmg_pinned_pool_create(uint64_t buf_size, int32_t initial_cap, przmg_pinned_pool** out) {
+    if (!out) return fail(PRZMG_ERR_INVALID_ARG, "null output pointer");
+    *out = nullptr;
+    if (buf_size == 0 || initial_cap < 0) return fail(PRZMG_ERR_INVALID_ARG, "invalid pool size");
+    auto* p = new przmg_pinned_pool();
+    p->buf_size = buf_size;
+    p->max_cap = std::max<size_t>((size_t)initial_cap, 8);
+    for (int32_t i = 0; i < initial_cap; i++) {
+        void* b = nullptr;
+        cudaError_t e = cudaHostAlloc(&b, buf_size, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            p->free_all();
+            delete p;
+            return cuda_fail("cudaHostAlloc", e);
+        }
+        p->free_bufs.push_back(b);
+    }
+    *out = p;
+    return PRZMG_OK;
+}
+
+// PinnedBufferPool.Get, gpu/memory.go:127-141
+extern "C" int32_t przmg_pinned_pool_get(przmg_pinned_pool* p, void** buf) {
+    if (!p || !buf) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    *buf = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(p->mu);
+        if (!p->free_bufs.empty()) {
+            *buf = p->free_bufs.back();
+            p->free_bufs.pop_back();
+            return PRZMG_OK;
+        }
+    }
+    CK(cudaHostAlloc(buf, p->buf_size, cudaHostAllocDefault));
+    return PRZMG_OK;
+}
+
+// PinnedBufferPool.Put, gpu/memory.go:144-155
+extern "C" void przmg_pinned_pool_put(przmg_pinned_pool* p, void* buf, uint64_t len) {
+    if (!p || !buf || len != p->buf_size) return;
+    {
+        std::lock_guard<std::mutex> lk(p->mu);
+        if (p->free_bufs.size() < p->max_cap) {
+            p->free_bufs.push_back(buf);
+            return;
+        }
+    }
+    cudaFreeHost(buf);
+}
+
+// PinnedBufferPool.Close, gpu/memory.go:158-165
+extern "C" int32_t przmg_pinned_pool_close(przmg_pinned_pool* p) {
+    if (!p) return PRZMG_OK;
+    p->free_all();
+    if (!p->ctx_owned) delete p;
+    return PRZMG_OK;
+}
+
+extern "C" uint64_t przmg_pinned_pool_buf_size(const przmg_pinned_pool* p) { return p ? p->buf_size : 0; }
+
+extern "C" uint64_t przmg_pinned_pool_pooled(przmg_pinned_pool* p) {
+    if (!p) return 0;
+    std::lock_guard<std::mutex> lk(p->mu);
+    return p->free_bufs.size();
+}
+
+// GetPinned, gpu/bridge.go:452-471: pools keyed by the next power of two
+extern "C" int32_t przmg_get_pinned(przmg_ctx* h, uint64_t size, void** buf, przmg_pinned_pool** pool) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c || !buf || !pool) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    *buf = nullptr;
+    *pool = nullptr;
+    if (size == 0 || size > (1ull << 62)) return fail(PRZMG_ERR_INVALID_ARG, "invalid size");
+    uint64_t alloc = 1;
+    while (alloc < size) alloc <<= 1;
+    przmg_pinned_pool* p = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(c->pools_mu);
+        auto it = c->pools.find(alloc);
+        if (it == c->pools.end()) {
+            int32_t r = przmg_pinned_pool_create(alloc, 0, &p);
+            if (r) return r;
+            p->ctx_owned = true;
+            c->pools[alloc] = p;
+        } else {
+            p = it->second;
+        }
+    }
+    *pool = p;
+    return przmg_pinned_pool_get(p, buf);
 }

@@ -79,11 +79,13 @@ __host__ __device__ inline uint64_t stream_region_bytes(const Job& j) {
 // 64-byte chunks (64-byte aligned), so every lane region is a multiple of 64
 // with room for the last partial chunk.
 constexpr uint32_t kStitchRounds = 4096;  // rounds of one stitch pass (256 threads x 16)
-__host__ __device__ inline uint64_t ans_lane_cap(uint32_t L) { return ((2ull * ((L + 3) / 4) + 128) + 63) & ~63ull; }
-__host__ __device__ inline uint64_t ans_nbw_words(uint32_t L) { return (((L + 3) / 4) + 15) / 16 + 1; }
-__host__ __device__ inline uint64_t ans_cum_words(uint32_t L) { return ((L + 3) / 4 + kStitchRounds - 1) / kStitchRounds + 1; }
-__host__ __device__ inline uint64_t ans_nbw_cap(uint32_t L) { return ans_nbw_words(L) + ans_cum_words(L); }  // u32 words
-__host__ __device__ inline uint64_t ans_task_bytes(uint32_t L) {
+// (constexpr, so that fixed-size scratch can be checked against them at
+// compile time)
+__host__ __device__ constexpr uint64_t ans_lane_cap(uint32_t L) { return ((2ull * ((L + 3) / 4) + 128) + 63) & ~63ull; }
+__host__ __device__ constexpr uint64_t ans_nbw_words(uint32_t L) { return (((L + 3) / 4) + 15) / 16 + 1; }
+__host__ __device__ constexpr uint64_t ans_cum_words(uint32_t L) { return ((L + 3) / 4 + kStitchRounds - 1) / kStitchRounds + 1; }
+__host__ __device__ constexpr uint64_t ans_nbw_cap(uint32_t L) { return ans_nbw_words(L) + ans_cum_words(L); }  // u32 words
+__host__ __device__ constexpr uint64_t ans_task_bytes(uint32_t L) {
     uint64_t b = 4 * ans_lane_cap(L) + 4 * 4 * ans_nbw_cap(L);
     return (b + 63) & ~63ull;
 }

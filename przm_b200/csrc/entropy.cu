@@ -6,7 +6,12 @@
 namespace pz {
 
 // ---------------------------------------------------------------------------
-// Encoding tables.
+// Encoding tables.  The step x' = x + bias + floor(x / f) * (M - f) with the
+// quotient from a multiply-high by a per-symbol reciprocal, and the f = 1
+// case done as a one-short reciprocal with the deficit moved into the bias,
+// is the reciprocal-encoder form of rANS that F. Giesen published with
+// ryg_rans (rans_byte.h, RansEncSymbolInit / RansEncPutSymbol, 2014); the
+// reciprocal itself is Granlund-Montgomery's (PLDI 1994).
 // ---------------------------------------------------------------------------
 __host__ __device__ inline EncSym make_encsym(uint32_t f, uint32_t c) {
     EncSym e;

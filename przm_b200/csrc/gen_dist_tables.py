@@ -15,8 +15,9 @@ import sys
 
 
 def main() -> None:
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    src = open(f"{root}/core/distance/distance.go").read()
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python gen_dist_tables.py /path/to/przm-checkout > dist_tables.h")
+    src = open(f"{sys.argv[1]}/core/distance/distance.go").read()
     start = src.index("{", src.index("var StaticDistFreq4"))
     stop = src.index("type distModel")
     nums = [int(x) for x in re.findall(r"\b\d+\b", src[start:stop])]

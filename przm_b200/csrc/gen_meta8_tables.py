@@ -15,8 +15,9 @@ import sys
 
 
 def main() -> None:
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    src = open(f"{root}/core/commands/vans_meta_tables.go").read()
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python gen_meta8_tables.py /path/to/przm-checkout > meta8_tables.h")
+    src = open(f"{sys.argv[1]}/core/commands/vans_meta_tables.go").read()
     start = src.index("{", src.index("StaticMetaFreq8"))
     stop = src.index("var staticMetaFreq8")
     nums = [int(x) for x in re.findall(r"\b\d+\b", src[start:stop])]

@@ -236,6 +236,54 @@ def FreePinnedHost(ptr: int) -> None:
     _check(L().przmg_free_pinned_host(C.c_void_p(ptr)))
 
 
+class PinnedBuffer:
+    """gpu/memory.go:91-95: a pinned slice (Bytes, a numpy view of the first
+    len bytes) and its host address Ptr."""
+
+    def __init__(self, Bytes: np.ndarray, Ptr: int):
+        self.Bytes = Bytes
+        self.Ptr = Ptr
+
+    @staticmethod
+    def _of(ptr: int, alloc: int, length: int) -> "PinnedBuffer":
+        raw = (C.c_uint8 * alloc).from_address(ptr)
+        return PinnedBuffer(np.frombuffer(raw, np.uint8)[:length], ptr)
+
+
+class PinnedBufferPool:
+    """gpu/memory.go:98-165 over przmg_pinned_pool_*: Get, Put, Close."""
+
+    def __init__(self, bufSize: int, initialCap: int = 0):
+        """NewPinnedBufferPool, gpu/memory.go:108"""
+        h = C.c_void_p()
+        _check(L().przmg_pinned_pool_create(bufSize, initialCap, C.byref(h)))
+        self._h = h
+        self.bufSize = bufSize
+
+    @classmethod
+    def _of(cls, handle, bufSize: int) -> "PinnedBufferPool":
+        p = cls.__new__(cls)
+        p._h = handle
+        p.bufSize = bufSize
+        return p
+
+    def Get(self) -> PinnedBuffer:
+        b = C.c_void_p()
+        _check(L().przmg_pinned_pool_get(self._h, C.byref(b)))
+        return PinnedBuffer._of(b.value, self.bufSize, self.bufSize)
+
+    def Put(self, buf: PinnedBuffer) -> None:
+        L().przmg_pinned_pool_put(self._h, C.c_void_p(buf.Ptr), len(buf.Bytes))
+
+    def Pooled(self) -> int:
+        return int(L().przmg_pinned_pool_pooled(self._h))
+
+    def Close(self) -> None:
+        if self._h:
+            _check(L().przmg_pinned_pool_close(self._h))
+        self._h = None
+
+
 class GPUCompressor:
     """gpu/bridge.go:239-288: one device context with its own stream and
     grow-only device pools; calls on one instance are serialised."""
@@ -325,6 +373,34 @@ class GPUCompressor:
                                    d.lit_len, d.num_chunks, d.stream), TokenizerProfile.of(p))
 
     TokenizeDeviceZeroCopy = TokenizeDevice  # gpu/bridge.go:2247
+
+    def TokenizeDeviceOnly(self, n: int) -> tuple[bytes, bytes, bytes, TokenizerProfile]:
+        """gpu/bridge.go:1915: the tokenizer alone, again, on the input and
+        match table staged by the last one-input call (n must be its size)."""
+        tiles = max((n + TokenizerTileSize - 1) // TokenizerTileSize, 1)
+        cap = tiles * 36864
+        cmd, off, lit = (np.zeros(cap, np.uint8) for _ in range(3))
+        lens = (C.c_uint64 * 3)()
+        p = _lib.TokProfile()
+        _check(L().przmg_tokenize_device_only(self._h, n, _ptr(cmd), cap, _ptr(off), cap, _ptr(lit), cap, lens,
+                                              C.byref(p)))
+        return bytes(cmd[: lens[0]]), bytes(off[: lens[1]]), bytes(lit[: lens[2]]), TokenizerProfile.of(p)
+
+    def TokenizePointersDeviceOnly(self, n: int) -> tuple[DeviceTokenStreams, TokenizerProfile]:
+        """gpu/bridge.go:2163 (pointers valid until the next call)"""
+        d = _lib.DevStreams()
+        p = _lib.TokProfile()
+        _check(L().przmg_tokenize_pointers_device_only(self._h, n, C.byref(d), C.byref(p)))
+        return (DeviceTokenStreams(d.d_final_cmds, d.d_final_offs, d.d_final_lits, d.d_totals, d.cmd_len, d.off_len,
+                                   d.lit_len, d.num_chunks, d.stream), TokenizerProfile.of(p))
+
+    def GetPinned(self, size: int) -> tuple["PinnedBuffer", "PinnedBufferPool"]:
+        """gpu/bridge.go:452: a buffer from the context's pool of the next
+        power-of-two size; Bytes is sliced to size (as in the reference)."""
+        buf, pool = C.c_void_p(), C.c_void_p()
+        _check(L().przmg_get_pinned(self._h, size, C.byref(buf), C.byref(pool)))
+        p = PinnedBufferPool._of(pool, int(L().przmg_pinned_pool_buf_size(pool)))
+        return PinnedBuffer._of(buf.value, p.bufSize, size), p
 
     def DownloadDeviceBytes(self, dPtr: int, size: int) -> bytes:
         """gpu/bridge.go:2253"""

@@ -1,8 +1,9 @@
 """przmg_vans_encode_noalloc: the allocation-free single-stream V-ANS entry
 point (static device scratch).  It must give the same container bytes as
-przmg_vans_encode_batch with one stream on consecutive calls, and refuse
-sizes beyond its fixed scratch.  The file name sorts last, so in a full run
-it also goes after every other GPU test of the process."""
+przmg_vans_encode_batch with one stream and as the oracle's encoder on
+consecutive calls, allocate no device memory, and refuse sizes beyond its
+fixed scratch.  The file name sorts last, so in a full run it also goes
+after every other GPU test of the process."""
 from __future__ import annotations
 
 import ctypes as C
@@ -35,8 +36,22 @@ def _encode_batch(comp, d_in: int, n: int, norm: int, d_out: int) -> bytes:
     return devmem.download(d_out, int(ol[0]))
 
 
+def _encode_oracle(oracle, a: np.ndarray, norm: int) -> bytes:
+    # VANSEncode4xHost (NormalizeFreq, flag 0x01) or EncodeAdaptiveVANS4x
+    # (NormalizeFrequencies, flag 0x00) restated on the CPU
+    return oracle.vans_encode_host(a) if norm == gpu.NORM_GO else oracle.adaptive_vans(a)
+
+
+def _free_device_bytes() -> int:
+    free, total = C.c_size_t(), C.c_size_t()
+    rt = devmem.rt()
+    rt.cudaMemGetInfo.argtypes = [C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+    assert rt.cudaMemGetInfo(C.byref(free), C.byref(total)) == 0
+    return free.value
+
+
 @pytest.mark.parametrize("norm", [gpu.NORM_GO, gpu.NORM_CPU])
-def test_noalloc_matches_batch_on_consecutive_calls(norm):
+def test_noalloc_matches_batch_on_consecutive_calls(oracle, norm):
     # inputs of different size and statistics back to back: a call that saw
     # the previous call's histogram, table or lane records would differ
     inputs = [W.zipf(101, MAXN), W.gen("markov", 102, 300_001), W.gen("uniform", 103, 65_537)]
@@ -53,13 +68,14 @@ def test_noalloc_matches_batch_on_consecutive_calls(norm):
         devmem.upload_to(d_in.ptr, a)
         want = _encode_batch(comp, d_in.ptr, len(a), norm, d_ref.ptr)
         assert len(g) == len(want) and g == want
+        assert g == _encode_oracle(oracle, a, norm)
     # and the same input twice in a row gives the same bytes
     devmem.upload_to(d_in.ptr, inputs[1])
     again = [_encode_noalloc(d_in.ptr, len(inputs[1]), norm, d_out.ptr, d_len.ptr) for _ in range(2)]
     assert again[0] == again[1] == got[1]
 
 
-def test_noalloc_small_and_empty_streams():
+def test_noalloc_small_and_empty_streams(oracle):
     comp = gpu.GetGlobalCompressor()
     d_in = devmem.alloc(4096)
     d_out = devmem.alloc(1024 + 2 * MAXN)
@@ -72,6 +88,24 @@ def test_noalloc_small_and_empty_streams():
         got = _encode_noalloc(d_in.ptr, n, gpu.NORM_CPU, d_out.ptr, d_len.ptr)
         want = _encode_batch(comp, d_in.ptr, n, gpu.NORM_CPU, d_ref.ptr)
         assert got == want, n
+        if n:
+            assert got == _encode_oracle(oracle, a, gpu.NORM_CPU), n
+
+
+def test_noalloc_allocates_no_device_memory():
+    # buffers first, then one call (the first call on a device may load the
+    # module), then the free device memory must not move over more calls
+    d_in = devmem.alloc(MAXN + 64)
+    d_out = devmem.alloc(1024 + 2 * MAXN)
+    d_len = devmem.alloc(16)
+    a = W.gen("markov", 301, MAXN)
+    devmem.upload_to(d_in.ptr, a)
+    first = _encode_noalloc(d_in.ptr, MAXN, gpu.NORM_GO, d_out.ptr, d_len.ptr)
+    before = _free_device_bytes()
+    for norm in (gpu.NORM_GO, gpu.NORM_CPU, gpu.NORM_GO):
+        _encode_noalloc(d_in.ptr, MAXN, norm, d_out.ptr, d_len.ptr)
+    assert _free_device_bytes() == before
+    assert _encode_noalloc(d_in.ptr, MAXN, gpu.NORM_GO, d_out.ptr, d_len.ptr) == first
 
 
 def test_noalloc_rejects_what_does_not_fit():
@@ -87,3 +121,6 @@ def test_noalloc_rejects_what_does_not_fit():
     assert _noalloc(d_buf.ptr, 10, gpu.NORM_GO, 0, 1 << 20, d_buf.ptr) == -1
     assert _noalloc(d_buf.ptr, 10, gpu.NORM_GO, d_buf.ptr, 1 << 20, 0) == -1
     assert _noalloc(0, 10, gpu.NORM_GO, d_buf.ptr, 1 << 20, d_buf.ptr) == -1
+    # the length is stored as a u32: its address must be 4-byte aligned
+    assert _noalloc(d_buf.ptr, 10, gpu.NORM_GO, d_buf.ptr, 1 << 20, d_buf.ptr + 2) == -1
+    assert b"aligned" in L.przmg_last_error()
