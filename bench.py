@@ -187,17 +187,12 @@ def measured_peaks() -> tuple[float, str]:
         return 6650.0, "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"
 
 
-def ncu_traffic() -> dict:
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
-    summary (profiles/rans_mixed256.md, line `traffic_bytes_per_MiB: X`)."""
-    path = os.path.join(ROOT, "profiles", "rans_mixed256.md")
-    try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_input_MiB:"):
-                return {"per_input_mib": float(line.split(":")[1])}
-    except OSError:
-        pass
-    return {}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per encoded
+# symbol of one k_rans launch, from an ncu capture of the same kernel on a
+# smaller batch of the same workload (its traffic grows with the symbols it
+# encodes, so it scales to a full launch by the launch's symbols).  The
+# capture and its command are summarised in profiles/k_rans_mixed16.md.
+RANS_TRAFFIC_PER_SYMBOL: float | None = None
 
 
 def gpu_local_cpus(dev: int) -> dict:
@@ -357,7 +352,28 @@ def uneven_measure(comp, count: int, sample: int) -> dict:
         e1.record(st)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / 3
-        out["batched_device"] = {"gbps": round(total / ms / 1e6, 3), "ms": round(ms, 3)}
+        out["batched_device"] = {"gbps": round(total / ms / 1e6, 3), "ms": round(ms, 3),
+                                 "launches": b.launches(), "graph": True}
+        from przm_b200 import devmem
+        fs_b = b.frame_sizes().copy()
+        probe = list(range(0, count, max(1, count // 64)))  # frames compared byte for byte
+        frames_b = [devmem.download(b.d_out + int(b.out_offs[i]), int(fs_b[i])) for i in probe]
+        # plain per-input launches of the same inputs on the same device
+        # buffers: the pipeline once per input, input after input, one stream
+        b.enqueue_plain(st.cuda_stream)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(st)
+        nl = b.enqueue_plain(st.cuda_stream)
+        p1.record(st)
+        p1.synchronize()
+        pms = p0.elapsed_time(p1)
+        fs_p = b.frame_sizes()
+        same = bool(np.array_equal(fs_b, fs_p)) and all(
+            devmem.download(b.d_out + int(b.out_offs[i]), int(fs_p[i])) == f for i, f in zip(probe, frames_b))
+        out["plain_device"] = {"gbps": round(total / pms / 1e6, 3), "ms": round(pms, 3), "launches": nl,
+                               "identical_frames": same, "compared": f"all sizes, {len(probe)} frames byte for byte"}
+        out["batched_over_plain_device"] = round(pms / ms, 2)
     finally:
         b.close()
     # the sample, through the packed host API with pinned buffers: batched =
@@ -393,6 +409,121 @@ def uneven_measure(comp, count: int, sample: int) -> dict:
     out["sample"] = {"inputs": len(sub), "bytes": sb, "api": "przmg_compress_packed, pinned host buffers",
                      "batched_e2e_gbps": round(sb / tb / 1e9, 3), "plain_e2e_gbps": round(sb / tp / 1e9, 3),
                      "batched_over_plain": round(tp / tb, 2), "identical_bytes": same}
+    return out
+
+
+def _flush_l2(buf, stream) -> None:
+    """Writes a buffer larger than the 126 MB L2 on `stream` (between timed
+    iterations of workloads that fit in L2)."""
+    import torch
+    with torch.cuda.stream(stream):
+        buf.add_(1)
+
+
+def config0_measure(comp, reps: int = 20) -> dict:
+    """One 4 MiB order-1 Markov frame with ~30% copies (the reference's
+    CPU-runnable configuration): the whole pipeline as one frame, device
+    time per frame (graph replay, L2 flushed before every timed replay),
+    and end to end through the one-input API (przmg_compress, host buffers)."""
+    import numpy as np
+    import torch
+    from oracle import oracle as O
+    from przm_b200 import gpu
+    from przm_b200 import workloads as W
+    a = W.config0()
+    n = len(a)
+    b = gpu.DeviceBatch(comp, [n], gpu.PROFILE_ANS)
+    try:
+        b.upload(a)
+        st = torch.cuda.Stream()
+        flush = torch.zeros(64 << 20, dtype=torch.int32, device="cuda")  # 256 MB
+        for _ in range(3):
+            b.enqueue(st.cuda_stream, graph=True)
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(reps):
+            _flush_l2(flush, st)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            b.enqueue(st.cuda_stream, graph=True)
+            e1.record(st)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms = sorted(times)[len(times) // 2]
+        stats = b.stats()
+        stages = b.stage_times()
+        del flush
+    finally:
+        b.close()
+    fr, prof = comp.Compress(a, gpu.PROFILE_ANS)  # warm the one-input buffers
+    e2e = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        fr, prof = comp.Compress(a, gpu.PROFILE_ANS)
+        e2e.append(time.perf_counter() - t0)
+    ok = fr == O.compress_p1(a) and (not O.ref_decoder_available() or O.ref_decompress(fr, n) == a.tobytes())
+    peak, _ = measured_peaks()
+    alg = n + len(fr)
+    return {"workload": "c0: one 4 MiB order-1 Markov frame (64-symbol alphabet, Dirichlet(0.3) rows, 30% copies)",
+            "gbps": round(n / ms / 1e6, 3), "ms": round(ms, 3), "frame_bytes": len(fr),
+            "ratio": round(len(fr) / n, 4), "stage_ms": {k: round(v, 3) for k, v in stages.items()},
+            "pipeline_roofline": {"alg_bytes": alg, "achieved_gbs": round(alg / ms / 1e6, 2),
+                                  "frac_of_hbm": round(alg / ms / 1e6 / peak, 5)},
+            "longest_lane_rounds": (int(stats["literal_bytes"]) + 3) // 4,
+            "e2e_gbps": round(n / sorted(e2e)[2] / 1e9, 3), "e2e_api": "przmg_compress (pageable host buffers)",
+            "l2": "256 MB written between timed replays", "verified": bool(ok)}
+
+
+def config1_measure(comp, reps: int = 10) -> dict:
+    """Histogram + normalisation + V-ANS in isolation: 64 Mi Zipf(1.1)
+    symbols as 64 streams of 1 MiB, through przmg_vans_encode_batch with
+    each normaliser (NormalizeFreq, flag 0x01; NormalizeFrequencies, flag
+    0x00).  Device time per call (L2 flushed before each), algorithmic bytes
+    = symbols read + containers written."""
+    import numpy as np
+    import torch
+    from oracle import oracle as O
+    from przm_b200 import devmem, gpu
+    from przm_b200 import workloads as W
+    streams = W.config1()
+    n = len(streams[0])
+    cnt = len(streams)
+    d_in = devmem.upload(np.concatenate(streams + [np.zeros(64, np.uint8)]))
+    cap = 1024 + 2 * n
+    d_out = devmem.alloc(cnt * cap)
+    in_offs = [i * n for i in range(cnt)]
+    out_offs = [i * cap for i in range(cnt)]
+    st = torch.cuda.Stream()
+    flush = torch.zeros(64 << 20, dtype=torch.int32, device="cuda")
+    peak, _ = measured_peaks()
+    out = {"workload": "c1: 64 x 1 MiB Zipf(1.1) streams over 256 symbols, histogram + normalise + V-ANS",
+           "l2": "256 MB written before every timed call"}
+    try:
+        for name, norm in (("normalize_freq_go", gpu.NORM_GO), ("normalize_frequencies", gpu.NORM_CPU)):
+            for _ in range(2):
+                ol = comp.VANSEncodeBatch(d_in.ptr, in_offs, [n] * cnt, norm, d_out.ptr, out_offs, st.cuda_stream)
+            torch.cuda.synchronize()
+            times = []
+            for _ in range(reps):
+                _flush_l2(flush, st)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                ol = comp.VANSEncodeBatch(d_in.ptr, in_offs, [n] * cnt, norm, d_out.ptr, out_offs, st.cuda_stream)
+                e1.record(st)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+            ms = sorted(times)[len(times) // 2]
+            outb = int(np.sum(ol))
+            first = devmem.download(d_out.ptr, int(ol[0]))
+            want = O.vans_encode_host(streams[0]) if norm == gpu.NORM_GO else O.adaptive_vans(streams[0])
+            alg = cnt * n + outb
+            out[name] = {"gbps": round(cnt * n / ms / 1e6, 3), "ms": round(ms, 3), "container_bytes": outb,
+                         "alg_bytes": alg, "achieved_gbs": round(alg / ms / 1e6, 2),
+                         "frac_of_hbm": round(alg / ms / 1e6 / peak, 5), "first_stream_matches_oracle": first == want}
+    finally:
+        del flush
+        d_in.free()
+        d_out.free()
     return out
 
 
@@ -446,6 +577,8 @@ def main() -> None:
                     help="sections of the Section 3 distance-coding measurement (0: skip)")
     ap.add_argument("--section4-streams", type=int, default=64,
                     help="literal streams of the Section 4 selection measurement (0: skip)")
+    ap.add_argument("--no-configs01", dest="configs01", action="store_false",
+                    help="skip the one-frame 4 MiB and the histogram + V-ANS (64 x 1 MiB Zipf) legs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -626,7 +759,18 @@ def main() -> None:
         bt.close()
     batches = batches[:1]
     # single-GPU runs only (under torchrun the other ranks would wait for them)
-    serve = serve_measure(comp, args.serve_requests) if args.serve_requests > 0 and world == 1 else None
+    serve = (serve_measure(comp, args.serve_requests, fractions=(0.1, 0.25, 0.5, 0.75, 0.9, 1.0, 1.2))
+             if args.serve_requests > 0 and world == 1 else None)
+    c0 = c1 = None
+    if args.configs01 and world == 1:
+        try:
+            c0 = config0_measure(comp)
+        except Exception as e:  # an extra leg never costs the bench line
+            c0 = {"error": f"{type(e).__name__}: {e}"[:300]}
+        try:
+            c1 = config1_measure(comp)
+        except Exception as e:
+            c1 = {"error": f"{type(e).__name__}: {e}"[:300]}
     uneven = (uneven_measure(comp, args.uneven_inputs, args.uneven_sample)
               if args.uneven_inputs > 0 and world == 1 else None)
     section3 = None
@@ -654,8 +798,8 @@ def main() -> None:
         "assemble": stats["frame_bytes"] + stats["rans_emitted_bytes"] + stats["input_bytes"] // 64,
     }.get(dom, stats["input_bytes"] + stats["frame_bytes"])
     achieved = alg / (stages[dom] / 1e3) / 1e9
-    tr = ncu_traffic()
-    traffic = tr["per_input_mib"] * stats["input_bytes"] / (1 << 20) if tr and dom == "rans" else None
+    traffic = (RANS_TRAFFIC_PER_SYMBOL * stats["rans_symbols"]
+               if RANS_TRAFFIC_PER_SYMBOL is not None and dom == "rans" else None)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 5), "peak_source": peak_kind,
                 "traffic": traffic, "algorithmic_bytes_per_launch": int(alg),
@@ -705,6 +849,7 @@ def main() -> None:
             "roofline": roofline, "pipeline_roofline": pipeline, "stage_ms": {k: round(v, 3) for k, v in stages.items()},
             "cpu_baseline": cpu_base, "plain_per_frame": plain, "clocks": clk, "gpu_launches": gl,
             "serving": serve, "uneven_batch": uneven, "section3": section3, "section4": section4,
+            "config0_one_frame": c0, "config1_hist_vans": c1,
         }
         print(json.dumps(line), flush=True)
     for bt in batches:

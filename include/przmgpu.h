@@ -209,6 +209,13 @@ int32_t przmg_batch_enqueue(przmg_batch* b, uint64_t stream, int32_t use_graph);
 int32_t przmg_batch_sizes(przmg_batch* b, uint32_t* sizes);
 /* kernels a single enqueue launches (for launch accounting) */
 int32_t przmg_batch_launch_count(przmg_batch* b);
+/* Plain per-input launches of the same batch: the pipeline enqueued once per
+ * input, input after input on `stream`, each launch sized for that input
+ * alone -- what a caller of the reference's one-input API gets
+ * (gpu/bridge.go:2486-2544 compresses one input per call).  The frames are
+ * byte-identical to przmg_batch_enqueue's; *launches (optional) = kernels
+ * launched.  For comparisons of batched against plain launches. */
+int32_t przmg_batch_enqueue_plain(przmg_batch* b, uint64_t stream, int32_t* launches);
 /* copy back-to-back host inputs (sum of the sizes, pinned for full PCIe
  * speed) into the batch's inputs, asynchronously on `stream` */
 int32_t przmg_batch_upload(przmg_batch* b, const uint8_t* host, uint64_t stream);

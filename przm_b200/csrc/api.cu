@@ -127,6 +127,10 @@ struct przmg_batch {
     DevBuf d_rtiles, d_rx_cnt, d_rx_parts, d_rx_ent, d_rx_key, d_rx_pred, d_stage_in, d_stage_out, d_stage_offs, d_up_offs;
     DevBuf d_tile_sched;  // tokenizer tile weights [0, ntiles) and walk order [ntiles, 2 ntiles)
     DevBuf d_asm;         // assembly work items (frame, part)
+    DevBuf d_asm_job;     // the same items grouped by input (plain per-input launches)
+    // per input i, where its items start in each work list ([i + 1] = end)
+    std::vector<uint32_t> job_small0, job_rt0, job_big0, job_tile0, job_asm0;
+    int launches_plain = 0;
     HostBuf h_offs;
     std::vector<RxTile> rtiles;
     uint64_t max_big_cand = 0;  // most radix candidates of one frame
@@ -147,7 +151,7 @@ struct przmg_batch {
         DevBuf* all[] = {&d_in, &d_jobs, &d_small, &d_big, &d_tiles, &d_desc, &d_slots, &d_tile_lens, &d_streams,
                          &d_job_lens, &d_hist, &d_tabs, &d_infos, &d_ans, &d_outs, &d_plans, &d_sizes, &d_out, &d_misc,
                          &d_lists, &d_rtiles, &d_rx_cnt, &d_rx_parts, &d_rx_ent, &d_rx_key, &d_rx_pred, &d_stage_in,
-                         &d_stage_out, &d_stage_offs, &d_up_offs, &d_tile_sched, &d_asm};
+                         &d_stage_out, &d_stage_offs, &d_up_offs, &d_tile_sched, &d_asm, &d_asm_job};
         for (DevBuf* b : all) b->release();
         h_offs.release();
     }
@@ -205,7 +209,12 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     b->out_offs.assign(njobs, 0);
     uint64_t in = 0, desc = 0, str = 0, ans = 0, out = 0;
     uint32_t tile0 = 0;
+    for (auto* v : {&b->job_small0, &b->job_rt0, &b->job_big0, &b->job_tile0, &b->job_asm0}) v->assign(njobs + 1, 0);
     for (uint32_t i = 0; i < njobs; i++) {
+        b->job_small0[i] = (uint32_t)b->small.size();
+        b->job_rt0[i] = (uint32_t)b->rtiles.size();
+        b->job_big0[i] = (uint32_t)b->big.size();
+        b->job_tile0[i] = (uint32_t)b->tiles.size();
         Job& j = b->jobs[i];
         const uint64_t n = sizes[i];
         if (n >= (1ull << 32) - 4096) return fail(PRZMG_ERR_EXCEEDS_MAX_BLOCK, "input too large for one frame");
@@ -247,11 +256,23 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     b->ntiles = tile0;
     b->nsmall = (uint32_t)b->small.size();
     b->nbig = (uint32_t)b->big.size();
+    b->job_small0[njobs] = b->nsmall;
+    b->job_rt0[njobs] = (uint32_t)b->rtiles.size();
+    b->job_big0[njobs] = b->nbig;
+    b->job_tile0[njobs] = (uint32_t)b->tiles.size();
     b->in_bytes = in + 64;
     b->asm_items.clear();
     for (uint32_t i = 0; i < njobs; i++) b->asm_items.push_back(make_uint2(i, 0));
     for (uint32_t i = 0; i < njobs; i++)
         for (uint32_t k = 0, np = asm_lit_parts(b->jobs[i]); k < np; k++) b->asm_items.push_back(make_uint2(i, k + 1));
+    // the same items grouped by input, for per-input launches
+    std::vector<uint2> asm_job;
+    asm_job.reserve(b->asm_items.size());
+    for (uint32_t i = 0; i < njobs; i++) {
+        b->job_asm0[i] = (uint32_t)asm_job.size();
+        for (uint32_t k = 0, np = asm_lit_parts(b->jobs[i]); k <= np; k++) asm_job.push_back(make_uint2(i, k));
+    }
+    b->job_asm0[njobs] = (uint32_t)asm_job.size();
     b->desc_words = desc + 16;
     b->stream_bytes = str + 64;
     b->ans_bytes = ans + 64;
@@ -263,6 +284,7 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     CK(b->d_tiles.ensure(sizeof(TokTile) * std::max<size_t>(b->tiles.size(), 1)));
     CK(b->d_tile_sched.ensure(2 * sizeof(uint32_t) * std::max<size_t>(b->tiles.size(), 1)));
     CK(b->d_asm.ensure(sizeof(uint2) * std::max<size_t>(b->asm_items.size(), 1)));
+    CK(b->d_asm_job.ensure(sizeof(uint2) * std::max<size_t>(asm_job.size(), 1)));
     CK(b->d_desc.ensure(b->desc_words * 4));
     CK(b->d_slots.ensure((size_t)b->ntiles * kSlotStride));
     CK(b->d_tile_lens.ensure((size_t)b->ntiles * S_COUNT * 4));
@@ -300,6 +322,8 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
         CK(cudaMemcpyAsync(b->d_tiles.p, b->tiles.data(), sizeof(TokTile) * b->tiles.size(), cudaMemcpyHostToDevice, s));
     if (!b->asm_items.empty())
         CK(cudaMemcpyAsync(b->d_asm.p, b->asm_items.data(), sizeof(uint2) * b->asm_items.size(), cudaMemcpyHostToDevice, s));
+    if (!asm_job.empty())
+        CK(cudaMemcpyAsync(b->d_asm_job.p, asm_job.data(), sizeof(uint2) * asm_job.size(), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(b->d_sizes.p, 0, (size_t)njobs * 4 + 16, s));
     CK(cudaMemsetAsync(b->d_job_lens.p, 0, (size_t)njobs * S_COUNT * 4 + 16, s));
     // the host-side vectors above must stay alive until the copies ran
@@ -313,69 +337,117 @@ static const char* const kStageNames[] = {"tile_find", "radix_find", "tokenize",
                                           "normalize", "rans", "plan", "assemble"};
 constexpr int kStages = 8;
 
+// The part of a batch one launch sequence covers: inputs [j0, j0 + nj) and
+// the matching runs of the batch's work lists (every list is ordered by
+// input, so one input's items are contiguous).
+struct Range {
+    uint32_t j0, nj;
+    uint32_t small0, nsmall;  // tile-finder tiles
+    uint32_t rt0, nrt;        // radix tiles
+    uint32_t big0, nbig;      // radix frames
+    uint32_t tile0, nt;       // tokenizer tiles
+    uint32_t asm0, nasm;      // assembly items (of d_asm, or of d_asm_job for one input)
+    const uint2* asm_list;
+    uint32_t maxtiles;
+    uint64_t max_big_cand;
+};
+
+static Range whole_range(const przmg_batch* b) {
+    Range r{};
+    r.j0 = 0;
+    r.nj = b->njobs;
+    r.nsmall = b->nsmall;
+    r.nrt = (uint32_t)b->rtiles.size();
+    r.nbig = b->nbig;
+    r.nt = (uint32_t)b->tiles.size();
+    r.nasm = (uint32_t)b->asm_items.size();
+    r.asm_list = b->d_asm.as<uint2>();
+    r.maxtiles = 1;
+    for (const Job& j : b->jobs) r.maxtiles = std::max(r.maxtiles, j.ntiles);
+    r.max_big_cand = b->max_big_cand;
+    return r;
+}
+
+static Range job_range(const przmg_batch* b, uint32_t i) {
+    Range r{};
+    r.j0 = i;
+    r.nj = 1;
+    r.small0 = b->job_small0[i];
+    r.nsmall = b->job_small0[i + 1] - r.small0;
+    r.rt0 = b->job_rt0[i];
+    r.nrt = b->job_rt0[i + 1] - r.rt0;
+    r.big0 = b->job_big0[i];
+    r.nbig = b->job_big0[i + 1] - r.big0;
+    r.tile0 = b->job_tile0[i];
+    r.nt = b->job_tile0[i + 1] - r.tile0;
+    r.asm0 = b->job_asm0[i];
+    r.nasm = b->job_asm0[i + 1] - r.asm0;
+    r.asm_list = b->d_asm_job.as<uint2>();
+    r.maxtiles = std::max<uint32_t>(1, b->jobs[i].ntiles);
+    r.max_big_cand = rx_ncand(b->jobs[i].n);
+    return r;
+}
+
 // ev (optional): kStages + 1 events; ev[0] before the first kernel and
 // ev[k + 1] after stage k (stages that do not run record back to back).
 // skip_match: the match table is already in d_desc (tokenizer-only runs).
-static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cudaEvent_t* ev = nullptr,
-                            bool skip_match = false) {
+static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, const Range& R, cudaEvent_t* ev,
+                            bool skip_match, int& launches) {
     Ctx* c = b->ctx;
-    int launches = 0;
-    CK(cudaMemsetAsync(b->d_misc.p, 0, 16, s));
     auto mark = [&](int k) -> cudaError_t { return ev ? cudaEventRecord(ev[k], s) : cudaSuccess; };
     CK(mark(0));
-    if (b->nsmall && !skip_match) {
-        const uint32_t grid = std::min<uint32_t>(b->nsmall, 8u * c->sms);
-        k_tile_find<<<grid, 256, kTileFindSmem, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_small.as<TileRef>(),
-                                                     b->nsmall, b->d_desc.as<uint32_t>());
+    if (R.nsmall && !skip_match) {
+        const uint32_t grid = std::min<uint32_t>(R.nsmall, 8u * c->sms);
+        k_tile_find<<<grid, 256, kTileFindSmem, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(),
+                                                     b->d_small.as<TileRef>() + R.small0, R.nsmall,
+                                                     b->d_desc.as<uint32_t>());
         CK(cudaGetLastError());
         launches++;
     }
     CK(mark(1));
-    if (b->nbig && !b->rtiles.empty() && !skip_match) {
-        const uint32_t nrt = (uint32_t)b->rtiles.size();
-        const uint32_t gt = std::min<uint32_t>(nrt, 16u * c->sms);
-        k_rx_count<<<gt, 256, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_rtiles.as<RxTile>(), nrt,
-                                      b->d_rx_cnt.as<uint32_t>());
+    if (R.nbig && R.nrt && !skip_match) {
+        const uint32_t gt = std::min<uint32_t>(R.nrt, 16u * c->sms);
+        const RxTile* rt = b->d_rtiles.as<RxTile>() + R.rt0;
+        const uint32_t* big = b->d_big.as<uint32_t>() + R.big0;
+        k_rx_count<<<gt, 256, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), rt, R.nrt, b->d_rx_cnt.as<uint32_t>());
         CK(cudaGetLastError());
-        k_rx_scan<<<std::min<uint32_t>(b->nbig, 16u * c->sms), kRxParts, 0, s>>>(
-            b->d_jobs.as<Job>(), b->d_big.as<uint32_t>(), b->nbig, b->d_rx_cnt.as<uint32_t>(), b->d_rx_parts.as<uint2>());
+        k_rx_scan<<<std::min<uint32_t>(R.nbig, 16u * c->sms), kRxParts, 0, s>>>(
+            b->d_jobs.as<Job>(), big, R.nbig, b->d_rx_cnt.as<uint32_t>(), b->d_rx_parts.as<uint2>());
         CK(cudaGetLastError());
-        k_rx_scatter<<<gt, 256, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_rtiles.as<RxTile>(), nrt,
-                                        b->d_rx_cnt.as<uint32_t>(), b->d_rx_ent.as<uint32_t>(),
-                                        b->d_rx_key.as<uint16_t>());
+        k_rx_scatter<<<gt, 256, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), rt, R.nrt, b->d_rx_cnt.as<uint32_t>(),
+                                        b->d_rx_ent.as<uint32_t>(), b->d_rx_key.as<uint16_t>());
         CK(cudaGetLastError());
-        const uint32_t nwarps = b->nbig * kRxParts;
+        const uint32_t nwarps = R.nbig * kRxParts;
         const uint32_t gr = std::min<uint32_t>((nwarps + kRxResolveWarps - 1) / kRxResolveWarps, 4u * c->sms);
         k_rx_resolve<<<gr, kRxResolveWarps * 32, kRxResolveSmem, s>>>(
-            b->d_jobs.as<Job>(), b->d_big.as<uint32_t>(), b->nbig, b->d_rx_parts.as<uint2>(), b->d_rx_ent.as<uint32_t>(),
+            b->d_jobs.as<Job>(), big, R.nbig, b->d_rx_parts.as<uint2>(), b->d_rx_ent.as<uint32_t>(),
             b->d_rx_key.as<uint16_t>(), b->d_rx_pred.as<uint32_t>());
         CK(cudaGetLastError());
-        const uint32_t vx = std::max<uint32_t>(1, std::min<uint32_t>(64u, (uint32_t)((b->max_big_cand + 255) / 256)));
-        k_rx_verify<<<dim3(vx, std::min<uint32_t>(b->nbig, 65535u)), 256, 0, s>>>(
-            b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_big.as<uint32_t>(), b->d_rx_ent.as<uint32_t>(),
-            b->d_rx_pred.as<uint32_t>(), b->nbig, b->d_desc.as<uint32_t>());
+        const uint32_t vx = std::max<uint32_t>(1, std::min<uint32_t>(64u, (uint32_t)((R.max_big_cand + 255) / 256)));
+        k_rx_verify<<<dim3(vx, std::min<uint32_t>(R.nbig, 65535u)), 256, 0, s>>>(
+            b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), big, b->d_rx_ent.as<uint32_t>(), b->d_rx_pred.as<uint32_t>(),
+            R.nbig, b->d_desc.as<uint32_t>());
         CK(cudaGetLastError());
         launches += 5;
     }
     CK(mark(2));
-    if (stop_after >= 1 && !b->tiles.empty()) {
-        const uint32_t nt = (uint32_t)b->tiles.size();
-        uint32_t* tile_w = b->d_tile_sched.as<uint32_t>();
-        uint32_t* tile_order = tile_w + nt;
-        k_tile_weight<<<std::min<uint32_t>(nt, 16u * c->sms), 256, 0, s>>>(b->d_jobs.as<Job>(), b->d_tiles.as<TokTile>(), nt,
+    if (stop_after >= 1 && R.nt) {
+        const uint32_t nt = R.nt;
+        uint32_t* tile_w = b->d_tile_sched.as<uint32_t>() + R.tile0;
+        uint32_t* tile_order = b->d_tile_sched.as<uint32_t>() + b->tiles.size() + R.tile0;
+        const TokTile* tiles = b->d_tiles.as<TokTile>() + R.tile0;
+        k_tile_weight<<<std::min<uint32_t>(nt, 16u * c->sms), 256, 0, s>>>(b->d_jobs.as<Job>(), tiles, nt,
                                                                           b->d_desc.as<uint32_t>(), tile_w);
         CK(cudaGetLastError());
         k_tile_order<<<1, 1024, 0, s>>>(tile_w, nt, tile_order);
         CK(cudaGetLastError());
-        k_tokenize<<<(nt + kTokWarps - 1) / kTokWarps, kTokWarps * 32, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_tiles.as<TokTile>(), nt,
-                                               tile_order, b->d_desc.as<uint32_t>(), b->d_slots.as<uint8_t>(),
-                                               b->d_tile_lens.as<uint32_t>(), b->err_word());
+        k_tokenize<<<(nt + kTokWarps - 1) / kTokWarps, kTokWarps * 32, 0, s>>>(
+            b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), tiles, nt, tile_order, b->d_desc.as<uint32_t>(),
+            b->d_slots.as<uint8_t>(), b->d_tile_lens.as<uint32_t>(), b->err_word());
         CK(cudaGetLastError());
         CK(mark(3));
-        uint32_t maxtiles = 1;
-        for (const Job& j : b->jobs) maxtiles = std::max(maxtiles, j.ntiles);
-        k_gather<<<std::min<uint32_t>(b->njobs, 16u * c->sms), kGatherThreads, (maxtiles + 1) * 4, s>>>(
-            b->d_jobs.as<Job>(), b->njobs, b->d_slots.as<uint8_t>(), b->d_tile_lens.as<uint32_t>(),
+        k_gather<<<std::min<uint32_t>(R.nj, 16u * c->sms), kGatherThreads, (R.maxtiles + 1) * 4, s>>>(
+            b->d_jobs.as<Job>(), R.j0, R.nj, b->d_slots.as<uint8_t>(), b->d_tile_lens.as<uint32_t>(),
             b->d_streams.as<uint8_t>(), b->d_job_lens.as<uint32_t>(), b->d_hist.as<uint32_t>(), b->err_word());
         CK(cudaGetLastError());
         launches += 4;
@@ -383,20 +455,20 @@ static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cuda
         CK(mark(3));
     }
     CK(mark(4));
-    if (stop_after >= 2) {
+    if (stop_after >= 2 && R.nj) {
         if (b->profile == 1) {
-            k_normalize<<<b->njobs, 128, 0, s>>>(b->d_jobs.as<Job>(), b->njobs, b->d_job_lens.as<uint32_t>(),
-                                                 b->d_hist.as<uint32_t>(), b->d_tabs.as<EncSym>(), b->d_infos.as<TableInfo>());
+            k_normalize<<<R.nj, 128, 0, s>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_job_lens.as<uint32_t>(),
+                                             b->d_hist.as<uint32_t>(), b->d_tabs.as<EncSym>(), b->d_infos.as<TableInfo>());
             CK(cudaGetLastError());
             CK(mark(5));
             const uint32_t list_cap = 4 * b->njobs;
             uint32_t* lists = b->d_lists.as<uint32_t>();
             uint32_t* counts = lists + 2 * list_cap;
-            k_task_list<<<1, 1024, 0, s>>>(b->d_jobs.as<Job>(), b->njobs, b->d_job_lens.as<uint32_t>(), lists, list_cap,
-                                           counts);
+            k_task_list<<<1, 1024, 0, s>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_job_lens.as<uint32_t>(), lists,
+                                           list_cap, counts);
             CK(cudaGetLastError());
-            const uint32_t nb_ad = (4 * b->njobs + 8 * kRansWarps - 1) / (8 * kRansWarps);
-            const uint32_t nb_m8 = (3 * b->njobs + 8 * kRansWarps - 1) / (8 * kRansWarps);
+            const uint32_t nb_ad = (4 * R.nj + 8 * kRansWarps - 1) / (8 * kRansWarps);
+            const uint32_t nb_m8 = (3 * R.nj + 8 * kRansWarps - 1) / (8 * kRansWarps);
             k_rans<<<nb_ad + nb_m8, kRansWarps * 32, kRansSmem, s>>>(
                 b->d_jobs.as<Job>(), b->d_job_lens.as<uint32_t>(), b->d_streams.as<uint8_t>(), b->d_ans.as<uint8_t>(),
                 b->d_tabs.as<EncSym>(), c->d_meta8.as<EncSym>(), c->d_ctxlut.as<uint8_t>(), lists, list_cap, counts, nb_ad,
@@ -408,24 +480,46 @@ static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cuda
             CK(mark(5));
             CK(mark(6));
         }
-        k_plan<<<(b->njobs + 127) / 128, 128, 0, s>>>(b->d_jobs.as<Job>(), b->njobs, b->d_job_lens.as<uint32_t>(),
-                                                      b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(),
-                                                      b->d_streams.as<uint8_t>(), b->d_plans.as<Plan>(),
-                                                      b->d_sizes.as<uint32_t>());
+        k_plan<<<(R.nj + 127) / 128, 128, 0, s>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_job_lens.as<uint32_t>(),
+                                                  b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(),
+                                                  b->d_streams.as<uint8_t>(), b->d_plans.as<Plan>(),
+                                                  b->d_sizes.as<uint32_t>());
         CK(cudaGetLastError());
         CK(mark(7));
-        const uint32_t nitems = (uint32_t)b->asm_items.size();
-        k_assemble<<<std::max<uint32_t>(1, std::min<uint32_t>(nitems, 1u << 20)), kAsmThreads, 0, s>>>(
-            b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), b->d_asm.as<uint2>(), nitems, b->d_job_lens.as<uint32_t>(), b->d_plans.as<Plan>(),
-            b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(), b->d_streams.as<uint8_t>(), b->d_ans.as<uint8_t>(),
-            b->d_out.as<uint8_t>());
+        k_assemble<<<std::max<uint32_t>(1, std::min<uint32_t>(R.nasm, 1u << 20)), kAsmThreads, 0, s>>>(
+            b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), R.asm_list + R.asm0, R.nasm, b->d_job_lens.as<uint32_t>(),
+            b->d_plans.as<Plan>(), b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(), b->d_streams.as<uint8_t>(),
+            b->d_ans.as<uint8_t>(), b->d_out.as<uint8_t>());
         CK(cudaGetLastError());
         launches += 2;
         CK(mark(8));
     } else {
         for (int k = 5; k <= 8; k++) CK(mark(k));
     }
+    return PRZMG_OK;
+}
+
+// The whole batch as one launch sequence.
+static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cudaEvent_t* ev = nullptr,
+                            bool skip_match = false) {
+    CK(cudaMemsetAsync(b->d_misc.p, 0, 16, s));
+    int launches = 0;
+    int32_t r = launch_range(b, s, stop_after, whole_range(b), ev, skip_match, launches);
     b->launches = launches;
+    return r;
+}
+
+// Plain per-input launches: the same pipeline once per input, one input
+// after another on one stream (what a caller without batching does).
+static int32_t batch_launch_plain(przmg_batch* b, cudaStream_t s) {
+    CK(cudaMemsetAsync(b->d_misc.p, 0, 16, s));
+    int launches = 0;
+    for (uint32_t i = 0; i < b->njobs; i++) {
+        if (b->jobs[i].n == 0) continue;
+        int32_t r = launch_range(b, s, 2, job_range(b, i), nullptr, false, launches);
+        if (r) return r;
+    }
+    b->launches_plain = launches;
     return PRZMG_OK;
 }
 
@@ -1069,6 +1163,15 @@ extern "C" int32_t przmg_batch_sizes(przmg_batch* b, uint32_t* sizes) {
 }
 
 extern "C" int32_t przmg_batch_launch_count(przmg_batch* b) { return b ? b->launches : 0; }
+
+extern "C" int32_t przmg_batch_enqueue_plain(przmg_batch* b, uint64_t stream, int32_t* launches) {
+    if (!b) return fail(PRZMG_ERR_INVALID_ARG, "null batch");
+    Ctx* c = b->ctx;
+    LOCKED(c);
+    int32_t r = batch_launch_plain(b, stream ? (cudaStream_t)(uintptr_t)stream : c->stream);
+    if (launches) *launches = b->launches_plain;
+    return r;
+}
 
 // Scatter of back-to-back inputs into the padded per-frame layout, and the
 // inverse gather of the frames into back-to-back output.

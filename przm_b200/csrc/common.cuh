@@ -97,17 +97,26 @@ __host__ __device__ inline uint64_t ans_task_off(const Job& j, int t) {
 }
 __host__ __device__ inline uint64_t ans_region_bytes(const Job& j) { return ans_task_off(j, T_COUNT); }
 
-// Encoding table entry for one symbol of one model:
-//   m   : 32-bit reciprocal so that floor(x_r / f) == umulhi(x_r, m) >> s for
-//         every x_r < 2^24 (Granlund-Montgomery 1994, round-up variant);
-//         f = 2^t uses m = 2^(32-t), s = 0; f = 1 uses m = 2^32-1 (one short)
-//         with the deficit folded into cb.
-//   t1  : 4096 * f, the renormalisation bound (x >= t1 -> emit a byte)
-//   t2  : 256 * t1 saturated to 2^32-1 (x >= t2 -> emit a second byte)
-//   w   : cb | (4096 - f) << 13 | s << 25, cb = cumulative frequency c
-//         (+4095 when f == 1)
+// Encoding table entry for one symbol of one model (frequency f, cumulative
+// frequency c).  The reference step on a state 2^16 <= x < 2^24 emits the
+// low byte of x while x >= 4096 f, then sets x = floor(x_r / f) * 4096 + c +
+// (x_r mod f) for the remaining x_r = x >> 8k.  k takes only two values per
+// symbol: 0 or 1 when f >= 16 (x < 2^24 <= 2^20 f), 1 or 2 when f < 16
+// (x >= 2^16 > 4096 f).  So k = kb + p with kb = (f < 16) and p = (x >= t),
+// and with d = f << 8 kb a single multiply-high gives both quotients:
+// floor(x / d) = umulhi(x, m) >> s exactly for every x < 2^24
+// (Granlund-Montgomery 1994 with s = max(0, ceil(log2 d) - 8)), and
+// floor(x / 256 d) = floor(x / d) >> 8.  The step is then
+//   x' = (umulhi(x, m) >> (s + 8p)) * (4096 - f) + (x >> (8 kb + 8p)) + c,
+// whose chain is compare | multiply-high -> shift -> multiply-add.
+//   m   : ceil(2^(32+s) / d)
+//   t   : 4096 f (f >= 16) or 2^20 f (f < 16): x >= t -> one more byte;
+//         2^32 - 1 for f = 4096 (never)
+//   cc  : c | (4096 - f) << 16
+//   sh  : s | (s + 8) << 8 | 8 kb << 16 | (8 kb + 8) << 24
+// f = 0 (a symbol that never occurs) gets t = 2^32 - 1 and zeros.
 struct __align__(16) EncSym {
-    uint32_t m, t1, t2, w;
+    uint32_t m, t, cc, sh;
 };
 
 // Per-task results of the rANS kernel.

@@ -6,26 +6,27 @@
 namespace pz {
 
 // ---------------------------------------------------------------------------
-// Encoding tables.  The step x' = x + bias + floor(x / f) * (M - f) with the
-// quotient from a multiply-high by a per-symbol reciprocal, and the f = 1
-// case done as a one-short reciprocal with the deficit moved into the bias,
-// is the reciprocal-encoder form of rANS that F. Giesen published with
-// ryg_rans (rans_byte.h, RansEncSymbolInit / RansEncPutSymbol, 2014); the
-// reciprocal itself is Granlund-Montgomery's (PLDI 1994).
+// Encoding tables.  The step x' = x_r + c + floor(x_r / f) * (M - f) with the
+// quotient from a multiply-high by a per-symbol reciprocal is the
+// reciprocal-encoder form of rANS that F. Giesen published with ryg_rans
+// (rans_byte.h, RansEncSymbolInit / RansEncPutSymbol, 2014); the reciprocal
+// is Granlund-Montgomery's (PLDI 1994).  Here the divisor folds in the
+// renormalisation shift (see EncSym), so one reciprocal serves both byte
+// counts a symbol can emit.
 // ---------------------------------------------------------------------------
 __host__ __device__ inline EncSym make_encsym(uint32_t f, uint32_t c) {
     EncSym e;
-    if (f == 0) { e.m = 0; e.t1 = 0xFFFFFFFFu; e.t2 = 0xFFFFFFFFu; e.w = 0; return e; }
-    uint32_t s = 0;
-    while ((2u << s) <= f) s++;  // floor(log2 f)
-    uint32_t cb = c;
-    if (f == 1) { e.m = 0xFFFFFFFFu; s = 0; cb = c + 4095; }
-    else if ((f & (f - 1)) == 0) { e.m = 1u << (32 - s); s = 0; }
-    else e.m = (uint32_t)(((1ull << (32 + s)) + f - 1) / f);
-    e.t1 = 4096u * f;
-    const uint64_t t2 = 256ull * e.t1;
-    e.t2 = t2 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)t2;
-    e.w = cb | ((4096u - f) << 13) | (s << 25);
+    if (f == 0) { e.m = 0; e.t = 0xFFFFFFFFu; e.cc = 0; e.sh = 0; return e; }
+    const uint32_t kb = f < 16 ? 1u : 0u;
+    const uint64_t d = (uint64_t)f << (8 * kb);  // 16 <= d <= 4096
+    uint32_t lg = 0;
+    while ((1ull << lg) < d) lg++;  // ceil(log2 d)
+    const uint32_t s = lg > 8 ? lg - 8 : 0;
+    // x * (m d - 2^(32+s)) < 2^24 d <= 2^(32+s) for every x < 2^24
+    e.m = (uint32_t)(((1ull << (32 + s)) + d - 1) / d);
+    e.t = f == 4096 ? 0xFFFFFFFFu : (kb ? (f << 20) : 4096u * f);
+    e.cc = c | ((4096u - f) << 16);
+    e.sh = s | ((s + 8) << 8) | ((8 * kb) << 16) | ((8 * kb + 8) << 24);
     return e;
 }
 
@@ -302,15 +303,16 @@ __device__ void warp_build_table(const uint16_t* __restrict__ freq /* smem */, E
     }
 }
 
-// One warp per (frame, model stream): lit, op, meta, var.
-__global__ void k_normalize(const Job* __restrict__ jobs, uint32_t njobs, const uint32_t* __restrict__ job_lens,
+// One warp per (frame, model stream): lit, op, meta, var, for frames
+// [j0, j0 + njobs).
+__global__ void k_normalize(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs, const uint32_t* __restrict__ job_lens,
                             const uint32_t* __restrict__ hist, EncSym* __restrict__ tabs, TableInfo* __restrict__ infos) {
     __shared__ uint32_t s_cnt[4][256];
     __shared__ uint16_t s_freq[4][256];
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const uint32_t gw = blockIdx.x * 4 + w;
-    if (gw >= njobs * 4) return;
-    const uint32_t j = gw >> 2, si = gw & 3;
+    const uint32_t lw = blockIdx.x * 4 + w;
+    if (lw >= njobs * 4) return;
+    const uint32_t j = j0 + (lw >> 2), si = lw & 3, gw = 4 * j + si;
     (void)job_lens;
     for (uint32_t s = lane; s < 256; s += 32) s_cnt[w][s] = hist[(uint64_t)j * 1024 + si * 256 + s];
     __syncwarp();
@@ -347,22 +349,20 @@ __device__ __forceinline__ LaneIO lane_io(uint8_t* task_base, uint32_t cap, uint
 }
 
 // One rANS step (table entry e of the symbol already in registers): returns
-// the number k of low bytes of x the reference would emit (x >= 4096 f, and
-// again when x >= 2^20 f), and advances x.  The caller keeps the low 16 bits
-// of x from before the step; its first k bytes (low byte first) are what the
-// reference writes.  x < 2^24 throughout, so x >= t2 can only hold for f < 16.
-// The renormalised state is selected first and divided once: computing the
-// three candidates (0, 1 or 2 bytes shifted out) side by side and selecting
-// last keeps the compares off the multiply's chain, but its extra
-// instructions made the kernel slower (7.68 vs 7.45 ms on the 256 x 1 MiB
-// mixed batch).
+// the number k = kb + p of low bytes of x the reference would emit, and
+// advances x.  The caller keeps the low 16 bits of x from before the step;
+// its first k bytes (low byte first) are what the reference writes.  The
+// multiply-high runs on x itself, beside the compare that picks the shifts
+// (see EncSym), so the dependent chain per step is multiply-high -> shift ->
+// multiply-add.
 __device__ __forceinline__ uint32_t rans_next(uint32_t x, const EncSym& e) {
-    const uint32_t s = e.w >> 25, cf = (e.w >> 13) & 0xFFFu, cb = e.w & 0x1FFFu;
-    const uint32_t xs = x >= e.t2 ? (x >> 16) : (x >= e.t1 ? (x >> 8) : x);
-    return xs + cb + (__umulhi(xs, e.m) >> s) * cf;
+    const bool p = x >= e.t;
+    const uint32_t q = __umulhi(x, e.m) >> (p ? ((e.sh >> 8) & 0xFFu) : (e.sh & 0xFFu));
+    return q * (e.cc >> 16) + (x >> (p ? (e.sh >> 24) : ((e.sh >> 16) & 0xFFu))) + (e.cc & 0xFFFFu);
 }
+__device__ __forceinline__ uint32_t enc_kb(const EncSym& e) { return (e.sh >> 19) & 1u; }
 __device__ __forceinline__ uint32_t rans_step(uint32_t& x, const EncSym& e) {
-    const uint32_t k = (uint32_t)(x >= e.t1) + (uint32_t)(x >= e.t2);
+    const uint32_t k = enc_kb(e) + (uint32_t)(x >= e.t);
     x = rans_next(x, e);
     return k;
 }
@@ -391,17 +391,17 @@ __device__ __forceinline__ void words16(const uint4* c, uint32_t* w) {
 // registers; writes the group's records and its 2-bit count word.
 __device__ __forceinline__ void encode_group(uint32_t& x, uint32_t& cnt, const EncSym* e, int32_t g, uint4* r4,
                                              uint32_t* nbw) {
-    uint32_t rec[16], m1 = 0, m2 = 0;
+    uint32_t rec[16], mp = 0, mk = 0;
 #pragma unroll
     for (int r = 15; r >= 0; r--) {
         rec[r] = x & 0xFFFFu;
-        m1 |= x >= e[r].t1 ? (1u << r) : 0u;
-        m2 |= x >= e[r].t2 ? (1u << r) : 0u;
+        mp |= x >= e[r].t ? (1u << r) : 0u;
+        mk |= enc_kb(e[r]) << r;
         x = rans_next(x, e[r]);
     }
-    // k = p1 + p2 with p2 => p1: bit 0 = p1 ^ p2, bit 1 = p2
-    nbw[g] = spread16(m1 ^ m2) | (spread16(m2) << 1);
-    cnt += __popc(m1) + __popc(m2);
+    // k = kb + p: bit 0 = kb ^ p, bit 1 = kb & p
+    nbw[g] = spread16(mp ^ mk) | (spread16(mp & mk) << 1);
+    cnt += __popc(mp) + __popc(mk);
     r4[2 * g] = make_uint4(rec[0] | (rec[1] << 16), rec[2] | (rec[3] << 16), rec[4] | (rec[5] << 16),
                            rec[6] | (rec[7] << 16));
     r4[2 * g + 1] = make_uint4(rec[8] | (rec[9] << 16), rec[10] | (rec[11] << 16), rec[12] | (rec[13] << 16),
@@ -540,7 +540,7 @@ __host__ __device__ inline bool task_active(const Job& job, const uint32_t* lens
 // ordered longest-first (by the bit length of the symbol count) so that the
 // 8 tasks sharing a warp have similar lengths and the long chains start
 // first.  Entry = frame << 3 | task.  One block.
-__global__ void __launch_bounds__(1024) k_task_list(const Job* __restrict__ jobs, uint32_t njobs,
+__global__ void __launch_bounds__(1024) k_task_list(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs,
                                                     const uint32_t* __restrict__ job_lens, uint32_t* __restrict__ lists,
                                                     uint32_t list_cap, uint32_t* __restrict__ counts) {
     __shared__ uint32_t s_cnt[2][33];
@@ -550,7 +550,7 @@ __global__ void __launch_bounds__(1024) k_task_list(const Job* __restrict__ jobs
     __syncthreads();
     const uint32_t total = njobs * T_COUNT;
     for (uint32_t e = tid; e < total; e += blockDim.x) {
-        const uint32_t j = e / T_COUNT;
+        const uint32_t j = j0 + e / T_COUNT;
         const int t = (int)(e % T_COUNT);
         const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
         const Job job = jobs[j];
@@ -566,7 +566,7 @@ __global__ void __launch_bounds__(1024) k_task_list(const Job* __restrict__ jobs
     }
     __syncthreads();
     for (uint32_t e = tid; e < total; e += blockDim.x) {
-        const uint32_t j = e / T_COUNT;
+        const uint32_t j = j0 + e / T_COUNT;
         const int t = (int)(e % T_COUNT);
         const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
         const Job job = jobs[j];

@@ -22,11 +22,12 @@ __device__ inline uint32_t rd32b(const uint8_t* p) {
     return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
 }
 
-__global__ void k_plan(const Job* __restrict__ jobs, uint32_t njobs, const uint32_t* __restrict__ job_lens,
+__global__ void k_plan(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs, const uint32_t* __restrict__ job_lens,
                        const TableInfo* __restrict__ infos, const TaskOut* __restrict__ outs,
                        const uint8_t* __restrict__ streams, Plan* __restrict__ plans, uint32_t* __restrict__ sizes) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= njobs) return;
+    const uint32_t jl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jl >= njobs) return;
+    const uint32_t j = j0 + jl;
     const Job job = jobs[j];
     const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
     Plan p = {};

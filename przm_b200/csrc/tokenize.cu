@@ -605,7 +605,7 @@ __global__ void __launch_bounds__(1024) k_tile_order(const uint32_t* __restrict_
 // ---------------------------------------------------------------------------
 constexpr uint32_t kGatherThreads = 512;
 
-__global__ void __launch_bounds__(kGatherThreads) k_gather(const Job* __restrict__ jobs, uint32_t njobs,
+__global__ void __launch_bounds__(kGatherThreads) k_gather(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs,
                                                           const uint8_t* __restrict__ slots,
                                                           const uint32_t* __restrict__ tile_lens,
                                                           uint8_t* __restrict__ streams, uint32_t* __restrict__ job_lens,
@@ -615,7 +615,8 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather(const Job* __restrict
     uint32_t* s_off = smem_g;                      // (maxtiles + 1) per stream, filled per stream
     __shared__ uint32_t s_hist[4][4][256];         // [stream][warp group][symbol]
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
+    for (uint32_t jl = blockIdx.x; jl < njobs; jl += gridDim.x) {
+        const uint32_t j = j0 + jl;
         const Job job = jobs[j];
         uint8_t* sreg = streams + job.str_off;
         for (uint32_t i = tid; i < 4 * 4 * 256; i += kGatherThreads) (&s_hist[0][0][0])[i] = 0;

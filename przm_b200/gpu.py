@@ -595,6 +595,13 @@ class DeviceBatch:
     def enqueue(self, stream: int = 0, graph: bool = False) -> None:
         _check(L().przmg_batch_enqueue(self._h, stream, 1 if graph else 0))
 
+    def enqueue_plain(self, stream: int = 0) -> int:
+        """The pipeline once per input, input after input (plain per-input
+        launches); returns the kernels launched."""
+        n = C.c_int32()
+        _check(L().przmg_batch_enqueue_plain(self._h, stream, C.byref(n)))
+        return n.value
+
     def frame_sizes(self) -> np.ndarray:
         out = np.zeros(max(len(self.sizes), 1), np.uint32)
         _check(L().przmg_batch_sizes(self._h, _ptr(out)))

@@ -52,6 +52,33 @@ def test_device_batch_graph_replay(comp, oracle):
         b.close()
 
 
+@pytest.mark.parametrize("profile", [gpu.PROFILE_D2D, gpu.PROFILE_ANS])
+def test_plain_per_input_launches_equal_the_batched_launch(comp, oracle, profile):
+    from przm_b200 import devmem
+    xs = _uneven(30, 321)
+    sizes = [len(x) for x in xs]
+    b = gpu.DeviceBatch(comp, sizes, profile)
+    try:
+        host = np.zeros(int(b.in_offs[-1]) + max(sizes[-1], 1) + 64, np.uint8)
+        for x, o in zip(xs, b.in_offs):
+            host[int(o):int(o) + len(x)] = x
+        devmem.upload_to(b.d_in, host)
+        b.enqueue(graph=True)
+        fs = b.frame_sizes().copy()
+        batched = [devmem.download(b.d_out + int(o), int(s)) for o, s in zip(b.out_offs, fs)]
+        devmem.upload_to(b.d_out, np.zeros(int(b.out_offs[-1]) + 64, np.uint8))
+        launches = b.enqueue_plain()
+        assert launches > b.launches()  # one launch sequence per non-empty input
+        fp = b.frame_sizes()
+        assert np.array_equal(fs, fp)
+        ref = oracle.compress_p1 if profile == gpu.PROFILE_ANS else oracle.compress_p0
+        for x, o, s, want in zip(xs, b.out_offs, fp, batched):
+            got = devmem.download(b.d_out + int(o), int(s))
+            assert got == want == ref(x)
+    finally:
+        b.close()
+
+
 @pytest.mark.parametrize("norm", [gpu.NORM_GO, gpu.NORM_CPU])
 def test_vans_batch_config1_shapes(comp, oracle, norm):
     streams = W.config1(count=8, size=1 << 18)
