@@ -216,6 +216,31 @@ int32_t przmg_batch_launch_count(przmg_batch* b);
  * byte-identical to przmg_batch_enqueue's; *launches (optional) = kernels
  * launched.  For comparisons of batched against plain launches. */
 int32_t przmg_batch_enqueue_plain(przmg_batch* b, uint64_t stream, int32_t* launches);
+
+/* ---- launch geometry per size class (no reference counterpart: the
+ * reference launches fixed grids, gpu/bridge.go:924-1068) ------------------
+ * A batch belongs to size class przmg_size_class(mean input bytes): 0 up to
+ * 64 KiB, 1 up to 768 KiB, 2 up to 2 MiB, 3 above.  Per class: front = 1 runs
+ * the match finders, tokenizer and gather as ONE persistent launch whose
+ * blocks take work items (tiles, verify chunks, frames) from a device queue,
+ * front = 0 one kernel per stage; ctas_per_sm (1-3) and verify_chunk (radix
+ * candidates per work item, a multiple of 256) shape the persistent launch.
+ * The values come from the autotuner (przm_b200/autotune.py); none changes an
+ * output byte.  A batch takes its class's values when it is laid out
+ * (przmg_batch_create, or each one-input / many-input call). */
+int32_t przmg_size_class(uint64_t mean_input_bytes);
+int32_t przmg_set_tuning(przmg_ctx* ctx, int32_t size_class, int32_t front, int32_t ctas_per_sm, int32_t verify_chunk);
+int32_t przmg_get_tuning(przmg_ctx* ctx, int32_t size_class, int32_t* front, int32_t* ctas_per_sm,
+                         int32_t* verify_chunk);
+/* info[0] = 1 if the batch runs the persistent front end, [1] size class,
+ * [2] blocks per SM, [3] verify chunk */
+int32_t przmg_batch_info(przmg_batch* b, uint32_t info[4]);
+/* Every wait of the persistent front end (an item waiting for the earlier
+ * stages of its input) gives up after limit_ns (default 1 s), sets an error
+ * bit and stops the launch; the call then returns PRZMG_ERR_DEVICE and the
+ * context stays usable.  add_unreachable_wait = 1 appends to batches laid
+ * out afterwards one item whose wait never ends (for testing that path). */
+int32_t przmg_set_front_wait(przmg_ctx* ctx, uint64_t limit_ns, int32_t add_unreachable_wait);
 /* copy back-to-back host inputs (sum of the sizes, pinned for full PCIe
  * speed) into the batch's inputs, asynchronously on `stream` */
 int32_t przmg_batch_upload(przmg_batch* b, const uint8_t* host, uint64_t stream);

@@ -82,6 +82,11 @@ SIGNATURES: dict[str, tuple] = {
     "przmg_batch_sizes": (i32, [vp, vp]),
     "przmg_batch_launch_count": (i32, [vp]),
     "przmg_batch_enqueue_plain": (i32, [vp, u64, vp]),
+    "przmg_size_class": (i32, [u64]),
+    "przmg_set_tuning": (i32, [vp, i32, i32, i32, i32]),
+    "przmg_get_tuning": (i32, [vp, i32, vp, vp, vp]),
+    "przmg_batch_info": (i32, [vp, vp]),
+    "przmg_set_front_wait": (i32, [vp, u64, i32]),
     "przmg_batch_destroy": (i32, [vp]),
     "przmg_batch_upload": (i32, [vp, vp, u64]),
     "przmg_batch_download": (i32, [vp, vp, u64, vp, vp, u64]),

@@ -23,6 +23,7 @@
 #include "frame.cu"
 #include "match.cu"
 #include "tokenize.cu"
+#include "front.cu"
 #include "streams.cu"
 
 using namespace pz;
@@ -106,6 +107,23 @@ extern "C" uint64_t przmg_frame_bound(uint64_t n) { return 2 * n + (n >> 13) + 4
 // ---------------------------------------------------------------------------
 struct Ctx;
 
+// Launch geometry of one size class (mean input size of a batch), chosen by
+// the autotuner (przm_b200/autotune.py); never changes an output byte.
+//   front        0: one kernel per front-end stage, 1: the persistent front end
+//   ctas_per_sm  resident blocks per SM of the persistent front end
+//   verify_chunk radix candidates per verify item of the persistent front end
+struct Tuning {
+    uint32_t front = 0, ctas_per_sm = 2, verify_chunk = 2048;
+};
+constexpr int kSizeClasses = 4;
+// upper bounds of the mean input size of classes 0..2 (class 3: above)
+constexpr uint64_t kClassBound[kSizeClasses - 1] = {64ull << 10, 768ull << 10, 2ull << 20};
+static inline int size_class(uint64_t mean) {
+    int k = 0;
+    while (k < kSizeClasses - 1 && mean > kClassBound[k]) k++;
+    return k;
+}
+
 struct przmg_batch {
     Ctx* ctx = nullptr;
     int profile = 1;
@@ -131,6 +149,12 @@ struct przmg_batch {
     // per input i, where its items start in each work list ([i + 1] = end)
     std::vector<uint32_t> job_small0, job_rt0, job_big0, job_tile0, job_asm0;
     int launches_plain = 0;
+    // persistent front end (used when tune.front == 1 and every input has at
+    // most 512 tiles): its work items, tile list and per-input tokenizer targets
+    Tuning tune;
+    bool front = false;
+    uint32_t nfront = 0;
+    DevBuf d_fitems, d_ftiles, d_ftarget, d_fctl;  // d_fctl: [0] next item, [16 ...] per-input progress
     HostBuf h_offs;
     std::vector<RxTile> rtiles;
     uint64_t max_big_cand = 0;  // most radix candidates of one frame
@@ -151,7 +175,8 @@ struct przmg_batch {
         DevBuf* all[] = {&d_in, &d_jobs, &d_small, &d_big, &d_tiles, &d_desc, &d_slots, &d_tile_lens, &d_streams,
                          &d_job_lens, &d_hist, &d_tabs, &d_infos, &d_ans, &d_outs, &d_plans, &d_sizes, &d_out, &d_misc,
                          &d_lists, &d_rtiles, &d_rx_cnt, &d_rx_parts, &d_rx_ent, &d_rx_key, &d_rx_pred, &d_stage_in,
-                         &d_stage_out, &d_stage_offs, &d_up_offs, &d_tile_sched, &d_asm, &d_asm_job};
+                         &d_stage_out, &d_stage_offs, &d_up_offs, &d_tile_sched, &d_asm, &d_asm_job,
+                         &d_fitems, &d_ftiles, &d_ftarget, &d_fctl};
         for (DevBuf* b : all) b->release();
         h_offs.release();
     }
@@ -177,6 +202,10 @@ struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::mutex mu;
+    Tuning tune[kSizeClasses];
+    uint64_t front_wait_ns = 1000000000ull;  // limit of one persistent front-end wait
+    bool front_unreachable = false;          // test hook: add a wait that nothing ends
+    int clock_khz = 1965000;
     std::mutex pools_mu;
     std::unordered_map<uint64_t, przmg_pinned_pool*> pools;  // GetPinned pools by power-of-two size
     cudaDeviceProp prop{};
@@ -189,6 +218,56 @@ struct Ctx {
     DevBuf d_lit;  // scratch of przmg_package_literals_batch
     cudaEvent_t ev[8] = {};
 };
+
+// Work items of the persistent front end in stage order, inputs largest
+// first within a stage (their long rANS chains then start first), with each
+// item's progress target: the number of items of its input in earlier
+// stages.  Per input, large (radix) frames have nrt count items, 1 scan, nrt
+// scatters, kFrontResolveItems resolves, nv verify chunks, then one item per
+// tokenizer tile and one gather; small frames one tile-finder item per tile,
+// then their tiles and the gather.
+static void front_build(const przmg_batch* b, uint32_t chunk, bool unreachable, std::vector<FrontItem>& items,
+                        std::vector<TokTile>& ftiles, std::vector<uint32_t>& tok_target) {
+    const uint32_t nj = b->njobs;
+    std::vector<uint32_t> ord(nj);
+    for (uint32_t i = 0; i < nj; i++) ord[i] = i;
+    std::stable_sort(ord.begin(), ord.end(), [&](uint32_t x, uint32_t y) { return b->jobs[x].n > b->jobs[y].n; });
+    items.clear();
+    ftiles.clear();
+    tok_target.assign(nj, 0);
+    auto nrt = [&](uint32_t j) { return b->job_rt0[j + 1] - b->job_rt0[j]; };
+    auto nv = [&](uint32_t j) { return (rx_ncand(b->jobs[j].n) + chunk - 1) / chunk; };
+    auto big = [&](uint32_t j) { return b->job_big0[j + 1] > b->job_big0[j]; };
+    for (uint32_t j : ord)
+        for (uint32_t t = b->job_rt0[j]; t < b->job_rt0[j + 1]; t++) items.push_back({FS_RX_COUNT, j, t, 0});
+    for (uint32_t j : ord)
+        for (uint32_t t = b->job_small0[j]; t < b->job_small0[j + 1]; t++) items.push_back({FS_TILE_FIND, j, t, 0});
+    for (uint32_t j : ord)
+        if (big(j)) items.push_back({FS_RX_SCAN, j, j, nrt(j)});
+    for (uint32_t j : ord)
+        if (big(j))
+            for (uint32_t t = b->job_rt0[j]; t < b->job_rt0[j + 1]; t++) items.push_back({FS_RX_SCATTER, j, t, nrt(j) + 1});
+    for (uint32_t j : ord)
+        if (big(j))
+            for (uint32_t g = 0; g < kFrontResolveItems; g++)
+                items.push_back({FS_RX_RESOLVE, j, g * kFrontWarps, 2 * nrt(j) + 1});
+    for (uint32_t j : ord)
+        if (big(j))
+            for (uint32_t c = 0; c < nv(j); c++)
+                items.push_back({FS_RX_VERIFY, j, c * chunk, 2 * nrt(j) + 1 + kFrontResolveItems});
+    for (uint32_t j : ord) {
+        const uint32_t nt = b->job_tile0[j + 1] - b->job_tile0[j];
+        tok_target[j] = big(j) ? 2 * nrt(j) + 1 + kFrontResolveItems + nv(j) : nt;
+        for (uint32_t t = b->job_tile0[j]; t < b->job_tile0[j + 1]; t++) ftiles.push_back(b->tiles[t]);
+    }
+    for (uint32_t t = 0; t < ftiles.size(); t += kFrontWarps)
+        items.push_back({FS_TOKENIZE, std::min<uint32_t>(kFrontWarps, (uint32_t)ftiles.size() - t), t, 0});
+    for (uint32_t j : ord) {
+        const uint32_t nt = b->job_tile0[j + 1] - b->job_tile0[j];
+        items.push_back({FS_GATHER, j, j, nt ? tok_target[j] + nt : 0});
+    }
+    if (unreachable && nj) items.push_back({FS_NOP, 0, 0, 0xFFFFFFFFu});
+}
 
 // Lay out a batch for the given input sizes; (re)allocates only when a
 // buffer is too small, so repeated calls of similar size reuse memory.
@@ -273,6 +352,19 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
         for (uint32_t k = 0, np = asm_lit_parts(b->jobs[i]); k <= np; k++) asm_job.push_back(make_uint2(i, k));
     }
     b->job_asm0[njobs] = (uint32_t)asm_job.size();
+    // launch geometry of this batch's size class; the persistent front end
+    // needs every input within 512 tiles (its gather's shared tile offsets)
+    uint64_t total_n = 0;
+    uint32_t max_tiles = 0;
+    for (uint32_t i = 0; i < njobs; i++) { total_n += b->jobs[i].n; max_tiles = std::max(max_tiles, b->jobs[i].ntiles); }
+    b->tune = b->ctx->tune[size_class(njobs ? total_n / njobs : 0)];
+    b->front = b->tune.front == 1 && njobs > 0 && max_tiles <= 512 && !force_radix;
+    std::vector<FrontItem> fitems;
+    std::vector<TokTile> ftiles;
+    std::vector<uint32_t> ftarget;
+    if (b->front)
+        front_build(b, std::max<uint32_t>(256, b->tune.verify_chunk), b->ctx->front_unreachable, fitems, ftiles, ftarget);
+    b->nfront = (uint32_t)fitems.size();
     b->desc_words = desc + 16;
     b->stream_bytes = str + 64;
     b->ans_bytes = ans + 64;
@@ -285,6 +377,12 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     CK(b->d_tile_sched.ensure(2 * sizeof(uint32_t) * std::max<size_t>(b->tiles.size(), 1)));
     CK(b->d_asm.ensure(sizeof(uint2) * std::max<size_t>(b->asm_items.size(), 1)));
     CK(b->d_asm_job.ensure(sizeof(uint2) * std::max<size_t>(asm_job.size(), 1)));
+    if (b->front) {
+        CK(b->d_fitems.ensure(sizeof(FrontItem) * fitems.size()));
+        CK(b->d_ftiles.ensure(sizeof(TokTile) * std::max<size_t>(ftiles.size(), 1)));
+        CK(b->d_ftarget.ensure(4ull * njobs));
+        CK(b->d_fctl.ensure(64 + 4ull * njobs));
+    }
     CK(b->d_desc.ensure(b->desc_words * 4));
     CK(b->d_slots.ensure((size_t)b->ntiles * kSlotStride));
     CK(b->d_tile_lens.ensure((size_t)b->ntiles * S_COUNT * 4));
@@ -324,6 +422,12 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
         CK(cudaMemcpyAsync(b->d_asm.p, b->asm_items.data(), sizeof(uint2) * b->asm_items.size(), cudaMemcpyHostToDevice, s));
     if (!asm_job.empty())
         CK(cudaMemcpyAsync(b->d_asm_job.p, asm_job.data(), sizeof(uint2) * asm_job.size(), cudaMemcpyHostToDevice, s));
+    if (b->front) {
+        CK(cudaMemcpyAsync(b->d_fitems.p, fitems.data(), sizeof(FrontItem) * fitems.size(), cudaMemcpyHostToDevice, s));
+        if (!ftiles.empty())
+            CK(cudaMemcpyAsync(b->d_ftiles.p, ftiles.data(), sizeof(TokTile) * ftiles.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(b->d_ftarget.p, ftarget.data(), 4ull * njobs, cudaMemcpyHostToDevice, s));
+    }
     CK(cudaMemsetAsync(b->d_sizes.p, 0, (size_t)njobs * 4 + 16, s));
     CK(cudaMemsetAsync(b->d_job_lens.p, 0, (size_t)njobs * S_COUNT * 4 + 16, s));
     // the host-side vectors above must stay alive until the copies ran
@@ -333,9 +437,9 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
 
 // Stages of one enqueue.  stop_after: 0 match only, 1 through tokenize +
 // gather, 2 the full frame pipeline.
-static const char* const kStageNames[] = {"tile_find", "radix_find", "tokenize", "gather",
+static const char* const kStageNames[] = {"tile_find", "radix_find", "tokenize", "gather", "front",
                                           "normalize", "rans", "plan", "assemble"};
-constexpr int kStages = 8;
+constexpr int kStages = 9;
 
 // The part of a batch one launch sequence covers: inputs [j0, j0 + nj) and
 // the matching runs of the batch's work lists (every list is ordered by
@@ -391,11 +495,48 @@ static Range job_range(const przmg_batch* b, uint32_t i) {
 // ev (optional): kStages + 1 events; ev[0] before the first kernel and
 // ev[k + 1] after stage k (stages that do not run record back to back).
 // skip_match: the match table is already in d_desc (tokenizer-only runs).
+// use_front: match, tokenize and gather of the whole batch in one launch of
+// the persistent front end (stages 0-3 then record back to back).
 static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, const Range& R, cudaEvent_t* ev,
-                            bool skip_match, int& launches) {
+                            bool skip_match, bool use_front, int& launches) {
     Ctx* c = b->ctx;
     auto mark = [&](int k) -> cudaError_t { return ev ? cudaEventRecord(ev[k], s) : cudaSuccess; };
     CK(mark(0));
+    if (use_front) {
+        for (int k = 1; k <= 4; k++) CK(mark(k));
+        CK(cudaMemsetAsync(b->d_fctl.p, 0, 64 + 4ull * b->njobs, s));
+        FrontArgs a;
+        a.in = b->d_in.as<uint8_t>();
+        a.jobs = b->d_jobs.as<Job>();
+        a.items = b->d_fitems.as<FrontItem>();
+        a.nitems = b->nfront;
+        a.head = b->d_fctl.as<uint32_t>();
+        a.progress = b->d_fctl.as<uint32_t>() + 16;
+        a.err = b->err_word();
+        a.tok_target = b->d_ftarget.as<uint32_t>();
+        a.wait_cycles = (long long)((double)c->front_wait_ns * c->clock_khz / 1e6);
+        a.small = b->d_small.as<TileRef>();
+        a.rtiles = b->d_rtiles.as<RxTile>();
+        a.tiles = b->d_ftiles.as<TokTile>();
+        a.ntiles = (uint32_t)b->tiles.size();
+        a.verify_chunk = std::max<uint32_t>(256, b->tune.verify_chunk);
+        a.desc = b->d_desc.as<uint32_t>();
+        a.rx_cnt = b->d_rx_cnt.as<uint32_t>();
+        a.rx_parts = b->d_rx_parts.as<uint2>();
+        a.rx_ent = b->d_rx_ent.as<uint32_t>();
+        a.rx_key = b->d_rx_key.as<uint16_t>();
+        a.rx_pred = b->d_rx_pred.as<uint32_t>();
+        a.slots = b->d_slots.as<uint8_t>();
+        a.tile_lens = b->d_tile_lens.as<uint32_t>();
+        a.streams = b->d_streams.as<uint8_t>();
+        a.job_lens = b->d_job_lens.as<uint32_t>();
+        a.hist = b->d_hist.as<uint32_t>();
+        const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(b->nfront, std::max<uint32_t>(1, b->tune.ctas_per_sm) * c->sms));
+        k_front<<<grid, kFrontThreads, kFrontSmem, s>>>(a);
+        CK(cudaGetLastError());
+        launches++;
+        CK(mark(5));
+    } else {
     if (R.nsmall && !skip_match) {
         const uint32_t grid = std::min<uint32_t>(R.nsmall, 8u * c->sms);
         k_tile_find<<<grid, 256, kTileFindSmem, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(),
@@ -455,12 +596,14 @@ static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, cons
         CK(mark(3));
     }
     CK(mark(4));
+    CK(mark(5));
+    }
     if (stop_after >= 2 && R.nj) {
         if (b->profile == 1) {
             k_normalize<<<R.nj, 128, 0, s>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_job_lens.as<uint32_t>(),
                                              b->d_hist.as<uint32_t>(), b->d_tabs.as<EncSym>(), b->d_infos.as<TableInfo>());
             CK(cudaGetLastError());
-            CK(mark(5));
+            CK(mark(6));
             const uint32_t list_cap = 4 * b->njobs;
             uint32_t* lists = b->d_lists.as<uint32_t>();
             uint32_t* counts = lists + 2 * list_cap;
@@ -475,26 +618,26 @@ static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, cons
                 b->d_outs.as<TaskOut>());
             CK(cudaGetLastError());
             launches += 3;
-            CK(mark(6));
+            CK(mark(7));
         } else {
-            CK(mark(5));
             CK(mark(6));
+            CK(mark(7));
         }
         k_plan<<<(R.nj + 127) / 128, 128, 0, s>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_job_lens.as<uint32_t>(),
                                                   b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(),
                                                   b->d_streams.as<uint8_t>(), b->d_plans.as<Plan>(),
                                                   b->d_sizes.as<uint32_t>());
         CK(cudaGetLastError());
-        CK(mark(7));
+        CK(mark(8));
         k_assemble<<<std::max<uint32_t>(1, std::min<uint32_t>(R.nasm, 1u << 20)), kAsmThreads, 0, s>>>(
             b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), R.asm_list + R.asm0, R.nasm, b->d_job_lens.as<uint32_t>(),
             b->d_plans.as<Plan>(), b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(), b->d_streams.as<uint8_t>(),
             b->d_ans.as<uint8_t>(), b->d_out.as<uint8_t>());
         CK(cudaGetLastError());
         launches += 2;
-        CK(mark(8));
+        CK(mark(9));
     } else {
-        for (int k = 5; k <= 8; k++) CK(mark(k));
+        for (int k = 6; k <= 9; k++) CK(mark(k));
     }
     return PRZMG_OK;
 }
@@ -504,7 +647,8 @@ static int32_t batch_launch(przmg_batch* b, cudaStream_t s, int stop_after, cuda
                             bool skip_match = false) {
     CK(cudaMemsetAsync(b->d_misc.p, 0, 16, s));
     int launches = 0;
-    int32_t r = launch_range(b, s, stop_after, whole_range(b), ev, skip_match, launches);
+    const bool use_front = b->front && stop_after >= 1 && !skip_match;
+    int32_t r = launch_range(b, s, stop_after, whole_range(b), ev, skip_match, use_front, launches);
     b->launches = launches;
     return r;
 }
@@ -516,18 +660,25 @@ static int32_t batch_launch_plain(przmg_batch* b, cudaStream_t s) {
     int launches = 0;
     for (uint32_t i = 0; i < b->njobs; i++) {
         if (b->jobs[i].n == 0) continue;
-        int32_t r = launch_range(b, s, 2, job_range(b, i), nullptr, false, launches);
+        int32_t r = launch_range(b, s, 2, job_range(b, i), nullptr, false, false, launches);
         if (r) return r;
     }
     b->launches_plain = launches;
     return PRZMG_OK;
 }
 
+static int32_t device_error(uint32_t err) {
+    if (err & E_SCHED_TIMEOUT)
+        return fail(PRZMG_ERR_DEVICE, "a wait of the persistent front end ran past its limit (error bits " +
+                                          std::to_string(err) + "); the batch's frames are not valid");
+    return fail(PRZMG_ERR_DEVICE, "device bound violation, error bits " + std::to_string(err));
+}
+
 static int32_t batch_check(przmg_batch* b) {
     uint32_t err = 0;
     CK(cudaMemcpyAsync(&err, b->err_word(), 4, cudaMemcpyDeviceToHost, b->ctx->stream));
     CK(cudaStreamSynchronize(b->ctx->stream));
-    if (err) return fail(PRZMG_ERR_DEVICE, "device bound violation, error bits " + std::to_string(err));
+    if (err) return device_error(err);
     return PRZMG_OK;
 }
 
@@ -558,6 +709,8 @@ static int32_t ctx_setup(Ctx* c) {
     CK(cudaFuncSetAttribute(k_tile_find, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileFindSmem));
     CK(cudaFuncSetAttribute(k_rx_resolve, cudaFuncAttributeMaxDynamicSharedMemorySize, kRxResolveSmem));
     CK(cudaFuncSetAttribute(k_rans, cudaFuncAttributeMaxDynamicSharedMemorySize, kRansSmem));
+    CK(cudaFuncSetAttribute(k_front, cudaFuncAttributeMaxDynamicSharedMemorySize, kFrontSmem));
+    CK(cudaDeviceGetAttribute(&c->clock_khz, cudaDevAttrClockRate, c->device));
     CK(cudaFuncSetAttribute(k_stream_rans, cudaFuncAttributeMaxDynamicSharedMemorySize, kRansSmem));
     CK(c->d_meta8.ensure(8 * 256 * sizeof(EncSym)));
     CK(c->d_ctxlut.ensure(256));
@@ -1164,6 +1317,54 @@ extern "C" int32_t przmg_batch_sizes(przmg_batch* b, uint32_t* sizes) {
 
 extern "C" int32_t przmg_batch_launch_count(przmg_batch* b) { return b ? b->launches : 0; }
 
+extern "C" int32_t przmg_size_class(uint64_t mean_input_bytes) { return size_class(mean_input_bytes); }
+
+extern "C" int32_t przmg_set_tuning(przmg_ctx* h, int32_t cls, int32_t front, int32_t ctas_per_sm, int32_t verify_chunk) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c) return fail(PRZMG_ERR_INVALID_ARG, "null context");
+    if (cls < 0 || cls >= kSizeClasses || front < 0 || front > 1 || ctas_per_sm < 1 || ctas_per_sm > 3 ||
+        verify_chunk < 256 || verify_chunk > (1 << 16) || (verify_chunk & 255))
+        return fail(PRZMG_ERR_INVALID_ARG, "tuning out of range (class 0-3, front 0/1, 1-3 blocks per SM, "
+                                           "verify chunk a multiple of 256 in [256, 65536])");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->tune[cls].front = (uint32_t)front;
+    c->tune[cls].ctas_per_sm = (uint32_t)ctas_per_sm;
+    c->tune[cls].verify_chunk = (uint32_t)verify_chunk;
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_get_tuning(przmg_ctx* h, int32_t cls, int32_t* front, int32_t* ctas_per_sm,
+                                    int32_t* verify_chunk) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c || cls < 0 || cls >= kSizeClasses) return fail(PRZMG_ERR_INVALID_ARG, "null context or unknown class");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (front) *front = (int32_t)c->tune[cls].front;
+    if (ctas_per_sm) *ctas_per_sm = (int32_t)c->tune[cls].ctas_per_sm;
+    if (verify_chunk) *verify_chunk = (int32_t)c->tune[cls].verify_chunk;
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_set_front_wait(przmg_ctx* h, uint64_t limit_ns, int32_t add_unreachable_wait) {
+    Ctx* c = reinterpret_cast<Ctx*>(h);
+    if (!c) return fail(PRZMG_ERR_INVALID_ARG, "null context");
+    if (limit_ns == 0 || limit_ns > 60ull * 1000000000ull) return fail(PRZMG_ERR_INVALID_ARG, "limit out of range");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->front_wait_ns = limit_ns;
+    c->front_unreachable = add_unreachable_wait != 0;
+    return PRZMG_OK;
+}
+
+extern "C" int32_t przmg_batch_info(przmg_batch* b, uint32_t info[4]) {
+    if (!b || !info) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
+    uint64_t total = 0;
+    for (const Job& j : b->jobs) total += j.n;
+    info[0] = b->front ? 1u : 0u;
+    info[1] = (uint32_t)size_class(b->njobs ? total / b->njobs : 0);
+    info[2] = b->tune.ctas_per_sm;
+    info[3] = b->tune.verify_chunk;
+    return PRZMG_OK;
+}
+
 extern "C" int32_t przmg_batch_enqueue_plain(przmg_batch* b, uint64_t stream, int32_t* launches) {
     if (!b) return fail(PRZMG_ERR_INVALID_ARG, "null batch");
     Ctx* c = b->ctx;
@@ -1217,7 +1418,7 @@ static int32_t batch_download_packed(przmg_batch* b, uint8_t* host, uint64_t cap
     uint32_t err = 0;
     CK(cudaMemcpyAsync(&err, b->err_word(), 4, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    if (err) return fail(PRZMG_ERR_DEVICE, "device bound violation, error bits " + std::to_string(err));
+    if (err) return device_error(err);
     std::vector<uint64_t> offs(b->njobs);
     uint64_t t = 0;
     for (uint32_t i = 0; i < b->njobs; i++) { offs[i] = t; t += fs[i]; }

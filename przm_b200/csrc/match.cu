@@ -31,18 +31,17 @@ __device__ __forceinline__ uint32_t lcp_smem(const uint8_t* t, uint32_t a, uint3
 struct TileRef { uint32_t job; uint32_t tile; };
 constexpr uint32_t kTileFindSmem = kTile + 16 + 3 * kBuckets * 4;
 
-__global__ void __launch_bounds__(256) k_tile_find(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
-                                                   const TileRef* __restrict__ refs, uint32_t nrefs,
-                                                   uint32_t* __restrict__ desc) {
-    extern __shared__ __align__(16) uint8_t smem_tf[];
+// One tile, by a block of 256 threads; smem = kTileFindSmem bytes.
+__device__ void tile_find_item(const uint8_t* __restrict__ in, const Job* __restrict__ jobs, const TileRef ref,
+                               uint32_t* __restrict__ desc, uint8_t* smem_tf) {
     uint8_t* s_tile = smem_tf;                                          // kTile + 16
     uint32_t* s_head = reinterpret_cast<uint32_t*>(smem_tf + kTile + 16); // kBuckets each
     uint32_t* s_top = s_head + kBuckets;
     uint32_t* s_sec = s_top + kBuckets;
     const uint32_t tid = threadIdx.x, lane = tid & 31;
-    for (uint32_t r = blockIdx.x; r < nrefs; r += gridDim.x) {
-        const Job job = jobs[refs[r].job];
-        const uint32_t ts = refs[r].tile * kTile;
+    {
+        const Job job = jobs[ref.job];
+        const uint32_t ts = ref.tile * kTile;
         const uint32_t tl = min(kTile, job.n - ts);
         const uint8_t* src = in + job.in_off + ts;
         uint32_t* out = desc + job.desc_off + ts;
@@ -106,6 +105,13 @@ __global__ void __launch_bounds__(256) k_tile_find(const uint8_t* __restrict__ i
     }
 }
 
+__global__ void __launch_bounds__(256) k_tile_find(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
+                                                   const TileRef* __restrict__ refs, uint32_t nrefs,
+                                                   uint32_t* __restrict__ desc) {
+    extern __shared__ __align__(16) uint8_t smem_tf[];
+    for (uint32_t r = blockIdx.x; r < nrefs; r += gridDim.x) tile_find_item(in, jobs, refs[r], desc, smem_tf);
+}
+
 // ---------------------------------------------------------------------------
 // Radix-strike finder, semantics of przm_lz77_radix_strike_kernel
 // (przm_lz77.cu:156-213) in sequential insertion order: candidate c (the
@@ -142,34 +148,35 @@ __device__ __forceinline__ uint32_t kmer_hash(uint64_t k) {
 }
 __host__ __device__ inline uint32_t rx_ncand(uint32_t n) { return n >= 8 ? (n - 8) / 8 + 1 : 0; }
 
+// One radix tile, block of 256; s_cnt = kRxParts words of shared memory.
+__device__ void rx_count_item(const uint8_t* __restrict__ in, const Job* __restrict__ jobs, const RxTile tt,
+                              uint32_t* __restrict__ cnt, uint32_t* s_cnt) {
+    const Job job = jobs[tt.job];
+    const uint64_t* src = reinterpret_cast<const uint64_t*>(in + job.in_off);
+    const uint32_t C = rx_ncand(job.n), c0 = tt.tile * kCandPerTile, c1 = min(C, c0 + kCandPerTile);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kRxParts; i += 256) s_cnt[i] = 0;
+    __syncthreads();
+    for (uint32_t c = c0 + threadIdx.x; c < c1; c += 256) atomicAdd(&s_cnt[kmer_hash(__ldg(src + c)) >> kRxKeyBits], 1u);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kRxParts; i += 256) cnt[(uint64_t)(job.tile0 + tt.tile) * kRxParts + i] = s_cnt[i];
+}
+
 __global__ void __launch_bounds__(256) k_rx_count(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
                                                   const RxTile* __restrict__ rt, uint32_t nrt,
                                                   uint32_t* __restrict__ cnt) {
     __shared__ uint32_t s_cnt[kRxParts];
-    for (uint32_t T = blockIdx.x; T < nrt; T += gridDim.x) {
-        const RxTile tt = rt[T];
-        const Job job = jobs[tt.job];
-        const uint64_t* src = reinterpret_cast<const uint64_t*>(in + job.in_off);
-        const uint32_t C = rx_ncand(job.n), c0 = tt.tile * kCandPerTile, c1 = min(C, c0 + kCandPerTile);
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < kRxParts; i += 256) s_cnt[i] = 0;
-        __syncthreads();
-        for (uint32_t c = c0 + threadIdx.x; c < c1; c += 256) atomicAdd(&s_cnt[kmer_hash(__ldg(src + c)) >> kRxKeyBits], 1u);
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < kRxParts; i += 256) cnt[(uint64_t)(job.tile0 + tt.tile) * kRxParts + i] = s_cnt[i];
-    }
+    for (uint32_t T = blockIdx.x; T < nrt; T += gridDim.x) rx_count_item(in, jobs, rt[T], cnt, s_cnt);
 }
 
 // One block of kRxParts threads per large frame: thread b owns partition b.
 // Turns the per-tile counts into per-tile starting slots (in place) and
 // writes the partition's (start, length) pair.
-__global__ void __launch_bounds__(kRxParts) k_rx_scan(const Job* __restrict__ jobs, const uint32_t* __restrict__ big,
-                                                      uint32_t nbig, uint32_t* __restrict__ cnt,
-                                                      uint2* __restrict__ parts) {
-    __shared__ uint32_t s_warp[kRxParts / 32];
+// One large frame j, block of kRxParts (256) threads; s_warp = 8 words.
+__device__ void rx_scan_item(const Job* __restrict__ jobs, uint32_t j, uint32_t* __restrict__ cnt,
+                             uint2* __restrict__ parts, uint32_t* s_warp) {
     const uint32_t b = threadIdx.x, lane = b & 31, warp = b >> 5;
-    for (uint32_t x = blockIdx.x; x < nbig; x += gridDim.x) {
-        const uint32_t j = big[x];
+    {
         const Job job = jobs[j];
         const uint32_t nt = (rx_ncand(job.n) + kCandPerTile - 1) / kCandPerTile;
         uint32_t* cj = cnt + (uint64_t)job.tile0 * kRxParts + b;
@@ -197,17 +204,22 @@ __global__ void __launch_bounds__(kRxParts) k_rx_scan(const Job* __restrict__ jo
     }
 }
 
+__global__ void __launch_bounds__(kRxParts) k_rx_scan(const Job* __restrict__ jobs, const uint32_t* __restrict__ big,
+                                                      uint32_t nbig, uint32_t* __restrict__ cnt,
+                                                      uint2* __restrict__ parts) {
+    __shared__ uint32_t s_warp[kRxParts / 32];
+    for (uint32_t x = blockIdx.x; x < nbig; x += gridDim.x) rx_scan_item(jobs, big[x], cnt, parts, s_warp);
+}
+
 // 8 warps per tile, warp w taking candidates [c0 + 512w, c0 + 512w + 512)
 // in 16 rounds of 32; slots are assigned in position order.
-__global__ void __launch_bounds__(256) k_rx_scatter(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
-                                                    const RxTile* __restrict__ rt, uint32_t nrt,
-                                                    const uint32_t* __restrict__ off, uint32_t* __restrict__ ent,
-                                                    uint16_t* __restrict__ key) {
-    __shared__ uint32_t s_w[8][kRxParts];
+// One radix tile, block of 256; s_w = 8 x kRxParts words of shared memory.
+__device__ void rx_scatter_item(const uint8_t* __restrict__ in, const Job* __restrict__ jobs, const RxTile tt,
+                                const uint32_t* __restrict__ off, uint32_t* __restrict__ ent,
+                                uint16_t* __restrict__ key, uint32_t (*s_w)[kRxParts]) {
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t lt = (1u << lane) - 1u;
-    for (uint32_t T = blockIdx.x; T < nrt; T += gridDim.x) {
-        const RxTile tt = rt[T];
+    {
         const Job job = jobs[tt.job];
         const uint64_t* src = reinterpret_cast<const uint64_t*>(in + job.in_off);
         const uint32_t C = rx_ncand(job.n), c0 = tt.tile * kCandPerTile, c1 = min(C, c0 + kCandPerTile);
@@ -254,6 +266,14 @@ __global__ void __launch_bounds__(256) k_rx_scatter(const uint8_t* __restrict__ 
     }
 }
 
+__global__ void __launch_bounds__(256) k_rx_scatter(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
+                                                    const RxTile* __restrict__ rt, uint32_t nrt,
+                                                    const uint32_t* __restrict__ off, uint32_t* __restrict__ ent,
+                                                    uint16_t* __restrict__ key) {
+    __shared__ uint32_t s_w[8][kRxParts];
+    for (uint32_t T = blockIdx.x; T < nrt; T += gridDim.x) rx_scatter_item(in, jobs, rt[T], off, ent, key, s_w);
+}
+
 // Verification and extension of candidate c against its predecessor q
 // (przm_lz77.cu:180-209): the match grows in 8-byte steps while
 // p + L + 8 <= n and L + 8 <= 4095, then byte by byte below 4095.  Four steps
@@ -296,22 +316,17 @@ bytes:
     return pack_match32(L, dist);
 }
 
-__global__ void __launch_bounds__(kRxResolveWarps * 32) k_rx_resolve(const Job* __restrict__ jobs,
-                                                                     const uint32_t* __restrict__ big, uint32_t nbig,
-                                                                     const uint2* __restrict__ parts,
-                                                                     const uint32_t* __restrict__ ent,
-                                                                     const uint16_t* __restrict__ key,
-                                                                     uint32_t* __restrict__ pred) {
-    extern __shared__ __align__(16) uint32_t smem_rx[];
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// Partition b of large frame j, by one warp; table = kRxKeys words of
+// shared memory (latest candidate + 1 per key, 0 = none).
+__device__ void rx_resolve_warp(const Job* __restrict__ jobs, uint32_t j, uint32_t b, const uint2* __restrict__ parts,
+                                const uint32_t* __restrict__ ent, const uint16_t* __restrict__ key,
+                                uint32_t* __restrict__ pred, uint32_t* table) {
+    const uint32_t lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
-    uint32_t* table = smem_rx + warp * kRxKeys;  // latest candidate + 1 per key, 0 = none
-    const uint32_t nw = gridDim.x * kRxResolveWarps;
-    for (uint32_t x = blockIdx.x * kRxResolveWarps + warp; x < nbig * kRxParts; x += nw) {
-        const uint32_t j = big[x / kRxParts], b = x % kRxParts;
+    {
         const Job job = jobs[j];
         const uint2 pr = parts[(uint64_t)j * kRxParts + b];
-        if (pr.y == 0) continue;
+        if (pr.y == 0) return;
         for (uint32_t i = lane; i < kRxKeys / 4; i += 32) reinterpret_cast<uint4*>(table)[i] = make_uint4(0, 0, 0, 0);
         __syncwarp();
         const uint32_t* ej = ent + job.desc_off + pr.x;
@@ -348,22 +363,37 @@ __global__ void __launch_bounds__(kRxResolveWarps * 32) k_rx_resolve(const Job* 
     }
 }
 
+__global__ void __launch_bounds__(kRxResolveWarps * 32) k_rx_resolve(const Job* __restrict__ jobs,
+                                                                     const uint32_t* __restrict__ big, uint32_t nbig,
+                                                                     const uint2* __restrict__ parts,
+                                                                     const uint32_t* __restrict__ ent,
+                                                                     const uint16_t* __restrict__ key,
+                                                                     uint32_t* __restrict__ pred) {
+    extern __shared__ __align__(16) uint32_t smem_rx[];
+    const uint32_t warp = threadIdx.x >> 5;
+    uint32_t* table = smem_rx + warp * kRxKeys;
+    const uint32_t nw = gridDim.x * kRxResolveWarps;
+    for (uint32_t x = blockIdx.x * kRxResolveWarps + warp; x < nbig * kRxParts; x += nw)
+        rx_resolve_warp(jobs, big[x / kRxParts], x % kRxParts, parts, ent, key, pred, table);
+}
+
 // One thread per candidate of every large frame (grid.y = frame): verify and
 // extend against the resolved predecessor, write the descriptor.
-__global__ void __launch_bounds__(256) k_rx_verify(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
-                                                   const uint32_t* __restrict__ big, const uint32_t* __restrict__ ent,
-                                                   const uint32_t* __restrict__ pred, uint32_t nbig,
-                                                   uint32_t* __restrict__ desc) {
-    for (uint32_t y = blockIdx.y; y < nbig; y += gridDim.y) {
-        const Job job = jobs[big[y]];
-        const uint32_t C = rx_ncand(job.n);
+// Entries [lo, hi) of large frame `job`'s candidate list, thread t of
+// nthr: two entries per thread per step, their first loads in flight
+// together.
+__device__ __forceinline__ void rx_verify_range(const uint8_t* __restrict__ in, const Job& job,
+                                                const uint32_t* __restrict__ ent, const uint32_t* __restrict__ pred,
+                                                uint32_t* __restrict__ desc, uint32_t lo, uint32_t hi, uint32_t t,
+                                                uint32_t nthr) {
+    {
+        const uint32_t C = hi;
         const uint8_t* src = in + job.in_off;
         const uint32_t* ej = ent + job.desc_off;
         const uint32_t* pj = pred + job.desc_off;
         uint32_t* d8 = desc + job.desc_off;
-        // two entries per thread per step, their first loads in flight together
-        const uint32_t stride = gridDim.x * 256;
-        for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < C; i += 2 * stride) {
+        const uint32_t stride = nthr;
+        for (uint32_t i = lo + t; i < C; i += 2 * stride) {
             const uint32_t i2 = i + stride;
             const bool two = i2 < C;
             const uint32_t c1 = ej[i], p1 = pj[i];
@@ -374,6 +404,16 @@ __global__ void __launch_bounds__(256) k_rx_verify(const uint8_t* __restrict__ i
             d8[c1] = p1 ? rx_finish(src, job.n, c1, p1 - 1, x1) : 0u;
             if (two) d8[c2] = p2 ? rx_finish(src, job.n, c2, p2 - 1, x2) : 0u;
         }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_rx_verify(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
+                                                   const uint32_t* __restrict__ big, const uint32_t* __restrict__ ent,
+                                                   const uint32_t* __restrict__ pred, uint32_t nbig,
+                                                   uint32_t* __restrict__ desc) {
+    for (uint32_t y = blockIdx.y; y < nbig; y += gridDim.y) {
+        const Job job = jobs[big[y]];
+        rx_verify_range(in, job, ent, pred, desc, 0, rx_ncand(job.n), blockIdx.x * 256 + threadIdx.x, gridDim.x * 256);
     }
 }
 

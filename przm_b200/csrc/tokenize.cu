@@ -322,18 +322,12 @@ __device__ void tok_emit(const uint4* rec, uint32_t nrec, const uint8_t* tile_sr
     }
 }
 
-__global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
-                                                            const TokTile* __restrict__ tiles, uint32_t ntiles,
-                                                            const uint32_t* __restrict__ order,
-                                                            const uint32_t* __restrict__ desc, uint8_t* __restrict__ slots,
-                                                            uint32_t* __restrict__ tile_lens, uint32_t* __restrict__ err) {
-    __shared__ TokSmem s_tok[kTokWarps];
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    TokSmem& sm = s_tok[warp];
-    const uint32_t wid = blockIdx.x * kTokWarps + warp;
-    const uint32_t nw = gridDim.x * kTokWarps;
-    for (uint32_t T = wid; T < ntiles; T += nw) {
-        const TokTile tt = tiles[order[T]];
+// One 32 KiB tile, by one warp with its TokSmem.
+__device__ void tokenize_tile(const uint8_t* __restrict__ in, const Job* __restrict__ jobs, const TokTile tt,
+                              const uint32_t* __restrict__ desc, uint8_t* __restrict__ slots,
+                              uint32_t* __restrict__ tile_lens, uint32_t* __restrict__ err, TokSmem& sm) {
+    const uint32_t lane = threadIdx.x & 31;
+    {
         const Job job = jobs[tt.job];
         const uint8_t* src = in + job.in_off;
         const uint32_t* dj = desc + job.desc_off;
@@ -519,6 +513,18 @@ __global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __re
     }
 }
 
+__global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
+                                                            const TokTile* __restrict__ tiles, uint32_t ntiles,
+                                                            const uint32_t* __restrict__ order,
+                                                            const uint32_t* __restrict__ desc, uint8_t* __restrict__ slots,
+                                                            uint32_t* __restrict__ tile_lens, uint32_t* __restrict__ err) {
+    __shared__ TokSmem s_tok[kTokWarps];
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t wid = blockIdx.x * kTokWarps + warp;
+    const uint32_t nw = gridDim.x * kTokWarps;
+    for (uint32_t T = wid; T < ntiles; T += nw) tokenize_tile(in, jobs, tiles[order[T]], desc, slots, tile_lens, err, s_tok[warp]);
+}
+
 // ---------------------------------------------------------------------------
 // Tokenizer schedule.  A tile's walk costs about one step per match it takes,
 // and tiles of one batch differ by 10x or more (a tile of short repeats
@@ -605,21 +611,18 @@ __global__ void __launch_bounds__(1024) k_tile_order(const uint32_t* __restrict_
 // ---------------------------------------------------------------------------
 constexpr uint32_t kGatherThreads = 512;
 
-__global__ void __launch_bounds__(kGatherThreads) k_gather(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs,
-                                                          const uint8_t* __restrict__ slots,
-                                                          const uint32_t* __restrict__ tile_lens,
-                                                          uint8_t* __restrict__ streams, uint32_t* __restrict__ job_lens,
-                                                          uint32_t* __restrict__ hist /* njobs x 4 x 256 */,
-                                                          uint32_t* __restrict__ err) {
-    extern __shared__ uint32_t smem_g[];
-    uint32_t* s_off = smem_g;                      // (maxtiles + 1) per stream, filled per stream
-    __shared__ uint32_t s_hist[4][4][256];         // [stream][warp group][symbol]
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (uint32_t jl = blockIdx.x; jl < njobs; jl += gridDim.x) {
-        const uint32_t j = j0 + jl;
+// Frame j by the whole block (any multiple of 128 threads); s_off =
+// ntiles + 1 words, s_hist = [stream][warp group][symbol] counts.
+__device__ void gather_item(const Job* __restrict__ jobs, uint32_t j, const uint8_t* __restrict__ slots,
+                            const uint32_t* __restrict__ tile_lens, uint8_t* __restrict__ streams,
+                            uint32_t* __restrict__ job_lens, uint32_t* __restrict__ hist, uint32_t* __restrict__ err,
+                            uint32_t* s_off, uint32_t (*s_hist)[4][256]) {
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nthr = blockDim.x;
+    {
         const Job job = jobs[j];
         uint8_t* sreg = streams + job.str_off;
-        for (uint32_t i = tid; i < 4 * 4 * 256; i += kGatherThreads) (&s_hist[0][0][0])[i] = 0;
+        __syncthreads();
+        for (uint32_t i = tid; i < 4 * 4 * 256; i += nthr) (&s_hist[0][0][0])[i] = 0;
         for (int s = 0; s < S_COUNT; s++) {
             __syncthreads();
             // exclusive scan of this stream's tile lengths (<= 512 tiles)
@@ -627,7 +630,9 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather(const Job* __restrict
                 uint32_t carry = 0;
                 for (uint32_t b = 0; b < job.ntiles; b += 32) {
                     uint32_t i = b + lane;
-                    uint32_t v = i < job.ntiles ? tile_lens[(uint64_t)(job.tile0 + i) * S_COUNT + s] : 0;
+                    // an empty input has no tokenizer tile: its one tile
+                    // slot is never written, so its streams are empty
+                    uint32_t v = (i < job.ntiles && job.n > 0) ? tile_lens[(uint64_t)(job.tile0 + i) * S_COUNT + s] : 0;
                     uint32_t x = v;
                     for (uint32_t o = 1; o < 32; o <<= 1) {
                         uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
@@ -648,7 +653,7 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather(const Job* __restrict
             uint8_t* dst = sreg + stream_base(job, s);
             const int hs = s == S_LIT ? 0 : (s == S_OP ? 1 : (s == S_META ? 2 : (s == S_VAR ? 3 : -1)));
             // one warp per tile
-            for (uint32_t t = warp; t < job.ntiles; t += kGatherThreads / 32) {
+            for (uint32_t t = warp; t < job.ntiles; t += nthr / 32) {
                 const uint32_t o = s_off[t], l = s_off[t + 1] - o;
                 const uint8_t* sp = slots + (uint64_t)(job.tile0 + t) * kSlotStride + slot_base(s);
                 warp_copy_hist(dst + o, sp, l, hs >= 0 ? s_hist[hs][warp & 3] : nullptr, lane);
@@ -656,12 +661,24 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather(const Job* __restrict
             if (tid == 0) job_lens[(uint64_t)j * S_COUNT + s] = total;
         }
         __syncthreads();
-        for (uint32_t i = tid; i < 4 * 256; i += kGatherThreads) {
+        for (uint32_t i = tid; i < 4 * 256; i += nthr) {
             uint32_t hs = i >> 8, sym = i & 255;
             hist[(uint64_t)j * 1024 + i] = s_hist[hs][0][sym] + s_hist[hs][1][sym] + s_hist[hs][2][sym] + s_hist[hs][3][sym];
         }
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(kGatherThreads) k_gather(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs,
+                                                          const uint8_t* __restrict__ slots,
+                                                          const uint32_t* __restrict__ tile_lens,
+                                                          uint8_t* __restrict__ streams, uint32_t* __restrict__ job_lens,
+                                                          uint32_t* __restrict__ hist /* njobs x 4 x 256 */,
+                                                          uint32_t* __restrict__ err) {
+    extern __shared__ uint32_t smem_g[];
+    __shared__ uint32_t s_hist[4][4][256];
+    for (uint32_t jl = blockIdx.x; jl < njobs; jl += gridDim.x)
+        gather_item(jobs, j0 + jl, slots, tile_lens, streams, job_lens, hist, err, smem_g, s_hist);
 }
 
 }  // namespace pz

@@ -32,6 +32,7 @@ MaxTileLitBytes = 36864
 
 PROFILE_D2D = 0
 PROFILE_ANS = 1
+TUNING_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
 NORM_GO = 0
 NORM_CPU = 1
 
@@ -220,6 +221,11 @@ def SerializeMatrix(freq) -> bytes:
     return bytes(out[:n])
 
 
+def SizeClass(meanInputBytes: int) -> int:
+    """Size class of a batch by its mean input size (0..3)."""
+    return int(L().przmg_size_class(meanInputBytes))
+
+
 def FrameBound(n: int) -> int:
     return int(L().przmg_frame_bound(n))
 
@@ -306,10 +312,37 @@ class GPUCompressor:
         self.DeviceName = name.value.decode(errors="replace")
         self.SMCount = sm.value
         self.TotalVRAMBytes = vram.value
+        self.LoadTuning()
 
     @property
     def handle(self):
         return self._h
+
+    # -- launch geometry per size class (przm_b200/tuning.json) --
+    def SetTuning(self, sizeClass: int, front: int, ctasPerSM: int, verifyChunk: int) -> None:
+        _check(L().przmg_set_tuning(self._h, sizeClass, front, ctasPerSM, verifyChunk))
+
+    def GetTuning(self, sizeClass: int) -> dict[str, int]:
+        f, c, v = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(L().przmg_get_tuning(self._h, sizeClass, C.byref(f), C.byref(c), C.byref(v)))
+        return {"front": f.value, "ctas_per_sm": c.value, "verify_chunk": v.value}
+
+    def LoadTuning(self, path: str | None = None) -> bool:
+        """Applies the autotuner's table (przm_b200/tuning.json by default);
+        False when there is none (the library's built-in values stay)."""
+        import json
+        path = path or TUNING_PATH
+        if not os.path.exists(path):
+            return False
+        table = json.load(open(path))
+        for cls, t in table.get("classes", {}).items():
+            self.SetTuning(int(cls), int(t["front"]), int(t["ctas_per_sm"]), int(t["verify_chunk"]))
+        return True
+
+    def SetFrontWait(self, limitNs: int, addUnreachableWait: bool = False) -> None:
+        """Limit of one wait of the persistent front end; the flag appends a
+        wait that never ends to batches laid out afterwards (testing)."""
+        _check(L().przmg_set_front_wait(self._h, limitNs, 1 if addUnreachableWait else 0))
 
     def Close(self) -> None:
         """gpu/bridge.go:513"""
@@ -606,6 +639,12 @@ class DeviceBatch:
         out = np.zeros(max(len(self.sizes), 1), np.uint32)
         _check(L().przmg_batch_sizes(self._h, _ptr(out)))
         return out[: len(self.sizes)]
+
+    def info(self) -> dict[str, int]:
+        """front (1: the persistent front end), size_class, ctas_per_sm, verify_chunk."""
+        i = np.zeros(4, np.uint32)
+        _check(L().przmg_batch_info(self._h, _ptr(i)))
+        return {"front": int(i[0]), "size_class": int(i[1]), "ctas_per_sm": int(i[2]), "verify_chunk": int(i[3])}
 
     def launches(self) -> int:
         return int(L().przmg_batch_launch_count(self._h))
