@@ -19,6 +19,14 @@
 // block stops taking items once that bit is set (the host then reports
 // PRZMG_ERR_DEVICE).  The output bytes do not depend on which block runs
 // which item.
+//
+// An item's progress is published with a fence and an atomic add after the
+// block's barrier, and a waiting item reads it with ld.acquire.gpu before its
+// block's barrier.  Data that other blocks of the same launch wrote
+// (descriptors, radix lists and counts, tokenizer slots and tile lengths) is
+// read with ld.global.cg, which goes to L2, never through the non-coherent
+// read-only path, whose contents are only valid for data that no block of
+// the running kernel writes.
 #include "common.cuh"
 
 namespace pz {

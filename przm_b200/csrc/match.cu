@@ -181,7 +181,7 @@ __device__ void rx_scan_item(const Job* __restrict__ jobs, uint32_t j, uint32_t*
         const uint32_t nt = (rx_ncand(job.n) + kCandPerTile - 1) / kCandPerTile;
         uint32_t* cj = cnt + (uint64_t)job.tile0 * kRxParts + b;
         uint32_t total = 0;
-        for (uint32_t t = 0; t < nt; t++) total += cj[(uint64_t)t * kRxParts];
+        for (uint32_t t = 0; t < nt; t++) total += __ldcg(cj + (uint64_t)t * kRxParts);
         // exclusive scan of the partition totals
         uint32_t v = total;
 #pragma unroll
@@ -197,7 +197,7 @@ __device__ void rx_scan_item(const Job* __restrict__ jobs, uint32_t j, uint32_t*
         parts[(uint64_t)j * kRxParts + b] = make_uint2(start, total);
         uint32_t run = start;
         for (uint32_t t = 0; t < nt; t++) {
-            const uint32_t k = cj[(uint64_t)t * kRxParts];
+            const uint32_t k = __ldcg(cj + (uint64_t)t * kRxParts);
             cj[(uint64_t)t * kRxParts] = run;
             run += k;
         }
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(kRxParts) k_rx_scan(const Job* __restrict__ jo
 // in 16 rounds of 32; slots are assigned in position order.
 // One radix tile, block of 256; s_w = 8 x kRxParts words of shared memory.
 __device__ void rx_scatter_item(const uint8_t* __restrict__ in, const Job* __restrict__ jobs, const RxTile tt,
-                                const uint32_t* __restrict__ off, uint32_t* __restrict__ ent,
+                                const uint32_t* off, uint32_t* __restrict__ ent,
                                 uint16_t* __restrict__ key, uint32_t (*s_w)[kRxParts]) {
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t lt = (1u << lane) - 1u;
@@ -240,7 +240,7 @@ __device__ void rx_scatter_item(const uint8_t* __restrict__ in, const Job* __res
         }
         __syncthreads();
         for (uint32_t pt = tid; pt < kRxParts; pt += 256) {
-            uint32_t base = off[(uint64_t)(job.tile0 + tt.tile) * kRxParts + pt];
+            uint32_t base = __ldcg(off + (uint64_t)(job.tile0 + tt.tile) * kRxParts + pt);
             for (int w = 0; w < 8; w++) {
                 const uint32_t k = s_w[w][pt];
                 s_w[w][pt] = base;
@@ -318,14 +318,14 @@ bytes:
 
 // Partition b of large frame j, by one warp; table = kRxKeys words of
 // shared memory (latest candidate + 1 per key, 0 = none).
-__device__ void rx_resolve_warp(const Job* __restrict__ jobs, uint32_t j, uint32_t b, const uint2* __restrict__ parts,
-                                const uint32_t* __restrict__ ent, const uint16_t* __restrict__ key,
-                                uint32_t* __restrict__ pred, uint32_t* table) {
+__device__ void rx_resolve_warp(const Job* __restrict__ jobs, uint32_t j, uint32_t b, const uint2* parts,
+                                const uint32_t* ent, const uint16_t* key, uint32_t* __restrict__ pred,
+                                uint32_t* table) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
     {
         const Job job = jobs[j];
-        const uint2 pr = parts[(uint64_t)j * kRxParts + b];
+        const uint2 pr = __ldcg(parts + (uint64_t)j * kRxParts + b);
         if (pr.y == 0) return;
         for (uint32_t i = lane; i < kRxKeys / 4; i += 32) reinterpret_cast<uint4*>(table)[i] = make_uint4(0, 0, 0, 0);
         __syncwarp();
@@ -339,8 +339,8 @@ __device__ void rx_resolve_warp(const Job* __restrict__ jobs, uint32_t j, uint32
 #pragma unroll
             for (int u = 0; u < 8; u++) {
                 const uint32_t i = b0 + 32 * u + lane;
-                cc[u] = i < pr.y ? ej[i] : 0u;
-                kk[u] = i < pr.y ? kj[i] : 0xFFFFu;
+                cc[u] = i < pr.y ? __ldcg(ej + i) : 0u;
+                kk[u] = i < pr.y ? __ldcg(kj + i) : 0xFFFFu;
             }
 #pragma unroll
             for (int u = 0; u < 8; u++) {
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(kRxResolveWarps * 32) k_rx_resolve(const Job* 
 // nthr: two entries per thread per step, their first loads in flight
 // together.
 __device__ __forceinline__ void rx_verify_range(const uint8_t* __restrict__ in, const Job& job,
-                                                const uint32_t* __restrict__ ent, const uint32_t* __restrict__ pred,
+                                                const uint32_t* ent, const uint32_t* pred,
                                                 uint32_t* __restrict__ desc, uint32_t lo, uint32_t hi, uint32_t t,
                                                 uint32_t nthr) {
     {
@@ -396,8 +396,8 @@ __device__ __forceinline__ void rx_verify_range(const uint8_t* __restrict__ in, 
         for (uint32_t i = lo + t; i < C; i += 2 * stride) {
             const uint32_t i2 = i + stride;
             const bool two = i2 < C;
-            const uint32_t c1 = ej[i], p1 = pj[i];
-            const uint32_t c2 = two ? ej[i2] : 0u, p2 = two ? pj[i2] : 0u;
+            const uint32_t c1 = __ldcg(ej + i), p1 = __ldcg(pj + i);
+            const uint32_t c2 = two ? __ldcg(ej + i2) : 0u, p2 = two ? __ldcg(pj + i2) : 0u;
             uint64_t x1[4], x2[4];
             if (p1) rx_first(src, c1, p1 - 1, x1);
             if (p2) rx_first(src, c2, p2 - 1, x2);

@@ -135,13 +135,16 @@ __device__ __forceinline__ void hist4(uint32_t* h, uint32_t w) {
 }
 
 // 16 source bytes at sw + 4v, shifted right by sh bits (sh = 8 x the
-// source's offset from its 4-byte boundary).
-__device__ __forceinline__ uint4 ld16_shifted(const uint32_t* __restrict__ sw, uint32_t v, uint32_t sh) {
+// source's offset from its 4-byte boundary).  Loads go to L2 (ld.global.cg):
+// the gather reads slots that other blocks of the same persistent launch
+// wrote, which a non-coherent or L1-cached load could see stale.
+__device__ __forceinline__ uint4 ld16_shifted(const uint32_t* sw, uint32_t v, uint32_t sh) {
     const uint32_t* q = sw + 4 * v;
-    if (sh == 0) return make_uint4(q[0], q[1], q[2], q[3]);
-    const uint32_t w4 = q[4];
-    return make_uint4(__funnelshift_r(q[0], q[1], sh), __funnelshift_r(q[1], q[2], sh),
-                      __funnelshift_r(q[2], q[3], sh), __funnelshift_r(q[3], w4, sh));
+    const uint32_t w0 = __ldcg(q), w1 = __ldcg(q + 1), w2 = __ldcg(q + 2), w3 = __ldcg(q + 3);
+    if (sh == 0) return make_uint4(w0, w1, w2, w3);
+    const uint32_t w4 = __ldcg(q + 4);
+    return make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh), __funnelshift_r(w2, w3, sh),
+                      __funnelshift_r(w3, w4, sh));
 }
 
 // Copies n bytes s -> d with the warp and counts them into h (shared, may be
@@ -149,11 +152,11 @@ __device__ __forceinline__ uint4 ld16_shifted(const uint32_t* __restrict__ sw, u
 // four per lane in flight (source words loaded aligned and funnel-shifted, so
 // reading up to 3 bytes past s + n: slot blocks and inputs have room), then
 // the tail bytes.
-__device__ void warp_copy_hist(uint8_t* __restrict__ d, const uint8_t* __restrict__ s, uint32_t n,
-                               uint32_t* __restrict__ h, uint32_t lane) {
+__device__ void warp_copy_hist(uint8_t* __restrict__ d, const uint8_t* s, uint32_t n, uint32_t* __restrict__ h,
+                               uint32_t lane) {
     const uint32_t head = min(n, (uint32_t)((16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15));
     if (lane < head) {
-        const uint8_t b = s[lane];
+        const uint8_t b = __ldcg(s + lane);
         d[lane] = b;
         if (h) atomicAdd(&h[b], 1u);
     }
@@ -181,7 +184,7 @@ __device__ void warp_copy_hist(uint8_t* __restrict__ d, const uint8_t* __restric
         if (h) { hist4(h, o.x); hist4(h, o.y); hist4(h, o.z); hist4(h, o.w); }
     }
     for (uint32_t i = 16 * nv + lane; i < n; i += 32) {
-        const uint8_t b = s[i];
+        const uint8_t b = __ldcg(s + i);
         d[i] = b;
         if (h) atomicAdd(&h[b], 1u);
     }
@@ -324,7 +327,7 @@ __device__ void tok_emit(const uint4* rec, uint32_t nrec, const uint8_t* tile_sr
 
 // One 32 KiB tile, by one warp with its TokSmem.
 __device__ void tokenize_tile(const uint8_t* __restrict__ in, const Job* __restrict__ jobs, const TokTile tt,
-                              const uint32_t* __restrict__ desc, uint8_t* __restrict__ slots,
+                              const uint32_t* desc, uint8_t* __restrict__ slots,
                               uint32_t* __restrict__ tile_lens, uint32_t* __restrict__ err, TokSmem& sm) {
     const uint32_t lane = threadIdx.x & 31;
     {
@@ -363,7 +366,7 @@ __device__ void tokenize_tile(const uint8_t* __restrict__ in, const Job* __restr
                     const uint32_t e = base + 128 * (h + u) + 4 * lane;
                     v[u] = make_uint4(0u, 0u, 0u, 0u);
                     if (e < e_hi) {  // dj + e is 16-byte aligned; the array holds whole uint4s below e_hi
-                        v[u] = __ldg(reinterpret_cast<const uint4*>(dj + e));
+                        v[u] = __ldcg(reinterpret_cast<const uint4*>(dj + e));
                         if (e + 1 >= e_hi) v[u].y = 0;
                         if (e + 2 >= e_hi) v[u].z = 0;
                         if (e + 3 >= e_hi) v[u].w = 0;
@@ -451,7 +454,7 @@ __device__ void tokenize_tile(const uint8_t* __restrict__ in, const Job* __restr
             // lookahead (przm_tokenizer.cuh:196-216): radix frames have no
             // descriptor at q + 1
             if (!radix && q + 1 < end) {
-                const uint32_t nd = ent + 1 - wb < kTokWin ? sm.desc[ent + 1 - wb] : __ldg(dj + ent + 1);
+                const uint32_t nd = ent + 1 - wb < kTokWin ? sm.desc[ent + 1 - wb] : __ldcg(dj + ent + 1);
                 if (nd != 0 && (nd >> 20) > mLen + 1) { pos = q + 1; continue; }
             }
             // run-length token (:218-286)
@@ -613,8 +616,8 @@ constexpr uint32_t kGatherThreads = 512;
 
 // Frame j by the whole block (any multiple of 128 threads); s_off =
 // ntiles + 1 words, s_hist = [stream][warp group][symbol] counts.
-__device__ void gather_item(const Job* __restrict__ jobs, uint32_t j, const uint8_t* __restrict__ slots,
-                            const uint32_t* __restrict__ tile_lens, uint8_t* __restrict__ streams,
+__device__ void gather_item(const Job* __restrict__ jobs, uint32_t j, const uint8_t* slots,
+                            const uint32_t* tile_lens, uint8_t* __restrict__ streams,
                             uint32_t* __restrict__ job_lens, uint32_t* __restrict__ hist, uint32_t* __restrict__ err,
                             uint32_t* s_off, uint32_t (*s_hist)[4][256]) {
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nthr = blockDim.x;
@@ -632,7 +635,7 @@ __device__ void gather_item(const Job* __restrict__ jobs, uint32_t j, const uint
                     uint32_t i = b + lane;
                     // an empty input has no tokenizer tile: its one tile
                     // slot is never written, so its streams are empty
-                    uint32_t v = (i < job.ntiles && job.n > 0) ? tile_lens[(uint64_t)(job.tile0 + i) * S_COUNT + s] : 0;
+                    uint32_t v = (i < job.ntiles && job.n > 0) ? __ldcg(tile_lens + (uint64_t)(job.tile0 + i) * S_COUNT + s) : 0;
                     uint32_t x = v;
                     for (uint32_t o = 1; o < 32; o <<= 1) {
                         uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
