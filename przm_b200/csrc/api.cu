@@ -541,7 +541,7 @@ static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, cons
         const uint32_t grid = std::min<uint32_t>(R.nsmall, 8u * c->sms);
         k_tile_find<<<grid, 256, kTileFindSmem, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(),
                                                      b->d_small.as<TileRef>() + R.small0, R.nsmall,
-                                                     b->d_desc.as<uint32_t>());
+                                                     b->d_desc.as<uint32_t>(), b->err_word());
         CK(cudaGetLastError());
         launches++;
     }
@@ -668,6 +668,9 @@ static int32_t batch_launch_plain(przmg_batch* b, cudaStream_t s) {
 }
 
 static int32_t device_error(uint32_t err) {
+    if (err & E_COPY_TIMEOUT)
+        return fail(PRZMG_ERR_DEVICE, "a bulk copy into shared memory did not complete within its wait limit (error bits " +
+                                          std::to_string(err) + ")");
     if (err & E_SCHED_TIMEOUT)
         return fail(PRZMG_ERR_DEVICE, "a wait of the persistent front end ran past its limit (error bits " +
                                           std::to_string(err) + "); the batch's frames are not valid");

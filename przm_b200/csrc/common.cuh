@@ -35,7 +35,55 @@ enum Stream : int { S_CMD = 0, S_OP = 1, S_META = 2, S_VAR = 3, S_OFF = 4, S_LIT
 enum Task : int { T_LIT = 0, T_OP_M8 = 1, T_OP_AD = 2, T_META_M8 = 3, T_META_AD = 4, T_VAR_M8 = 5, T_VAR_AD = 6, T_COUNT = 7 };
 
 // error bits reported through the per-batch status word
-enum Err : uint32_t { E_SLOT_OVERFLOW = 1, E_STREAM_OVERFLOW = 2, E_BAD_TOKEN = 4, E_TABLE = 8 };
+enum Err : uint32_t { E_SLOT_OVERFLOW = 1, E_STREAM_OVERFLOW = 2, E_BAD_TOKEN = 4, E_TABLE = 8, E_COPY_TIMEOUT = 32 };
+
+// ---- bulk copies (the TMA engine's one-dimensional form) into this CTA's
+// shared memory, completed on an mbarrier.  Source and destination 16-byte
+// aligned, size a multiple of 16.  No multicast.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* m, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(m)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_inval(uint64_t* m) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_u32(m)) : "memory");
+}
+// expect `bytes` and start one bulk copy global -> shared that completes them
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* m) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(m))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* m, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(m)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for phase `parity`: false (and E_COPY_TIMEOUT in *err) when
+// the copy has not completed after 2^22 polls, far beyond a tile's copy time.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* m, uint32_t parity, uint32_t* err) {
+    for (uint32_t it = 0; it < (1u << 22); it++)
+        if (mbar_try_wait(m, parity)) return true;
+    atomicOr(err, (uint32_t)E_COPY_TIMEOUT);
+    return false;
+}
+
+// Load of data an earlier stage wrote.  When that stage ran in an earlier
+// launch the data is read-only for this one and goes through the read-only
+// path (kCoherent = false); inside the persistent front end the producing
+// stage may have run in the same launch, on another SM, so the load goes to
+// L2 (ld.global.cg), where the producer's writes are.
+template <bool kCoherent, class T>
+__device__ __forceinline__ T ld_stage(const T* p) {
+    if constexpr (kCoherent) return __ldcg(p);
+    else return __ldg(p);
+}
 
 struct Job {
     uint64_t in_off;    // input byte offset (16-byte aligned)
@@ -97,26 +145,17 @@ __host__ __device__ inline uint64_t ans_task_off(const Job& j, int t) {
 }
 __host__ __device__ inline uint64_t ans_region_bytes(const Job& j) { return ans_task_off(j, T_COUNT); }
 
-// Encoding table entry for one symbol of one model (frequency f, cumulative
-// frequency c).  The reference step on a state 2^16 <= x < 2^24 emits the
-// low byte of x while x >= 4096 f, then sets x = floor(x_r / f) * 4096 + c +
-// (x_r mod f) for the remaining x_r = x >> 8k.  k takes only two values per
-// symbol: 0 or 1 when f >= 16 (x < 2^24 <= 2^20 f), 1 or 2 when f < 16
-// (x >= 2^16 > 4096 f).  So k = kb + p with kb = (f < 16) and p = (x >= t),
-// and with d = f << 8 kb a single multiply-high gives both quotients:
-// floor(x / d) = umulhi(x, m) >> s exactly for every x < 2^24
-// (Granlund-Montgomery 1994 with s = max(0, ceil(log2 d) - 8)), and
-// floor(x / 256 d) = floor(x / d) >> 8.  The step is then
-//   x' = (umulhi(x, m) >> (s + 8p)) * (4096 - f) + (x >> (8 kb + 8p)) + c,
-// whose chain is compare | multiply-high -> shift -> multiply-add.
-//   m   : ceil(2^(32+s) / d)
-//   t   : 4096 f (f >= 16) or 2^20 f (f < 16): x >= t -> one more byte;
-//         2^32 - 1 for f = 4096 (never)
-//   cc  : c | (4096 - f) << 16
-//   sh  : s | (s + 8) << 8 | 8 kb << 16 | (8 kb + 8) << 24
-// f = 0 (a symbol that never occurs) gets t = 2^32 - 1 and zeros.
+// Encoding table entry for one symbol of one model:
+//   m   : 32-bit reciprocal so that floor(x_r / f) == umulhi(x_r, m) >> s for
+//         every x_r < 2^24 (Granlund-Montgomery 1994, round-up variant);
+//         f = 2^t uses m = 2^(32-t), s = 0; f = 1 uses m = 2^32-1 (one short)
+//         with the deficit folded into cb.
+//   t1  : 4096 * f, the renormalisation bound (x >= t1 -> emit a byte)
+//   t2  : 256 * t1 saturated to 2^32-1 (x >= t2 -> emit a second byte)
+//   w   : cb | (4096 - f) << 13 | s << 25, cb = cumulative frequency c
+//         (+4095 when f == 1)
 struct __align__(16) EncSym {
-    uint32_t m, t, cc, sh;
+    uint32_t m, t1, t2, w;
 };
 
 // Per-task results of the rANS kernel.

@@ -6,52 +6,28 @@
 namespace pz {
 
 // ---------------------------------------------------------------------------
-// Encoding tables.  The step x' = x_r + c + floor(x_r / f) * (M - f) with the
-// quotient from a multiply-high by a per-symbol reciprocal is the
-// reciprocal-encoder form of rANS that F. Giesen published with ryg_rans
-// (rans_byte.h, RansEncSymbolInit / RansEncPutSymbol, 2014); the reciprocal
-// is Granlund-Montgomery's (PLDI 1994).  Here the divisor folds in the
-// renormalisation shift (see EncSym), so one reciprocal serves both byte
-// counts a symbol can emit.
+// Encoding tables.  The step x' = x + bias + floor(x / f) * (M - f) with the
+// quotient from a multiply-high by a per-symbol reciprocal, and the f = 1
+// case done as a one-short reciprocal with the deficit moved into the bias,
+// is the reciprocal-encoder form of rANS that F. Giesen published with
+// ryg_rans (rans_byte.h, RansEncSymbolInit / RansEncPutSymbol, 2014); the
+// reciprocal itself is Granlund-Montgomery's (PLDI 1994).
 // ---------------------------------------------------------------------------
-#ifndef PRZM_RANS_FORM
-#define PRZM_RANS_FORM 1
-#endif
-#if PRZM_RANS_FORM == 0
-// (experimental switch) renormalise first, then divide by f: fields
-// m = reciprocal of f, t = 4096 f, cc = 2^20 f (saturated), sh = cb | cf << 13 | s << 25
 __host__ __device__ inline EncSym make_encsym(uint32_t f, uint32_t c) {
     EncSym e;
-    if (f == 0) { e.m = 0; e.t = 0xFFFFFFFFu; e.cc = 0xFFFFFFFFu; e.sh = 0; return e; }
+    if (f == 0) { e.m = 0; e.t1 = 0xFFFFFFFFu; e.t2 = 0xFFFFFFFFu; e.w = 0; return e; }
     uint32_t s = 0;
     while ((2u << s) <= f) s++;  // floor(log2 f)
     uint32_t cb = c;
     if (f == 1) { e.m = 0xFFFFFFFFu; s = 0; cb = c + 4095; }
     else if ((f & (f - 1)) == 0) { e.m = 1u << (32 - s); s = 0; }
     else e.m = (uint32_t)(((1ull << (32 + s)) + f - 1) / f);
-    e.t = 4096u * f;
-    const uint64_t t2 = 256ull * e.t;
-    e.cc = t2 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)t2;
-    e.sh = cb | ((4096u - f) << 13) | (s << 25);
+    e.t1 = 4096u * f;
+    const uint64_t t2 = 256ull * e.t1;
+    e.t2 = t2 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)t2;
+    e.w = cb | ((4096u - f) << 13) | (s << 25);
     return e;
 }
-#else
-__host__ __device__ inline EncSym make_encsym(uint32_t f, uint32_t c) {
-    EncSym e;
-    if (f == 0) { e.m = 0; e.t = 0xFFFFFFFFu; e.cc = 0; e.sh = 0; return e; }
-    const uint32_t kb = f < 16 ? 1u : 0u;
-    const uint64_t d = (uint64_t)f << (8 * kb);  // 16 <= d <= 4096
-    uint32_t lg = 0;
-    while ((1ull << lg) < d) lg++;  // ceil(log2 d)
-    const uint32_t s = lg > 8 ? lg - 8 : 0;
-    // x * (m d - 2^(32+s)) < 2^24 d <= 2^(32+s) for every x < 2^24
-    e.m = (uint32_t)(((1ull << (32 + s)) + d - 1) / d);
-    e.t = f == 4096 ? 0xFFFFFFFFu : (kb ? (f << 20) : 4096u * f);
-    e.cc = c | ((4096u - f) << 16);
-    e.sh = s | ((s + 8) << 8) | ((8 * kb) << 16) | ((8 * kb + 8) << 24);
-    return e;
-}
-#endif
 
 // SerializeMatrix (gpu/bridge.go:2844-2886) == EncodeJointNibbleFreq
 // (core/literals/literals.go:143-184).
@@ -357,86 +333,40 @@ __global__ void k_normalize(const Job* __restrict__ jobs, uint32_t j0, uint32_t 
 // The division is a multiply-high by a per-symbol reciprocal (exact for
 // x < 2^24, see EncSym).
 // ---------------------------------------------------------------------------
-// A lane's records: per round j the low byte of x before the step at lo[j]
-// (the byte every emitting round writes first), and the second byte at
-// hi[j] -- stored only for the groups of 16 rounds in which some round emits
-// two bytes (a symbol with f < 16 at a large state), so most groups cost 16
-// bytes of records instead of 32.
 struct LaneIO {
-    uint8_t* lo;        // low bytes, one per round
-    uint8_t* hi;        // second bytes, one per round (written where a group has a k = 2 round)
+    uint8_t* bytes;     // lane byte stream
     uint32_t* nbw;      // 2-bit emitted-byte counts, 16 rounds per word (round j -> word j/16)
     uint32_t* cum;      // cum[k]: bytes of rounds >= kStitchRounds k (written where the lane has round kStitchRounds k)
 };
 
-// half of a lane region: ceil(L / 4) + 64 rounds or more, a multiple of 32
-__host__ __device__ constexpr uint64_t ans_lane_half(uint32_t L) { return ans_lane_cap(L) / 2; }
-
 __device__ __forceinline__ LaneIO lane_io(uint8_t* task_base, uint32_t cap, uint32_t l) {
     LaneIO io;
-    io.lo = task_base + (uint64_t)l * ans_lane_cap(cap);
-    io.hi = io.lo + ans_lane_half(cap);
+    io.bytes = task_base + (uint64_t)l * ans_lane_cap(cap);
     io.nbw = reinterpret_cast<uint32_t*>(task_base + 4 * ans_lane_cap(cap)) + (uint64_t)l * ans_nbw_cap(cap);
     io.cum = io.nbw + ans_nbw_words(cap);
     return io;
 }
 
-// byte b (0 or 1) of four u16 records as one word
-__device__ __forceinline__ uint32_t pack4(const uint32_t* r, uint32_t b) {
-    const uint32_t sel = b ? 0x0051u : 0x0040u;
-    return __byte_perm(__byte_perm(r[0], r[1], sel), __byte_perm(r[2], r[3], sel), 0x5410u);
-}
-
 // One rANS step (table entry e of the symbol already in registers): returns
-// the number k = kb + p of low bytes of x the reference would emit, and
-// advances x.  The caller keeps the low 16 bits of x from before the step;
-// its first k bytes (low byte first) are what the reference writes.  The
-// multiply-high runs on x itself, beside the compare that picks the shifts
-// (see EncSym), so the dependent chain per step is multiply-high -> shift ->
-// multiply-add.
-#if PRZM_RANS_FORM == 0
+// the number k of low bytes of x the reference would emit (x >= 4096 f, and
+// again when x >= 2^20 f), and advances x.  The caller keeps the low 16 bits
+// of x from before the step; its first k bytes (low byte first) are what the
+// reference writes.  x < 2^24 throughout, so x >= t2 can only hold for f < 16.
+// The renormalised state is selected first and divided once: computing the
+// three candidates (0, 1 or 2 bytes shifted out) side by side and selecting
+// last keeps the compares off the multiply's chain, but its extra
+// instructions made the kernel slower (7.68 vs 7.45 ms on the 256 x 1 MiB
+// mixed batch).
 __device__ __forceinline__ uint32_t rans_next(uint32_t x, const EncSym& e) {
-    const uint32_t s = e.sh >> 25, cf = (e.sh >> 13) & 0xFFFu, cb = e.sh & 0x1FFFu;
-    const uint32_t xs = x >= e.cc ? (x >> 16) : (x >= e.t ? (x >> 8) : x);
+    const uint32_t s = e.w >> 25, cf = (e.w >> 13) & 0xFFFu, cb = e.w & 0x1FFFu;
+    const uint32_t xs = x >= e.t2 ? (x >> 16) : (x >= e.t1 ? (x >> 8) : x);
     return xs + cb + (__umulhi(xs, e.m) >> s) * cf;
 }
 __device__ __forceinline__ uint32_t rans_step(uint32_t& x, const EncSym& e) {
-    const uint32_t k = (uint32_t)(x >= e.t) + (uint32_t)(x >= e.cc);
+    const uint32_t k = (uint32_t)(x >= e.t1) + (uint32_t)(x >= e.t2);
     x = rans_next(x, e);
     return k;
 }
-// count bits of a round: a = first byte, b = second byte (b implies a)
-__device__ __forceinline__ void rans_kbits(uint32_t x, const EncSym& e, bool& a, bool& b) { a = x >= e.t; b = x >= e.cc; }
-#else
-#if PRZM_RANS_FORM == 2
-__device__ __forceinline__ uint32_t rans_next(uint32_t x, const EncSym& e) {
-    const bool p = x >= e.t;
-    const uint32_t h = __umulhi(x, e.m), c = e.cc & 0xFFFFu, cf = e.cc >> 16;
-    const uint32_t a = (h >> (e.sh & 0xFFu)) * cf + (x >> ((e.sh >> 16) & 0xFFu)) + c;
-    const uint32_t b = (h >> ((e.sh >> 8) & 0xFFu)) * cf + (x >> (e.sh >> 24)) + c;
-    return p ? b : a;
-}
-#else
-__device__ __forceinline__ uint32_t rans_next(uint32_t x, const EncSym& e) {
-    const bool p = x >= e.t;
-    const uint32_t q = __umulhi(x, e.m) >> (p ? ((e.sh >> 8) & 0xFFu) : (e.sh & 0xFFu));
-    return q * (e.cc >> 16) + (x >> (p ? (e.sh >> 24) : ((e.sh >> 16) & 0xFFu))) + (e.cc & 0xFFFFu);
-}
-
-#endif
-__device__ __forceinline__ uint32_t enc_kb(const EncSym& e) { return (e.sh >> 19) & 1u; }
-__device__ __forceinline__ uint32_t rans_step(uint32_t& x, const EncSym& e) {
-    const uint32_t k = enc_kb(e) + (uint32_t)(x >= e.t);
-    x = rans_next(x, e);
-    return k;
-}
-// count bits of a round: k = a + b with b implying a
-__device__ __forceinline__ void rans_kbits(uint32_t x, const EncSym& e, bool& a, bool& b) {
-    const bool p = x >= e.t, kb = enc_kb(e) != 0;
-    a = p || kb;
-    b = p && kb;
-}
-#endif
 
 // Table index of round r of a 16-round group (words w, group g, lane l).
 template <bool kMeta8>
@@ -460,24 +390,23 @@ __device__ __forceinline__ void words16(const uint4* c, uint32_t* w) {
 
 // The 16 chain steps of one full group with the entries already in
 // registers; writes the group's records and its 2-bit count word.
-__device__ __forceinline__ void encode_group(uint32_t& x, uint32_t& cnt, const EncSym* e, int32_t g, uint4* lo4,
-                                             uint4* hi4, uint32_t* nbw) {
+__device__ __forceinline__ void encode_group(uint32_t& x, uint32_t& cnt, const EncSym* e, int32_t g, uint4* r4,
+                                             uint32_t* nbw) {
     uint32_t rec[16], m1 = 0, m2 = 0;
 #pragma unroll
     for (int r = 15; r >= 0; r--) {
         rec[r] = x & 0xFFFFu;
-        bool a, b;
-        rans_kbits(x, e[r], a, b);
-        m1 |= a ? (1u << r) : 0u;
-        m2 |= b ? (1u << r) : 0u;
+        m1 |= x >= e[r].t1 ? (1u << r) : 0u;
+        m2 |= x >= e[r].t2 ? (1u << r) : 0u;
         x = rans_next(x, e[r]);
     }
-    // k = a + b with b => a: bit 0 = a ^ b, bit 1 = b
-    const uint32_t two = m2;
-    nbw[g] = spread16(m1 ^ m2) | (spread16(two) << 1);
+    // k = p1 + p2 with p2 => p1: bit 0 = p1 ^ p2, bit 1 = p2
+    nbw[g] = spread16(m1 ^ m2) | (spread16(m2) << 1);
     cnt += __popc(m1) + __popc(m2);
-    lo4[g] = make_uint4(pack4(rec, 0), pack4(rec + 4, 0), pack4(rec + 8, 0), pack4(rec + 12, 0));
-    if (two) hi4[g] = make_uint4(pack4(rec, 1), pack4(rec + 4, 1), pack4(rec + 8, 1), pack4(rec + 12, 1));
+    r4[2 * g] = make_uint4(rec[0] | (rec[1] << 16), rec[2] | (rec[3] << 16), rec[4] | (rec[5] << 16),
+                           rec[6] | (rec[7] << 16));
+    r4[2 * g + 1] = make_uint4(rec[8] | (rec[9] << 16), rec[10] | (rec[11] << 16), rec[12] | (rec[13] << 16),
+                               rec[14] | (rec[15] << 16));
 }
 
 // ---- per-lane symbol ring: cp.async copies of the 64-byte groups ---------
@@ -505,10 +434,9 @@ __device__ __forceinline__ void ring_read(const uint4* ring, uint32_t t, int32_t
 }
 
 // Encodes lane l of one task.  Symbols of lane l are i = 4j + l, rounds j
-// from the top down.  Per round the lane stores the low byte of x before the
-// step at lo[j] (and its second byte at hi[j] where the round's group needs
-// it) and the byte count k in 2 bits of nbw[j / 16]; the stitch turns the
-// records and counts back into the reference byte order.  Rounds come in
+// from the top down.  Per round the lane stores the 16 low bits of x before
+// the step at raw[j] and the byte count k in 2 bits of nbw[j / 16]; the
+// stitch turns (raw, k) back into the reference byte order.  Rounds come in
 // groups of 16 (the 64 source bytes 64g .. 64g + 63 hold the four lanes'
 // symbols); the rounds above the G = n / 64 full groups take the byte path.
 // Full groups stream through the thread's ring: the 64 bytes of group g - 4
@@ -520,6 +448,7 @@ __device__ __forceinline__ void rans_lane(const uint8_t* __restrict__ src, uint3
                                           const EncSym* __restrict__ tab, const uint8_t* __restrict__ ctxlut,
                                           uint4* ring, LaneIO io, uint32_t* out_state, uint32_t* out_count) {
     uint32_t x = 65536, cnt = 0;
+    uint16_t* raw = reinterpret_cast<uint16_t*>(io.bytes);
     const uint32_t t = threadIdx.x & 31;
     if (n > l) {
         const uint32_t J = (n - 1 - l) >> 2;
@@ -531,8 +460,7 @@ __device__ __forceinline__ void rans_lane(const uint8_t* __restrict__ src, uint3
                 const uint32_t i = 4u * (uint32_t)j + l;
                 uint32_t ti = src[i];
                 if (kMeta8) ti |= (i ? (uint32_t)ctxlut[src[i - 1]] : 0u) << 8;
-                io.lo[j] = (uint8_t)x;
-                io.hi[j] = (uint8_t)(x >> 8);
+                raw[j] = (uint16_t)x;
                 const uint32_t k = rans_step(x, tab[ti]);
                 cnt += k;
                 acc |= k << (2 * (j & 15));
@@ -545,8 +473,7 @@ __device__ __forceinline__ void rans_lane(const uint8_t* __restrict__ src, uint3
         }
         if (G > 0) {
             const uint4* s4 = reinterpret_cast<const uint4*>(src);
-            uint4* lo4 = reinterpret_cast<uint4*>(io.lo);
-            uint4* hi4 = reinterpret_cast<uint4*>(io.hi);
+            uint4* r4 = reinterpret_cast<uint4*>(raw);
             const uint32_t sel = 0x4440u | l;               // __byte_perm selector of byte l
             const uint32_t selp = 0x4440u | ((l + 3) & 3);  // byte l-1 (used for l >= 1)
             // prologue: groups G-1 .. G-kRing (clamped at 0), one commit group each
@@ -569,7 +496,7 @@ __device__ __forceinline__ void rans_lane(const uint8_t* __restrict__ src, uint3
                 }
                 // the slot of group g is free once its words are in registers
                 ring_fetch(ring, t, g, s4, max(g - kRing, 0));
-                encode_group(x, cnt, e, g, lo4, hi4, io.nbw);
+                encode_group(x, cnt, e, g, r4, io.nbw);
                 if ((g & (kStitchRounds / 16 - 1)) == 0) io.cum[g / (kStitchRounds / 16)] = cnt;
 #pragma unroll
                 for (int v = 0; v < 4; v++) cur[v] = nxt[v];
@@ -761,10 +688,11 @@ __device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s_warp, uint32_t&
     return base + x - v;
 }
 
-// Byte r (0..15) of a uint4.
-__device__ __forceinline__ uint32_t byte16(const uint4& q, int r) {
-    const uint32_t w = (r >> 2) == 0 ? q.x : (r >> 2) == 1 ? q.y : (r >> 2) == 2 ? q.z : q.w;
-    return (w >> (8 * (r & 3))) & 0xFFu;
+// Byte r (0..15) of the 16 u16 records held in two uint4.
+__device__ __forceinline__ uint32_t rec16(const uint4* v, int r) {
+    const uint4 q = v[r >> 3];
+    const uint32_t w = ((r >> 1) & 3) == 0 ? q.x : ((r >> 1) & 3) == 1 ? q.y : ((r >> 1) & 3) == 2 ? q.z : q.w;
+    return (r & 1) ? (w >> 16) : (w & 0xFFFFu);
 }
 
 // Bytes a stitch pass of NT threads x 16 rounds can produce (8 per round).
@@ -787,24 +715,24 @@ __device__ uint32_t stitch_pass(const uint8_t* task_base, uint32_t cap, uint32_t
     const uint32_t rounds = (n + 3) / 4;
     const uint32_t rb = r0 + 16 * tid;  // first round of this thread (multiple of 16)
     uint32_t w[4] = {0, 0, 0, 0}, c = 0;
-    uint4 rlo[4], rhi[4];
+    uint4 rv[4][2];
 #pragma unroll
     for (uint32_t l = 0; l < 4; l++) {
-        rlo[l] = rhi[l] = make_uint4(0, 0, 0, 0);
+        rv[l][0] = rv[l][1] = make_uint4(0, 0, 0, 0);
         if (rb >= rounds || n <= l) continue;
         const uint32_t jmax = (n - 1 - l) / 4;
         if (rb > jmax) continue;
-        const uint8_t* lo = task_base + (uint64_t)l * ans_lane_cap(cap);
+        const uint16_t* raw = reinterpret_cast<const uint16_t*>(task_base + (uint64_t)l * ans_lane_cap(cap));
         const uint32_t* nw = reinterpret_cast<const uint32_t*>(task_base + 4 * ans_lane_cap(cap)) + (uint64_t)l * ans_nbw_cap(cap);
         uint32_t v = nw[rb >> 4];
         const uint32_t top = jmax - rb;  // rounds of this word the lane has
         if (top < 15) v &= (1u << (2 * (top + 1))) - 1u;
         w[l] = v;
         c += sum2(v);
-        // rounds past jmax are in the lane region (each half holds ceil(cap/4) + 64 records) and masked by w;
-        // the second bytes are read only where a round emits two
-        rlo[l] = *reinterpret_cast<const uint4*>(lo + rb);
-        if (v & 0xAAAAAAAAu) rhi[l] = *reinterpret_cast<const uint4*>(lo + ans_lane_half(cap) + rb);
+        // rounds past jmax are in the lane region (it holds ceil(cap/4) + 64 records) and masked by w
+        const uint4* rp = reinterpret_cast<const uint4*>(raw + rb);
+        rv[l][0] = rp[0];
+        rv[l][1] = rp[1];
     }
     uint32_t total;
     const uint32_t excl = block_exclusive_scan<NT>(c, s_warp, total);
@@ -816,9 +744,9 @@ __device__ uint32_t stitch_pass(const uint8_t* task_base, uint32_t cap, uint32_t
         for (int l = 0; l < 4; l++) {
             const uint32_t k = (w[l] >> (2 * r)) & 3u;
             if (!k) continue;
-            const uint32_t v = byte16(rlo[l], r);
+            const uint32_t v = rec16(rv[l], r);
             if (k == 2) {
-                s_stage[q] = (uint8_t)byte16(rhi[l], r);
+                s_stage[q] = (uint8_t)(v >> 8);
                 s_stage[q + 1] = (uint8_t)v;
                 q += 2;
             } else {

@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kFrontThreads, 3) k_front(const FrontArgs a) {
                 if (lane == 0) go = front_wait(a.progress + tt.job, a.tok_target[tt.job], a.err, a.wait_cycles) ? 1u : 0u;
                 go = __shfl_sync(0xFFFFFFFFu, go, 0);
                 if (go) {
-                    tokenize_tile(a.in, a.jobs, tt, a.desc, a.slots, a.tile_lens, a.err,
+                    tokenize_tile<true>(a.in, a.jobs, tt, a.desc, a.slots, a.tile_lens, a.err,
                                   reinterpret_cast<TokSmem*>(smem_f)[warp]);
                     __syncwarp();
                     if (lane == 0) front_signal(a.progress + tt.job);
@@ -150,30 +150,30 @@ __global__ void __launch_bounds__(kFrontThreads, 3) k_front(const FrontArgs a) {
         if (!s_go) continue;
         switch (fi.stage) {
             case FS_TILE_FIND:
-                tile_find_item(a.in, a.jobs, a.small[fi.idx], a.desc, smem_f);
+                tile_find_item(a.in, a.jobs, a.small[fi.idx], a.desc, smem_f, a.err);
                 break;
             case FS_RX_COUNT:
                 rx_count_item(a.in, a.jobs, a.rtiles[fi.idx], a.rx_cnt, reinterpret_cast<uint32_t*>(smem_f));
                 break;
             case FS_RX_SCAN:
-                rx_scan_item(a.jobs, fi.idx, a.rx_cnt, a.rx_parts, reinterpret_cast<uint32_t*>(smem_f));
+                rx_scan_item<true>(a.jobs, fi.idx, a.rx_cnt, a.rx_parts, reinterpret_cast<uint32_t*>(smem_f));
                 break;
             case FS_RX_SCATTER:
-                rx_scatter_item(a.in, a.jobs, a.rtiles[fi.idx], a.rx_cnt, a.rx_ent, a.rx_key,
+                rx_scatter_item<true>(a.in, a.jobs, a.rtiles[fi.idx], a.rx_cnt, a.rx_ent, a.rx_key,
                                 reinterpret_cast<uint32_t(*)[kRxParts]>(smem_f));
                 break;
             case FS_RX_RESOLVE:
-                rx_resolve_warp(a.jobs, fi.job, fi.idx + warp, a.rx_parts, a.rx_ent, a.rx_key, a.rx_pred,
+                rx_resolve_warp<true>(a.jobs, fi.job, fi.idx + warp, a.rx_parts, a.rx_ent, a.rx_key, a.rx_pred,
                                 reinterpret_cast<uint32_t*>(smem_f) + warp * kRxKeys);
                 break;
             case FS_RX_VERIFY: {
                 const Job job = a.jobs[fi.job];
                 const uint32_t hi = min(rx_ncand(job.n), fi.idx + a.verify_chunk);
-                rx_verify_range(a.in, job, a.rx_ent, a.rx_pred, a.desc, fi.idx, hi, tid, kFrontThreads);
+                rx_verify_range<true>(a.in, job, a.rx_ent, a.rx_pred, a.desc, fi.idx, hi, tid, kFrontThreads);
                 break;
             }
             case FS_GATHER:
-                gather_item(a.jobs, fi.idx, a.slots, a.tile_lens, a.streams, a.job_lens, a.hist, a.err,
+                gather_item<true>(a.jobs, fi.idx, a.slots, a.tile_lens, a.streams, a.job_lens, a.hist, a.err,
                             reinterpret_cast<uint32_t*>(smem_f) + 4 * 4 * 256,
                             reinterpret_cast<uint32_t(*)[4][256]>(smem_f));
                 break;

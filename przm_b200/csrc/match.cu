@@ -11,14 +11,33 @@ __device__ __forceinline__ uint32_t hash4(uint32_t w) { return ((w * kHashPrime)
 
 // Exact common-prefix length of two shared-memory byte runs that are known to
 // agree on their first 4 bytes, capped at limit (przm_lz77.cu:63-85).
+// 16 bytes of a 4-byte aligned shared buffer from byte i, as four words
+// (five aligned loads, funnel-shifted; the buffer is padded by 32 bytes).
+__device__ __forceinline__ void ld128_smem_u(const uint8_t* base, uint32_t i, uint32_t* o) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(base) + (i >> 2);
+    const uint32_t sh = (i & 3) * 8;
+    const uint32_t w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3], w4 = w[4];
+    o[0] = __funnelshift_r(w0, w1, sh);
+    o[1] = __funnelshift_r(w1, w2, sh);
+    o[2] = __funnelshift_r(w2, w3, sh);
+    o[3] = __funnelshift_r(w3, w4, sh);
+}
+
+// Exact common-prefix length of two shared-memory byte runs that are known to
+// agree on their first 4 bytes, capped at limit (przm_lz77.cu:63-85), 16
+// bytes per step.  Reads stay below a + limit + 20 (inside the tile's pad).
 __device__ __forceinline__ uint32_t lcp_smem(const uint8_t* t, uint32_t a, uint32_t b, uint32_t limit) {
-    uint32_t len = 4;
-    while (len < limit) {
-        uint32_t d = ld32_smem_u(t, a + len) ^ ld32_smem_u(t, b + len);
-        if (d) { len += (uint32_t)(__ffs(d) - 1) >> 3; break; }
-        len += 4;
+    for (uint32_t len = 4; len < limit; len += 16) {
+        uint32_t x[4], y[4];
+        ld128_smem_u(t, a + len, x);
+        ld128_smem_u(t, b + len, y);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint32_t d = x[k] ^ y[k];
+            if (d) return min(limit, len + 4 * k + ((uint32_t)(__ffs(d) - 1) >> 3));
+        }
     }
-    return len < limit ? len : limit;
+    return limit;
 }
 
 // ---------------------------------------------------------------------------
@@ -29,13 +48,17 @@ __device__ __forceinline__ uint32_t lcp_smem(const uint8_t* t, uint32_t a, uint3
 // its previous head when one position hit it (low half).
 // ---------------------------------------------------------------------------
 struct TileRef { uint32_t job; uint32_t tile; };
-constexpr uint32_t kTileFindSmem = kTile + 16 + 3 * kBuckets * 4;
+// shared layout: tile + 32 bytes of pad, the copy's mbarrier (16), then the
+// three bucket arrays
+constexpr uint32_t kTilePad = 32;
+constexpr uint32_t kTileFindSmem = kTile + kTilePad + 16 + 3 * kBuckets * 4;
 
 // One tile, by a block of 256 threads; smem = kTileFindSmem bytes.
 __device__ void tile_find_item(const uint8_t* __restrict__ in, const Job* __restrict__ jobs, const TileRef ref,
-                               uint32_t* __restrict__ desc, uint8_t* smem_tf) {
-    uint8_t* s_tile = smem_tf;                                          // kTile + 16
-    uint32_t* s_head = reinterpret_cast<uint32_t*>(smem_tf + kTile + 16); // kBuckets each
+                               uint32_t* __restrict__ desc, uint8_t* smem_tf, uint32_t* err) {
+    uint8_t* s_tile = smem_tf;                                                      // kTile + kTilePad
+    uint64_t* s_bar = reinterpret_cast<uint64_t*>(smem_tf + kTile + kTilePad);     // copy completion
+    uint32_t* s_head = reinterpret_cast<uint32_t*>(smem_tf + kTile + kTilePad + 16);  // kBuckets each
     uint32_t* s_top = s_head + kBuckets;
     uint32_t* s_sec = s_top + kBuckets;
     const uint32_t tid = threadIdx.x, lane = tid & 31;
@@ -46,13 +69,18 @@ __device__ void tile_find_item(const uint8_t* __restrict__ in, const Job* __rest
         const uint8_t* src = in + job.in_off + ts;
         uint32_t* out = desc + job.desc_off + ts;
         __syncthreads();
-        // stage the tile (16-byte vectors; the input region is padded)
+        // stage the tile with one bulk copy (src: in_off is 16-byte aligned,
+        // tiles are 32 KiB apart; the input region is padded past n, so the
+        // copy may round up to 16 bytes) while the buckets are cleared
         const uint32_t nv = (tl + 15) / 16;
-        for (uint32_t v = tid; v < nv; v += 256)
-            reinterpret_cast<uint4*>(s_tile)[v] = __ldg(reinterpret_cast<const uint4*>(src) + v);
-        if (tid < 4) reinterpret_cast<uint32_t*>(s_tile)[(nv * 16) / 4 + tid] = 0;
-        for (uint32_t h = tid; h < kBuckets; h += 256) { s_head[h] = 0; s_top[h] = 0; s_sec[h] = 0; }
+        if (tid == 0) mbar_init(s_bar, 1);
         __syncthreads();
+        if (tid == 0) bulk_load(s_tile, src, nv * 16, s_bar);
+        if (tid < kTilePad / 4) reinterpret_cast<uint32_t*>(s_tile)[(nv * 16) / 4 + tid] = 0;
+        for (uint32_t h = tid; h < kBuckets; h += 256) { s_head[h] = 0; s_top[h] = 0; s_sec[h] = 0; }
+        mbar_wait_bounded(s_bar, 0, err);
+        __syncthreads();
+        if (tid == 0) mbar_inval(s_bar);
         const uint32_t steps = (tl + 255) / 256;
         for (uint32_t st = 0; st < steps; st++) {
             const uint32_t p = st * 256 + tid;
@@ -107,9 +135,9 @@ __device__ void tile_find_item(const uint8_t* __restrict__ in, const Job* __rest
 
 __global__ void __launch_bounds__(256) k_tile_find(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
                                                    const TileRef* __restrict__ refs, uint32_t nrefs,
-                                                   uint32_t* __restrict__ desc) {
+                                                   uint32_t* __restrict__ desc, uint32_t* __restrict__ err) {
     extern __shared__ __align__(16) uint8_t smem_tf[];
-    for (uint32_t r = blockIdx.x; r < nrefs; r += gridDim.x) tile_find_item(in, jobs, refs[r], desc, smem_tf);
+    for (uint32_t r = blockIdx.x; r < nrefs; r += gridDim.x) tile_find_item(in, jobs, refs[r], desc, smem_tf, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -173,6 +201,7 @@ __global__ void __launch_bounds__(256) k_rx_count(const uint8_t* __restrict__ in
 // Turns the per-tile counts into per-tile starting slots (in place) and
 // writes the partition's (start, length) pair.
 // One large frame j, block of kRxParts (256) threads; s_warp = 8 words.
+template <bool kC>
 __device__ void rx_scan_item(const Job* __restrict__ jobs, uint32_t j, uint32_t* __restrict__ cnt,
                              uint2* __restrict__ parts, uint32_t* s_warp) {
     const uint32_t b = threadIdx.x, lane = b & 31, warp = b >> 5;
@@ -181,7 +210,7 @@ __device__ void rx_scan_item(const Job* __restrict__ jobs, uint32_t j, uint32_t*
         const uint32_t nt = (rx_ncand(job.n) + kCandPerTile - 1) / kCandPerTile;
         uint32_t* cj = cnt + (uint64_t)job.tile0 * kRxParts + b;
         uint32_t total = 0;
-        for (uint32_t t = 0; t < nt; t++) total += __ldcg(cj + (uint64_t)t * kRxParts);
+        for (uint32_t t = 0; t < nt; t++) total += ld_stage<kC>(cj + (uint64_t)t * kRxParts);
         // exclusive scan of the partition totals
         uint32_t v = total;
 #pragma unroll
@@ -197,7 +226,7 @@ __device__ void rx_scan_item(const Job* __restrict__ jobs, uint32_t j, uint32_t*
         parts[(uint64_t)j * kRxParts + b] = make_uint2(start, total);
         uint32_t run = start;
         for (uint32_t t = 0; t < nt; t++) {
-            const uint32_t k = __ldcg(cj + (uint64_t)t * kRxParts);
+            const uint32_t k = ld_stage<kC>(cj + (uint64_t)t * kRxParts);
             cj[(uint64_t)t * kRxParts] = run;
             run += k;
         }
@@ -208,12 +237,13 @@ __global__ void __launch_bounds__(kRxParts) k_rx_scan(const Job* __restrict__ jo
                                                       uint32_t nbig, uint32_t* __restrict__ cnt,
                                                       uint2* __restrict__ parts) {
     __shared__ uint32_t s_warp[kRxParts / 32];
-    for (uint32_t x = blockIdx.x; x < nbig; x += gridDim.x) rx_scan_item(jobs, big[x], cnt, parts, s_warp);
+    for (uint32_t x = blockIdx.x; x < nbig; x += gridDim.x) rx_scan_item<false>(jobs, big[x], cnt, parts, s_warp);
 }
 
 // 8 warps per tile, warp w taking candidates [c0 + 512w, c0 + 512w + 512)
 // in 16 rounds of 32; slots are assigned in position order.
 // One radix tile, block of 256; s_w = 8 x kRxParts words of shared memory.
+template <bool kC>
 __device__ void rx_scatter_item(const uint8_t* __restrict__ in, const Job* __restrict__ jobs, const RxTile tt,
                                 const uint32_t* off, uint32_t* __restrict__ ent,
                                 uint16_t* __restrict__ key, uint32_t (*s_w)[kRxParts]) {
@@ -240,7 +270,7 @@ __device__ void rx_scatter_item(const uint8_t* __restrict__ in, const Job* __res
         }
         __syncthreads();
         for (uint32_t pt = tid; pt < kRxParts; pt += 256) {
-            uint32_t base = __ldcg(off + (uint64_t)(job.tile0 + tt.tile) * kRxParts + pt);
+            uint32_t base = ld_stage<kC>(off + (uint64_t)(job.tile0 + tt.tile) * kRxParts + pt);
             for (int w = 0; w < 8; w++) {
                 const uint32_t k = s_w[w][pt];
                 s_w[w][pt] = base;
@@ -271,7 +301,7 @@ __global__ void __launch_bounds__(256) k_rx_scatter(const uint8_t* __restrict__ 
                                                     const uint32_t* __restrict__ off, uint32_t* __restrict__ ent,
                                                     uint16_t* __restrict__ key) {
     __shared__ uint32_t s_w[8][kRxParts];
-    for (uint32_t T = blockIdx.x; T < nrt; T += gridDim.x) rx_scatter_item(in, jobs, rt[T], off, ent, key, s_w);
+    for (uint32_t T = blockIdx.x; T < nrt; T += gridDim.x) rx_scatter_item<false>(in, jobs, rt[T], off, ent, key, s_w);
 }
 
 // Verification and extension of candidate c against its predecessor q
@@ -318,6 +348,7 @@ bytes:
 
 // Partition b of large frame j, by one warp; table = kRxKeys words of
 // shared memory (latest candidate + 1 per key, 0 = none).
+template <bool kC>
 __device__ void rx_resolve_warp(const Job* __restrict__ jobs, uint32_t j, uint32_t b, const uint2* parts,
                                 const uint32_t* ent, const uint16_t* key, uint32_t* __restrict__ pred,
                                 uint32_t* table) {
@@ -325,7 +356,7 @@ __device__ void rx_resolve_warp(const Job* __restrict__ jobs, uint32_t j, uint32
     const uint32_t lt = (1u << lane) - 1u;
     {
         const Job job = jobs[j];
-        const uint2 pr = __ldcg(parts + (uint64_t)j * kRxParts + b);
+        const uint2 pr = ld_stage<kC>(parts + (uint64_t)j * kRxParts + b);
         if (pr.y == 0) return;
         for (uint32_t i = lane; i < kRxKeys / 4; i += 32) reinterpret_cast<uint4*>(table)[i] = make_uint4(0, 0, 0, 0);
         __syncwarp();
@@ -339,8 +370,8 @@ __device__ void rx_resolve_warp(const Job* __restrict__ jobs, uint32_t j, uint32
 #pragma unroll
             for (int u = 0; u < 8; u++) {
                 const uint32_t i = b0 + 32 * u + lane;
-                cc[u] = i < pr.y ? __ldcg(ej + i) : 0u;
-                kk[u] = i < pr.y ? __ldcg(kj + i) : 0xFFFFu;
+                cc[u] = i < pr.y ? ld_stage<kC>(ej + i) : 0u;
+                kk[u] = i < pr.y ? ld_stage<kC>(kj + i) : 0xFFFFu;
             }
 #pragma unroll
             for (int u = 0; u < 8; u++) {
@@ -374,7 +405,7 @@ __global__ void __launch_bounds__(kRxResolveWarps * 32) k_rx_resolve(const Job* 
     uint32_t* table = smem_rx + warp * kRxKeys;
     const uint32_t nw = gridDim.x * kRxResolveWarps;
     for (uint32_t x = blockIdx.x * kRxResolveWarps + warp; x < nbig * kRxParts; x += nw)
-        rx_resolve_warp(jobs, big[x / kRxParts], x % kRxParts, parts, ent, key, pred, table);
+        rx_resolve_warp<false>(jobs, big[x / kRxParts], x % kRxParts, parts, ent, key, pred, table);
 }
 
 // One thread per candidate of every large frame (grid.y = frame): verify and
@@ -382,6 +413,7 @@ __global__ void __launch_bounds__(kRxResolveWarps * 32) k_rx_resolve(const Job* 
 // Entries [lo, hi) of large frame `job`'s candidate list, thread t of
 // nthr: two entries per thread per step, their first loads in flight
 // together.
+template <bool kC>
 __device__ __forceinline__ void rx_verify_range(const uint8_t* __restrict__ in, const Job& job,
                                                 const uint32_t* ent, const uint32_t* pred,
                                                 uint32_t* __restrict__ desc, uint32_t lo, uint32_t hi, uint32_t t,
@@ -396,8 +428,8 @@ __device__ __forceinline__ void rx_verify_range(const uint8_t* __restrict__ in, 
         for (uint32_t i = lo + t; i < C; i += 2 * stride) {
             const uint32_t i2 = i + stride;
             const bool two = i2 < C;
-            const uint32_t c1 = __ldcg(ej + i), p1 = __ldcg(pj + i);
-            const uint32_t c2 = two ? __ldcg(ej + i2) : 0u, p2 = two ? __ldcg(pj + i2) : 0u;
+            const uint32_t c1 = ld_stage<kC>(ej + i), p1 = ld_stage<kC>(pj + i);
+            const uint32_t c2 = two ? ld_stage<kC>(ej + i2) : 0u, p2 = two ? ld_stage<kC>(pj + i2) : 0u;
             uint64_t x1[4], x2[4];
             if (p1) rx_first(src, c1, p1 - 1, x1);
             if (p2) rx_first(src, c2, p2 - 1, x2);
@@ -413,7 +445,7 @@ __global__ void __launch_bounds__(256) k_rx_verify(const uint8_t* __restrict__ i
                                                    uint32_t* __restrict__ desc) {
     for (uint32_t y = blockIdx.y; y < nbig; y += gridDim.y) {
         const Job job = jobs[big[y]];
-        rx_verify_range(in, job, ent, pred, desc, 0, rx_ncand(job.n), blockIdx.x * 256 + threadIdx.x, gridDim.x * 256);
+        rx_verify_range<false>(in, job, ent, pred, desc, 0, rx_ncand(job.n), blockIdx.x * 256 + threadIdx.x, gridDim.x * 256);
     }
 }
 

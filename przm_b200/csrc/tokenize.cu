@@ -29,15 +29,39 @@ __host__ __device__ inline uint32_t slot_cap(int s) { return s == S_OFF ? kSlotO
 
 struct TokTile { uint32_t job; uint32_t tile; };
 
-// First index i in [from, lim) with src[i] != b (or lim), lanes in parallel.
+// 16 unaligned bytes at p as two little-endian u64 (three aligned 8-byte
+// loads; inputs are padded by 64 bytes, so reading up to 24 bytes past p is
+// safe).
+__device__ __forceinline__ void ld128_global_u(const uint8_t* p, uint64_t& lo, uint64_t& hi) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uint64_t* w = reinterpret_cast<const uint64_t*>(a & ~uintptr_t(7));
+    const uint32_t sh = (uint32_t)(a & 7) * 8;
+    const uint64_t w0 = __ldg(w), w1 = __ldg(w + 1);
+    if (!sh) { lo = w0; hi = w1; return; }
+    const uint64_t w2 = __ldg(w + 2);
+    lo = (w0 >> sh) | (w1 << (64 - sh));
+    hi = (w1 >> sh) | (w2 << (64 - sh));
+}
+
+// Position of the first set byte of a 16-byte difference (lo, hi) from k,
+// or 0xFFFFFFFF.
+__device__ __forceinline__ uint32_t first_diff16(uint32_t k, uint64_t lo, uint64_t hi) {
+    if (lo) return k + ((uint32_t)(__ffsll((long long)lo) - 1) >> 3);
+    if (hi) return k + 8 + ((uint32_t)(__ffsll((long long)hi) - 1) >> 3);
+    return 0xFFFFFFFFu;
+}
+
+// First index i in [from, lim) with src[i] != b (or lim), the warp comparing
+// 16 bytes per lane, 512 per step.
 __device__ uint32_t warp_run_end(const uint8_t* src, uint32_t from, uint32_t lim, uint8_t b, uint32_t lane) {
     const uint64_t rep = 0x0101010101010101ull * b;
-    for (uint32_t base = from; base < lim; base += 256) {
-        const uint32_t i = base + lane * 8;
+    for (uint32_t base = from; base < lim; base += 512) {
+        const uint32_t i = base + lane * 16;
         uint32_t first = 0xFFFFFFFFu;
         if (i < lim) {
-            uint64_t x = ld64_global_u(src + i) ^ rep;
-            if (x) first = i + ((uint32_t)(__ffsll((long long)x) - 1) >> 3);
+            uint64_t lo, hi;
+            ld128_global_u(src + i, lo, hi);
+            first = first_diff16(i, lo ^ rep, hi ^ rep);
         }
         uint32_t m = __ballot_sync(0xFFFFFFFFu, first != 0xFFFFFFFFu);
         if (m) {
@@ -48,15 +72,18 @@ __device__ uint32_t warp_run_end(const uint8_t* src, uint32_t from, uint32_t lim
     return lim;
 }
 
-// First k in [from, lim) with src[a+k] != src[b+k] (or lim), lanes in parallel.
+// First k in [from, lim) with src[a+k] != src[b+k] (or lim), the warp
+// comparing 16 bytes per lane, 512 per step.
 __device__ uint32_t warp_match_end(const uint8_t* src, uint32_t a, uint32_t b, uint32_t from, uint32_t lim,
                                    uint32_t lane) {
-    for (uint32_t base = from; base < lim; base += 256) {
-        const uint32_t k = base + lane * 8;
+    for (uint32_t base = from; base < lim; base += 512) {
+        const uint32_t k = base + lane * 16;
         uint32_t first = 0xFFFFFFFFu;
         if (k < lim) {
-            uint64_t x = ld64_global_u(src + a + k) ^ ld64_global_u(src + b + k);
-            if (x) first = k + ((uint32_t)(__ffsll((long long)x) - 1) >> 3);
+            uint64_t alo, ahi, blo, bhi;
+            ld128_global_u(src + a + k, alo, ahi);
+            ld128_global_u(src + b + k, blo, bhi);
+            first = first_diff16(k, alo ^ blo, ahi ^ bhi);
         }
         uint32_t m = __ballot_sync(0xFFFFFFFFu, first != 0xFFFFFFFFu);
         if (m) {
@@ -135,14 +162,13 @@ __device__ __forceinline__ void hist4(uint32_t* h, uint32_t w) {
 }
 
 // 16 source bytes at sw + 4v, shifted right by sh bits (sh = 8 x the
-// source's offset from its 4-byte boundary).  Loads go to L2 (ld.global.cg):
-// the gather reads slots that other blocks of the same persistent launch
-// wrote, which a non-coherent or L1-cached load could see stale.
+// source's offset from its 4-byte boundary); ld_stage<kC> loads (see there).
+template <bool kC>
 __device__ __forceinline__ uint4 ld16_shifted(const uint32_t* sw, uint32_t v, uint32_t sh) {
     const uint32_t* q = sw + 4 * v;
-    const uint32_t w0 = __ldcg(q), w1 = __ldcg(q + 1), w2 = __ldcg(q + 2), w3 = __ldcg(q + 3);
+    const uint32_t w0 = ld_stage<kC>(q), w1 = ld_stage<kC>(q + 1), w2 = ld_stage<kC>(q + 2), w3 = ld_stage<kC>(q + 3);
     if (sh == 0) return make_uint4(w0, w1, w2, w3);
-    const uint32_t w4 = __ldcg(q + 4);
+    const uint32_t w4 = ld_stage<kC>(q + 4);
     return make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh), __funnelshift_r(w2, w3, sh),
                       __funnelshift_r(w3, w4, sh));
 }
@@ -152,11 +178,12 @@ __device__ __forceinline__ uint4 ld16_shifted(const uint32_t* sw, uint32_t v, ui
 // four per lane in flight (source words loaded aligned and funnel-shifted, so
 // reading up to 3 bytes past s + n: slot blocks and inputs have room), then
 // the tail bytes.
+template <bool kC>
 __device__ void warp_copy_hist(uint8_t* __restrict__ d, const uint8_t* s, uint32_t n, uint32_t* __restrict__ h,
                                uint32_t lane) {
     const uint32_t head = min(n, (uint32_t)((16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15));
     if (lane < head) {
-        const uint8_t b = __ldcg(s + lane);
+        const uint8_t b = ld_stage<kC>(s + lane);
         d[lane] = b;
         if (h) atomicAdd(&h[b], 1u);
     }
@@ -171,7 +198,7 @@ __device__ void warp_copy_hist(uint8_t* __restrict__ d, const uint8_t* s, uint32
     for (; v + 96 < nv; v += 128) {
         uint4 o[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) o[u] = ld16_shifted(sw, v + 32 * u, sh);
+        for (int u = 0; u < 4; u++) o[u] = ld16_shifted<kC>(sw, v + 32 * u, sh);
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             d4[v + 32 * u] = o[u];
@@ -179,12 +206,12 @@ __device__ void warp_copy_hist(uint8_t* __restrict__ d, const uint8_t* s, uint32
         }
     }
     for (; v < nv; v += 32) {
-        const uint4 o = ld16_shifted(sw, v, sh);
+        const uint4 o = ld16_shifted<kC>(sw, v, sh);
         d4[v] = o;
         if (h) { hist4(h, o.x); hist4(h, o.y); hist4(h, o.z); hist4(h, o.w); }
     }
     for (uint32_t i = 16 * nv + lane; i < n; i += 32) {
-        const uint8_t b = __ldcg(s + i);
+        const uint8_t b = ld_stage<kC>(s + i);
         d[i] = b;
         if (h) atomicAdd(&h[b], 1u);
     }
@@ -316,7 +343,7 @@ __device__ void tok_emit(const uint4* rec, uint32_t nrec, const uint8_t* tile_sr
             while (lm) {
                 const uint32_t j = __ffs(lm) - 1;
                 lm &= lm - 1;
-                warp_copy_hist(dl + __shfl_sync(0xFFFFFFFFu, dx, j), tile_src + __shfl_sync(0xFFFFFFFFu, from, j),
+                warp_copy_hist<false>(dl + __shfl_sync(0xFFFFFFFFu, dx, j), tile_src + __shfl_sync(0xFFFFFFFFu, from, j),
                                __shfl_sync(0xFFFFFFFFu, cl, j), nullptr, lane);
             }
         }
@@ -326,6 +353,7 @@ __device__ void tok_emit(const uint4* rec, uint32_t nrec, const uint8_t* tile_sr
 }
 
 // One 32 KiB tile, by one warp with its TokSmem.
+template <bool kC>
 __device__ void tokenize_tile(const uint8_t* __restrict__ in, const Job* __restrict__ jobs, const TokTile tt,
                               const uint32_t* desc, uint8_t* __restrict__ slots,
                               uint32_t* __restrict__ tile_lens, uint32_t* __restrict__ err, TokSmem& sm) {
@@ -366,7 +394,7 @@ __device__ void tokenize_tile(const uint8_t* __restrict__ in, const Job* __restr
                     const uint32_t e = base + 128 * (h + u) + 4 * lane;
                     v[u] = make_uint4(0u, 0u, 0u, 0u);
                     if (e < e_hi) {  // dj + e is 16-byte aligned; the array holds whole uint4s below e_hi
-                        v[u] = __ldcg(reinterpret_cast<const uint4*>(dj + e));
+                        v[u] = ld_stage<kC>(reinterpret_cast<const uint4*>(dj + e));
                         if (e + 1 >= e_hi) v[u].y = 0;
                         if (e + 2 >= e_hi) v[u].z = 0;
                         if (e + 3 >= e_hi) v[u].w = 0;
@@ -454,7 +482,7 @@ __device__ void tokenize_tile(const uint8_t* __restrict__ in, const Job* __restr
             // lookahead (przm_tokenizer.cuh:196-216): radix frames have no
             // descriptor at q + 1
             if (!radix && q + 1 < end) {
-                const uint32_t nd = ent + 1 - wb < kTokWin ? sm.desc[ent + 1 - wb] : __ldcg(dj + ent + 1);
+                const uint32_t nd = ent + 1 - wb < kTokWin ? sm.desc[ent + 1 - wb] : ld_stage<kC>(dj + ent + 1);
                 if (nd != 0 && (nd >> 20) > mLen + 1) { pos = q + 1; continue; }
             }
             // run-length token (:218-286)
@@ -525,7 +553,7 @@ __global__ void __launch_bounds__(kTokWarps * 32) k_tokenize(const uint8_t* __re
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t wid = blockIdx.x * kTokWarps + warp;
     const uint32_t nw = gridDim.x * kTokWarps;
-    for (uint32_t T = wid; T < ntiles; T += nw) tokenize_tile(in, jobs, tiles[order[T]], desc, slots, tile_lens, err, s_tok[warp]);
+    for (uint32_t T = wid; T < ntiles; T += nw) tokenize_tile<false>(in, jobs, tiles[order[T]], desc, slots, tile_lens, err, s_tok[warp]);
 }
 
 // ---------------------------------------------------------------------------
@@ -616,6 +644,7 @@ constexpr uint32_t kGatherThreads = 512;
 
 // Frame j by the whole block (any multiple of 128 threads); s_off =
 // ntiles + 1 words, s_hist = [stream][warp group][symbol] counts.
+template <bool kC>
 __device__ void gather_item(const Job* __restrict__ jobs, uint32_t j, const uint8_t* slots,
                             const uint32_t* tile_lens, uint8_t* __restrict__ streams,
                             uint32_t* __restrict__ job_lens, uint32_t* __restrict__ hist, uint32_t* __restrict__ err,
@@ -635,7 +664,7 @@ __device__ void gather_item(const Job* __restrict__ jobs, uint32_t j, const uint
                     uint32_t i = b + lane;
                     // an empty input has no tokenizer tile: its one tile
                     // slot is never written, so its streams are empty
-                    uint32_t v = (i < job.ntiles && job.n > 0) ? __ldcg(tile_lens + (uint64_t)(job.tile0 + i) * S_COUNT + s) : 0;
+                    uint32_t v = (i < job.ntiles && job.n > 0) ? ld_stage<kC>(tile_lens + (uint64_t)(job.tile0 + i) * S_COUNT + s) : 0;
                     uint32_t x = v;
                     for (uint32_t o = 1; o < 32; o <<= 1) {
                         uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
@@ -659,7 +688,7 @@ __device__ void gather_item(const Job* __restrict__ jobs, uint32_t j, const uint
             for (uint32_t t = warp; t < job.ntiles; t += nthr / 32) {
                 const uint32_t o = s_off[t], l = s_off[t + 1] - o;
                 const uint8_t* sp = slots + (uint64_t)(job.tile0 + t) * kSlotStride + slot_base(s);
-                warp_copy_hist(dst + o, sp, l, hs >= 0 ? s_hist[hs][warp & 3] : nullptr, lane);
+                warp_copy_hist<kC>(dst + o, sp, l, hs >= 0 ? s_hist[hs][warp & 3] : nullptr, lane);
             }
             if (tid == 0) job_lens[(uint64_t)j * S_COUNT + s] = total;
         }
@@ -681,7 +710,7 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather(const Job* __restrict
     extern __shared__ uint32_t smem_g[];
     __shared__ uint32_t s_hist[4][4][256];
     for (uint32_t jl = blockIdx.x; jl < njobs; jl += gridDim.x)
-        gather_item(jobs, j0 + jl, slots, tile_lens, streams, job_lens, hist, err, smem_g, s_hist);
+        gather_item<false>(jobs, j0 + jl, slots, tile_lens, streams, job_lens, hist, err, smem_g, s_hist);
 }
 
 }  // namespace pz
