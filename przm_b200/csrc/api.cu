@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/przmgpu.h"
+
 #include "common.cuh"
 #include "entropy.cu"
 #include "frame.cu"
