@@ -40,6 +40,13 @@ extern "C" {
 
 #define PRZMG_PROFILE_D2D 0   /* CompressD2D frame: flat sections, raw literals */
 #define PRZMG_PROFILE_ANS 1   /* match + tokenize + ANS frame (Mode 8 + V-ANS)   */
+/* PRZMG_PROFILE_ANS with Section 3 as the CPU compressor writes it
+ * (PackageOffsetsSection, core/distance/distance.go:825-849, called from
+ * compress.go:956): the frame's distances as a distance-prefix container
+ * (Mode 12 or adaptive V-ANS codes + MSB-first extra bits) or 0x09 + LEB128
+ * varints, and an empty Section 3 when the frame has no distance.  No GPU
+ * entry point of the reference writes this frame; its decoders read it. */
+#define PRZMG_PROFILE_ANS_DIST 2
 
 #define PRZMG_NORM_GO 0       /* gpu.NormalizeFreq, container flag 0x01 */
 #define PRZMG_NORM_CPU 1      /* literals.NormalizeFrequencies, flag 0x00 */

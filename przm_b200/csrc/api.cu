@@ -21,6 +21,7 @@
 
 #include "common.cuh"
 #include "entropy.cu"
+#include "dists.cu"
 #include "frame.cu"
 #include "match.cu"
 #include "tokenize.cu"
@@ -119,6 +120,9 @@ struct Tuning {
 constexpr int kSizeClasses = 4;
 // upper bounds of the mean input size of classes 0..2 (class 3: above)
 constexpr uint64_t kClassBound[kSizeClasses - 1] = {64ull << 10, 768ull << 10, 2ull << 20};
+static inline bool valid_profile(int32_t p) {
+    return p == PRZMG_PROFILE_D2D || p == PRZMG_PROFILE_ANS || p == PRZMG_PROFILE_ANS_DIST;
+}
 static inline int size_class(uint64_t mean) {
     int k = 0;
     while (k < kSizeClasses - 1 && mean > kClassBound[k]) k++;
@@ -147,6 +151,7 @@ struct przmg_batch {
     DevBuf d_tile_sched;  // tokenizer tile weights [0, ntiles) and walk order [ntiles, 2 ntiles)
     DevBuf d_asm;         // assembly work items (frame, part)
     DevBuf d_asm_job;     // the same items grouped by input (plain per-input launches)
+    DevBuf d_s3, d_s3f;   // P2: per-input Section 3 regions and their S3Frame facts
     // per input i, where its items start in each work list ([i + 1] = end)
     std::vector<uint32_t> job_small0, job_rt0, job_big0, job_tile0, job_asm0;
     int launches_plain = 0;
@@ -177,7 +182,7 @@ struct przmg_batch {
                          &d_job_lens, &d_hist, &d_tabs, &d_infos, &d_ans, &d_outs, &d_plans, &d_sizes, &d_out, &d_misc,
                          &d_lists, &d_rtiles, &d_rx_cnt, &d_rx_parts, &d_rx_ent, &d_rx_key, &d_rx_pred, &d_stage_in,
                          &d_stage_out, &d_stage_offs, &d_up_offs, &d_tile_sched, &d_asm, &d_asm_job,
-                         &d_fitems, &d_ftiles, &d_ftarget, &d_fctl};
+                         &d_fitems, &d_ftiles, &d_ftarget, &d_fctl, &d_s3, &d_s3f};
         for (DevBuf* b : all) b->release();
         h_offs.release();
     }
@@ -212,6 +217,7 @@ struct Ctx {
     cudaDeviceProp prop{};
     int sms = 148;
     DevBuf d_meta8, d_ctxlut;
+    DevBuf d_dist12;  // Mode 12 static weights in EncSym form (4 x 64)
     przmg_batch single;  // reused by the one-input calls
     HostBuf h_in, h_out, h_aux;
     DevBuf d_scr_in, d_scr_out, d_scr_aux, d_scr_tab;
@@ -287,7 +293,7 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     b->max_big_cand = 0;
     b->in_offs.assign(njobs, 0);
     b->out_offs.assign(njobs, 0);
-    uint64_t in = 0, desc = 0, str = 0, ans = 0, out = 0;
+    uint64_t in = 0, desc = 0, str = 0, ans = 0, out = 0, s3 = 0;
     uint32_t tile0 = 0;
     for (auto* v : {&b->job_small0, &b->job_rt0, &b->job_big0, &b->job_tile0, &b->job_asm0}) v->assign(njobs + 1, 0);
     for (uint32_t i = 0; i < njobs; i++) {
@@ -314,8 +320,13 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
         j.lit_cap = j.ntiles * kSlotLit;
         j.str_off = str;
         str += align16(stream_region_bytes(j));
+        if (profile >= 2) {
+            j.dist_cap = (uint32_t)(n / 4 + 64);
+            j.s3_off = s3;
+            s3 += align16(s3_region_bytes(j));
+        }
         j.ans_off = ans;
-        if (profile == 1) ans += align16(ans_region_bytes(j));
+        if (profile >= 1) ans += align16(ans_region_bytes(j));
         j.out_cap = (uint32_t)std::min<uint64_t>(przmg_frame_bound(n), 0xFFFFFFF0u);
         j.out_off = out;
         b->out_offs[i] = out;
@@ -390,15 +401,17 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     CK(b->d_streams.ensure(b->stream_bytes));
     CK(b->d_job_lens.ensure((size_t)njobs * S_COUNT * 4 + 16));
     CK(b->d_hist.ensure((size_t)njobs * 1024 * 4 + 16));
-    CK(b->d_tabs.ensure((size_t)njobs * 4 * 256 * sizeof(EncSym) + 16));
-    CK(b->d_infos.ensure((size_t)njobs * 4 * sizeof(TableInfo) + 16));
+    CK(b->d_tabs.ensure((size_t)njobs * kModels * 256 * sizeof(EncSym) + 16));
+    CK(b->d_infos.ensure((size_t)njobs * kModels * sizeof(TableInfo) + 16));
+    CK(b->d_s3.ensure(s3 + 64));
+    CK(b->d_s3f.ensure(sizeof(S3Frame) * std::max<uint32_t>(njobs, 1)));
     CK(b->d_ans.ensure(b->ans_bytes));
     CK(b->d_outs.ensure((size_t)njobs * T_COUNT * sizeof(TaskOut) + 16));
     CK(b->d_plans.ensure((size_t)njobs * sizeof(Plan) + 16));
     CK(b->d_sizes.ensure((size_t)njobs * 4 + 16));
     CK(b->d_out.ensure(b->out_bytes));
     CK(b->d_misc.ensure(64));
-    CK(b->d_lists.ensure((size_t)2 * 4 * std::max<uint32_t>(njobs, 1) * 4 + 64));
+    CK(b->d_lists.ensure((size_t)2 * kModels * std::max<uint32_t>(njobs, 1) * 4 + 64));
     CK(b->d_up_offs.ensure(8ull * std::max<uint32_t>(njobs, 1) + 64));
     if (b->nbig) {
         CK(b->d_rtiles.ensure(sizeof(RxTile) * std::max<size_t>(b->rtiles.size(), 1)));
@@ -600,23 +613,38 @@ static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, cons
     CK(mark(5));
     }
     if (stop_after >= 2 && R.nj) {
-        if (b->profile == 1) {
-            k_normalize<<<R.nj, 128, 0, s>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_job_lens.as<uint32_t>(),
-                                             b->d_hist.as<uint32_t>(), b->d_tabs.as<EncSym>(), b->d_infos.as<TableInfo>());
+        if (b->profile >= 1) {
+            if (b->profile >= 2) {  // Section 3: the distances' codes, extra bits and histogram
+                k_s3_frame<<<R.nj, kS3Threads, 0, s>>>(b->d_jobs.as<Job>(), R.j0, b->d_job_lens.as<uint32_t>(),
+                                                      b->d_streams.as<uint8_t>(), b->d_s3.as<uint8_t>(),
+                                                      b->d_s3f.as<S3Frame>(), b->err_word());
+                CK(cudaGetLastError());
+                launches++;
+            }
+            k_normalize<<<R.nj, 32 * kModels, 0, s>>>(b->d_jobs.as<Job>(), R.j0, b->d_hist.as<uint32_t>(),
+                                                      b->d_s3.as<uint8_t>(), b->d_s3f.as<S3Frame>(),
+                                                      b->d_tabs.as<EncSym>(), b->d_infos.as<TableInfo>());
             CK(cudaGetLastError());
             CK(mark(6));
-            const uint32_t list_cap = 4 * b->njobs;
+            const uint32_t list_cap = kModels * b->njobs;
             uint32_t* lists = b->d_lists.as<uint32_t>();
             uint32_t* counts = lists + 2 * list_cap;
-            k_task_list<<<1, 1024, 0, s>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_job_lens.as<uint32_t>(), lists,
-                                           list_cap, counts);
+            k_task_list<<<1, 1024, 0, s>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_job_lens.as<uint32_t>(),
+                                           b->d_s3f.as<S3Frame>(), lists, list_cap, counts);
             CK(cudaGetLastError());
-            const uint32_t nb_ad = (4 * R.nj + 8 * kRansWarps - 1) / (8 * kRansWarps);
+            const uint32_t nad = (b->profile >= 2 ? 5 : 4) * R.nj;  // adaptive tasks at most
+            const uint32_t nb_ad = (nad + 8 * kRansWarps - 1) / (8 * kRansWarps);
             const uint32_t nb_m8 = (3 * R.nj + 8 * kRansWarps - 1) / (8 * kRansWarps);
+            if (b->profile >= 2) {  // the Mode 12 chains
+                k_s3_chain<<<(R.nj + 31) / 32, 32, 0, s>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_s3.as<uint8_t>(),
+                                                          b->d_s3f.as<S3Frame>(), c->d_dist12.as<EncSym>());
+                CK(cudaGetLastError());
+                launches++;
+            }
             k_rans<<<nb_ad + nb_m8, kRansWarps * 32, kRansSmem, s>>>(
                 b->d_jobs.as<Job>(), b->d_job_lens.as<uint32_t>(), b->d_streams.as<uint8_t>(), b->d_ans.as<uint8_t>(),
                 b->d_tabs.as<EncSym>(), c->d_meta8.as<EncSym>(), c->d_ctxlut.as<uint8_t>(), lists, list_cap, counts, nb_ad,
-                b->d_outs.as<TaskOut>());
+                b->d_s3.as<uint8_t>(), b->d_s3f.as<S3Frame>(), b->d_outs.as<TaskOut>());
             CK(cudaGetLastError());
             launches += 3;
             CK(mark(7));
@@ -626,14 +654,14 @@ static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, cons
         }
         k_plan<<<(R.nj + 127) / 128, 128, 0, s>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_job_lens.as<uint32_t>(),
                                                   b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(),
-                                                  b->d_streams.as<uint8_t>(), b->d_plans.as<Plan>(),
-                                                  b->d_sizes.as<uint32_t>());
+                                                  b->d_streams.as<uint8_t>(), b->d_s3f.as<S3Frame>(),
+                                                  b->d_plans.as<Plan>(), b->d_sizes.as<uint32_t>());
         CK(cudaGetLastError());
         CK(mark(8));
         k_assemble<<<std::max<uint32_t>(1, std::min<uint32_t>(R.nasm, 1u << 20)), kAsmThreads, 0, s>>>(
             b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), R.asm_list + R.asm0, R.nasm, b->d_job_lens.as<uint32_t>(),
             b->d_plans.as<Plan>(), b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(), b->d_streams.as<uint8_t>(),
-            b->d_ans.as<uint8_t>(), b->d_out.as<uint8_t>());
+            b->d_ans.as<uint8_t>(), b->d_s3.as<uint8_t>(), b->d_s3f.as<S3Frame>(), b->d_out.as<uint8_t>());
         CK(cudaGetLastError());
         launches += 2;
         CK(mark(9));
@@ -724,6 +752,14 @@ static int32_t ctx_setup(Ctx* c) {
         build_meta8_tables(tab.data(), lut.data());
         CK(cudaMemcpy(c->d_meta8.p, tab.data(), tab.size() * sizeof(EncSym), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(c->d_ctxlut.p, lut.data(), 256, cudaMemcpyHostToDevice));
+        std::vector<EncSym> t12(4 * 64);
+        for (int k = 0; k < 4; k++)
+            for (uint32_t sym = 0, cum = 0; sym < 64; sym++) {
+                t12[k * 64 + sym] = make_encsym(przm_dist_freq4[k][sym], cum);
+                cum += przm_dist_freq4[k][sym];
+            }
+        CK(c->d_dist12.ensure(t12.size() * sizeof(EncSym)));
+        CK(cudaMemcpy(c->d_dist12.p, t12.data(), t12.size() * sizeof(EncSym), cudaMemcpyHostToDevice));
     }
     c->single.ctx = c;
     CK(cudaStreamSynchronize(c->stream));
@@ -754,7 +790,7 @@ extern "C" int32_t przmg_close(przmg_ctx* h) {
         cudaStreamSynchronize(c->stream);
         c->single.drop_graph();
         c->single.release();
-        DevBuf* bufs[] = {&c->d_meta8, &c->d_ctxlut, &c->d_scr_in, &c->d_scr_out, &c->d_scr_aux,
+        DevBuf* bufs[] = {&c->d_meta8, &c->d_ctxlut, &c->d_dist12, &c->d_scr_in, &c->d_scr_out, &c->d_scr_aux,
                           &c->d_scr_tab, &c->d_s3, &c->d_lit};
         for (DevBuf* b : bufs) b->release();
         c->h_in.release();
@@ -885,7 +921,7 @@ static int32_t compress_one(Ctx* c, const uint8_t* src, uint64_t n, int profile,
     if (out_len) *out_len = 0;
     if (n == 0) { if (prof) { *prof = przmg_profile_t{}; fill_profile(c, prof); } return PRZMG_OK; }
     if (!src || !dst || !out_len) return fail(PRZMG_ERR_INVALID_ARG, "null buffer");
-    if (profile == PRZMG_PROFILE_ANS && n >= (1u << 24))
+    if (profile >= PRZMG_PROFILE_ANS && n >= (1u << 24))
         return fail(PRZMG_ERR_EXCEEDS_MAX_BLOCK, "the frame header holds 24-bit sizes: input must be < 16 MiB");
     int32_t r = single_run(c, src, n, profile, 2, false, prof);
     if (r) return r;
@@ -927,7 +963,7 @@ extern "C" int32_t przmg_compress(przmg_ctx* h, const uint8_t* src, uint64_t n, 
                                   uint64_t cap, uint64_t* out_len, przmg_profile_t* prof) {
     Ctx* c = reinterpret_cast<Ctx*>(h);
     if (!c) return fail(PRZMG_ERR_INVALID_ARG, "null context");
-    if (profile != PRZMG_PROFILE_D2D && profile != PRZMG_PROFILE_ANS) return fail(PRZMG_ERR_INVALID_ARG, "unknown profile");
+    if (!valid_profile(profile)) return fail(PRZMG_ERR_INVALID_ARG, "unknown profile");
     if (int32_t m = mock_check()) return m;
     LOCKED(c);
     return compress_one(c, src, n, profile, dst, cap, out_len, prof);
@@ -1184,13 +1220,13 @@ extern "C" int32_t przmg_compress_batch(przmg_ctx* h, przmg_job_t* jobs, uint64_
                                         int32_t batched, przmg_profile_t* prof) {
     Ctx* c = reinterpret_cast<Ctx*>(h);
     if (!c || (!jobs && njobs)) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
-    if (profile != PRZMG_PROFILE_D2D && profile != PRZMG_PROFILE_ANS) return fail(PRZMG_ERR_INVALID_ARG, "unknown profile");
+    if (!valid_profile(profile)) return fail(PRZMG_ERR_INVALID_ARG, "unknown profile");
     if (int32_t m = mock_check()) return m;
     LOCKED(c);
     for (uint64_t i = 0; i < njobs; i++) {
         jobs[i].out_len = 0;
         jobs[i].status = PRZMG_OK;
-        if (profile == PRZMG_PROFILE_ANS && jobs[i].n >= (1u << 24)) jobs[i].status = PRZMG_ERR_EXCEEDS_MAX_BLOCK;
+        if (profile >= PRZMG_PROFILE_ANS && jobs[i].n >= (1u << 24)) jobs[i].status = PRZMG_ERR_EXCEEDS_MAX_BLOCK;
     }
     if (!batched) {
         for (uint64_t i = 0; i < njobs; i++) {
@@ -1255,9 +1291,9 @@ extern "C" int32_t przmg_batch_create(przmg_ctx* h, const uint64_t* sizes, uint6
                                       przmg_batch** out) {
     Ctx* c = reinterpret_cast<Ctx*>(h);
     if (!c || !out || (!sizes && njobs)) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
-    if (profile != PRZMG_PROFILE_D2D && profile != PRZMG_PROFILE_ANS) return fail(PRZMG_ERR_INVALID_ARG, "unknown profile");
+    if (!valid_profile(profile)) return fail(PRZMG_ERR_INVALID_ARG, "unknown profile");
     for (uint64_t i = 0; i < njobs; i++)
-        if (profile == PRZMG_PROFILE_ANS && sizes[i] >= (1u << 24))
+        if (profile >= PRZMG_PROFILE_ANS && sizes[i] >= (1u << 24))
             return fail(PRZMG_ERR_EXCEEDS_MAX_BLOCK, "the frame header holds 24-bit sizes: inputs must be < 16 MiB");
     LOCKED(c);
     przmg_batch* b = new przmg_batch();
@@ -1491,12 +1527,15 @@ extern "C" int32_t przmg_batch_stats(przmg_batch* b, uint64_t stats[8]) {
     std::vector<uint32_t> lens((size_t)nj * S_COUNT + 1), sizes(nj + 1);
     std::vector<TaskOut> outs((size_t)nj * T_COUNT + 1);
     std::vector<Plan> plans(nj + 1);
+    std::vector<S3Frame> s3f(nj + 1);
     if (nj) {
         CK(cudaMemcpyAsync(lens.data(), b->d_job_lens.p, 4ull * nj * S_COUNT, cudaMemcpyDeviceToHost, c->stream));
         CK(cudaMemcpyAsync(sizes.data(), b->d_sizes.p, 4ull * nj, cudaMemcpyDeviceToHost, c->stream));
         CK(cudaMemcpyAsync(plans.data(), b->d_plans.p, sizeof(Plan) * nj, cudaMemcpyDeviceToHost, c->stream));
-        if (b->profile == 1)
+        if (b->profile >= 1)
             CK(cudaMemcpyAsync(outs.data(), b->d_outs.p, sizeof(TaskOut) * nj * T_COUNT, cudaMemcpyDeviceToHost, c->stream));
+        if (b->profile >= 2)
+            CK(cudaMemcpyAsync(s3f.data(), b->d_s3f.p, sizeof(S3Frame) * nj, cudaMemcpyDeviceToHost, c->stream));
     }
     CK(cudaStreamSynchronize(c->stream));
     for (uint32_t j = 0; j < nj; j++) {
@@ -1507,10 +1546,11 @@ extern "C" int32_t przmg_batch_stats(przmg_batch* b, uint64_t stats[8]) {
         stats[3] += l[S_CMD];
         stats[4] += l[S_OFF];
         stats[7] += plans[j].uncompressed;
-        if (b->profile != 1) continue;
+        if (b->profile < 1) continue;
         for (int t = 0; t < T_COUNT; t++) {
-            if (!task_active(b->jobs[j], l, t)) continue;
-            stats[5] += task_len(l, t);
+            const uint32_t nd = t == T_S3 && b->profile >= 2 ? s3_task_nd(s3f[j]) : 0u;
+            if (!task_active(b->jobs[j], l, t, nd)) continue;
+            stats[5] += task_len(l, t, nd);
             const TaskOut& o = outs[(size_t)j * T_COUNT + t];
             stats[6] += (uint64_t)o.count[0] + o.count[1] + o.count[2] + o.count[3];
         }
@@ -1525,9 +1565,9 @@ extern "C" int32_t przmg_compress_packed(przmg_ctx* h, const uint8_t* host_in, c
                                          uint64_t* out_total) {
     Ctx* c = reinterpret_cast<Ctx*>(h);
     if (!c || !sizes || !out_total || (njobs && (!host_in || !host_out))) return fail(PRZMG_ERR_INVALID_ARG, "null argument");
-    if (profile != PRZMG_PROFILE_D2D && profile != PRZMG_PROFILE_ANS) return fail(PRZMG_ERR_INVALID_ARG, "unknown profile");
+    if (!valid_profile(profile)) return fail(PRZMG_ERR_INVALID_ARG, "unknown profile");
     for (uint64_t i = 0; i < njobs; i++)
-        if (profile == PRZMG_PROFILE_ANS && sizes[i] >= (1u << 24))
+        if (profile >= PRZMG_PROFILE_ANS && sizes[i] >= (1u << 24))
             return fail(PRZMG_ERR_EXCEEDS_MAX_BLOCK, "the frame header holds 24-bit sizes: inputs must be < 16 MiB");
     if (int32_t m = mock_check()) return m;
     LOCKED(c);

@@ -30,9 +30,15 @@ constexpr uint32_t kSlotLit = 33024;
 
 enum Stream : int { S_CMD = 0, S_OP = 1, S_META = 2, S_VAR = 3, S_OFF = 4, S_LIT = 5, S_COUNT = 6 };
 
-// ANS task slots per job: literal stream (adaptive) and the three command
-// substreams, each with the Meta8 and the adaptive model.
-enum Task : int { T_LIT = 0, T_OP_M8 = 1, T_OP_AD = 2, T_META_M8 = 3, T_META_AD = 4, T_VAR_M8 = 5, T_VAR_AD = 6, T_COUNT = 7 };
+// ANS task slots per job: literal stream (adaptive), the three command
+// substreams, each with the Meta8 and the adaptive model, and (P2 frames)
+// the adaptive container of the Section 3 distance codes.
+enum Task : int {
+    T_LIT = 0, T_OP_M8 = 1, T_OP_AD = 2, T_META_M8 = 3, T_META_AD = 4, T_VAR_M8 = 5, T_VAR_AD = 6, T_S3 = 7, T_COUNT = 8
+};
+// adaptive models per job (tables and serialized matrices): literals, op,
+// meta, var, distance codes
+constexpr int kModels = 5;
 
 // error bits reported through the per-batch status word
 enum Err : uint32_t { E_SLOT_OVERFLOW = 1, E_STREAM_OVERFLOW = 2, E_BAD_TOKEN = 4, E_TABLE = 8, E_COPY_TIMEOUT = 32 };
@@ -98,10 +104,39 @@ struct Job {
     uint32_t cmd_cap;   // capacity of cmd/op/meta/var streams
     uint32_t off_cap;   // capacity of the offset stream
     uint32_t lit_cap;   // capacity of the literal stream
-    uint32_t profile;   // 0: CompressD2D frame (P0), 1: entropy-coded frame (P1)
+    uint32_t profile;   // 0: CompressD2D frame (P0), 1: entropy-coded frame (P1), 2: P1 with coded Section 3 (P2)
     uint32_t out_cap;
-    uint32_t pad;
+    uint32_t dist_cap;  // distances a P2 frame can hold (n / 4 + 64: every match covers >= 4 bytes); 0 below P2
+    uint64_t s3_off;    // byte offset of this job's Section 3 region (P2)
 };
+
+// A P2 job's Section 3 region: the distance codes (dist_cap + 16 bytes),
+// the MSB-first extra-bit stream (3 bytes per distance + 16: at most 18
+// extra bits for distances below 2^20, so at most four bytes are touched
+// per distance), the Mode 12 bytes in emission order (2 per code at most,
+// capped at the reference's 2 MiB scratch, + 16), and the codes' histogram
+// (256 u32).
+constexpr uint32_t kS3Scratch = 2u * 1024 * 1024;  // the reference's 2 MiB distance scratch buffers
+__host__ __device__ inline uint64_t s3_extra_off(const Job& j) { return (j.dist_cap + 16ull + 15) & ~15ull; }
+__host__ __device__ inline uint64_t s3_em_off(const Job& j) { return s3_extra_off(j) + ((3ull * j.dist_cap + 16 + 15) & ~15ull); }
+__host__ __device__ inline uint64_t s3_em_cap(const Job& j) {
+    return 2ull * j.dist_cap < kS3Scratch ? 2ull * j.dist_cap : (uint64_t)kS3Scratch;
+}
+__host__ __device__ inline uint64_t s3_hist_off(const Job& j) { return s3_em_off(j) + ((s3_em_cap(j) + 16 + 15) & ~15ull); }
+__host__ __device__ inline uint64_t s3_region_bytes(const Job& j) { return s3_hist_off(j) + 256 * 4; }
+
+// Per-frame Section 3 facts from k_s3_frame and k_s3_chain.
+struct S3Frame {
+    uint32_t nd;     // distances
+    uint32_t bits;   // their extra bits
+    uint32_t bad;    // a distance of 0 or above 2^24 (the reference's ErrOffsetOOB)
+    uint32_t orig;   // bytes of their LEB128 varints
+    uint32_t m12e;   // Mode 12 bytes emitted; 0xFFFFFFFF past the 2 MiB scratch
+    uint32_t m12x;   // Mode 12 final state
+    uint32_t pad[2];
+};
+// distances the codes' adaptive task codes (0: no task)
+__host__ __device__ inline uint32_t s3_task_nd(const S3Frame& f) { return f.bad ? 0u : f.nd; }
 
 // byte offsets of the six streams inside a job's stream region
 __host__ __device__ inline uint64_t stream_base(const Job& j, int s) {
@@ -137,7 +172,9 @@ __host__ __device__ constexpr uint64_t ans_task_bytes(uint32_t L) {
     uint64_t b = 4 * ans_lane_cap(L) + 4 * 4 * ans_nbw_cap(L);
     return (b + 63) & ~63ull;
 }
-__host__ __device__ inline uint32_t task_cap(const Job& j, int t) { return t == T_LIT ? j.lit_cap : j.cmd_cap; }
+__host__ __device__ inline uint32_t task_cap(const Job& j, int t) {
+    return t == T_LIT ? j.lit_cap : t == T_S3 ? j.dist_cap : j.cmd_cap;
+}
 __host__ __device__ inline uint64_t ans_task_off(const Job& j, int t) {
     uint64_t o = 0;
     for (int k = 0; k < t; k++) o += ans_task_bytes(task_cap(j, k));
@@ -175,6 +212,11 @@ struct Plan {
     uint32_t s4_mode;         // 0 raw, 1 V-ANS
     uint32_t uncompressed;
     uint32_t wlog;
+    // Section 3 of a P2 frame: form 0 flat 0x00 (P0/P1), 1 distance-prefix
+    // container, 2 flat 0x09 varints, 3 empty (no distance); code stream 0
+    // Mode 12, 1 the adaptive container; header, code stream and extra-bit
+    // bytes of the container
+    uint32_t s3_form, s3_code, s3_hlen, s3_cl, s3_xl;
 };
 
 struct TableInfo {            // adaptive model of one (job, stream)

@@ -302,22 +302,30 @@ __device__ void warp_build_table(const uint16_t* __restrict__ freq /* smem */, E
     }
 }
 
-// One warp per (frame, model stream): lit, op, meta, var, for frames
-// [j0, j0 + njobs).
-__global__ void k_normalize(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs, const uint32_t* __restrict__ job_lens,
-                            const uint32_t* __restrict__ hist, EncSym* __restrict__ tabs, TableInfo* __restrict__ infos) {
-    __shared__ uint32_t s_cnt[4][256];
-    __shared__ uint16_t s_freq[4][256];
+// One block per frame of [j0, j0 + njobs), one warp per adaptive model:
+// lit, op, meta, var, and for P2 frames with a codes task the distance
+// codes (their histogram in the frame's Section 3 region).
+__global__ void __launch_bounds__(32 * kModels) k_normalize(const Job* __restrict__ jobs, uint32_t j0,
+                                                            const uint32_t* __restrict__ hist,
+                                                            const uint8_t* __restrict__ s3base,
+                                                            const S3Frame* __restrict__ s3f, EncSym* __restrict__ tabs,
+                                                            TableInfo* __restrict__ infos) {
+    __shared__ uint32_t s_cnt[kModels][256];
+    __shared__ uint16_t s_freq[kModels][256];
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const uint32_t lw = blockIdx.x * 4 + w;
-    if (lw >= njobs * 4) return;
-    const uint32_t j = j0 + (lw >> 2), si = lw & 3, gw = 4 * j + si;
-    (void)job_lens;
-    for (uint32_t s = lane; s < 256; s += 32) s_cnt[w][s] = hist[(uint64_t)j * 1024 + si * 256 + s];
+    const uint32_t j = j0 + blockIdx.x, gw = kModels * j + w;
+    const uint32_t* src;
+    if (w < 4) {
+        src = hist + (uint64_t)j * 1024 + w * 256;
+    } else {
+        const Job job = jobs[j];
+        if (job.profile < 2 || s3_task_nd(s3f[j]) < 64) return;
+        src = reinterpret_cast<const uint32_t*>(s3base + job.s3_off + s3_hist_off(job));
+    }
+    for (uint32_t s = lane; s < 256; s += 32) s_cnt[w][s] = src[s];
     __syncwarp();
     warp_normalize_frequencies(s_cnt[w], s_freq[w], lane);
     warp_build_table(s_freq[w], tabs + (uint64_t)gw * 256, infos + gw, lane);
-    (void)jobs;
 }
 
 // ---------------------------------------------------------------------------
@@ -524,17 +532,21 @@ inline void build_meta8_tables(EncSym* tab, uint8_t* ctxlut) {
 }
 
 // Task eligibility for the entropy-coded frame (packSubstream,
-// core/commands/commands.go:371-406; PackageLiteralsSection selection).
-__host__ __device__ inline uint32_t task_len(const uint32_t* lens, int t) {
-    return t == T_LIT ? lens[S_LIT] : lens[S_OP + (t - 1) / 2];
+// core/commands/commands.go:371-406; PackageLiteralsSection selection; the
+// adaptive container of the distance codes for 64 codes or more,
+// PackDistancePrefix, core/distance/distance.go:692-748).  nd: the frame's
+// distances for the codes' task (s3_task_nd), 0 otherwise.
+__host__ __device__ inline bool task_is_m8(int t) { return t == T_OP_M8 || t == T_META_M8 || t == T_VAR_M8; }
+__host__ __device__ inline uint32_t task_len(const uint32_t* lens, int t, uint32_t nd = 0) {
+    return t == T_LIT ? lens[S_LIT] : t == T_S3 ? nd : lens[S_OP + (t - 1) / 2];
 }
-__host__ __device__ inline bool task_active(const Job& job, const uint32_t* lens, int t) {
-    if (job.profile != 1) return false;
-    const uint32_t n = task_len(lens, t);
+__host__ __device__ inline bool task_active(const Job& job, const uint32_t* lens, int t, uint32_t nd = 0) {
+    if (job.profile == 0) return false;
+    const uint32_t n = task_len(lens, t, nd);
+    if (t == T_S3) return job.profile >= 2 && n >= 64 && n <= kS3Scratch;
     if (t == T_LIT) return n >= 1 && n <= (8u << 20);
     if (lens[S_CMD] > (2u << 20)) return false;
-    const bool m8 = (t & 1) == 1;  // T_OP_M8, T_META_M8, T_VAR_M8 are odd
-    return n <= (2u << 20) && n >= (m8 ? 24u : 16u);
+    return n <= (2u << 20) && n >= (task_is_m8(t) ? 24u : 16u);
 }
 
 // Task list: every active (frame, task) pair, split by model kind and
@@ -542,7 +554,8 @@ __host__ __device__ inline bool task_active(const Job& job, const uint32_t* lens
 // 8 tasks sharing a warp have similar lengths and the long chains start
 // first.  Entry = frame << 3 | task.  One block.
 __global__ void __launch_bounds__(1024) k_task_list(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs,
-                                                    const uint32_t* __restrict__ job_lens, uint32_t* __restrict__ lists,
+                                                    const uint32_t* __restrict__ job_lens,
+                                                    const S3Frame* __restrict__ s3f, uint32_t* __restrict__ lists,
                                                     uint32_t list_cap, uint32_t* __restrict__ counts) {
     __shared__ uint32_t s_cnt[2][33];
     __shared__ uint32_t s_pos[2][33];
@@ -555,9 +568,10 @@ __global__ void __launch_bounds__(1024) k_task_list(const Job* __restrict__ jobs
         const int t = (int)(e % T_COUNT);
         const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
         const Job job = jobs[j];
-        if (!task_active(job, lens, t)) continue;
-        const uint32_t kind = (t != T_LIT && (t & 1)) ? 1u : 0u;
-        atomicAdd(&s_cnt[kind][32 - __clz(task_len(lens, t))], 1u);
+        const uint32_t nd = t == T_S3 && job.profile >= 2 ? s3_task_nd(s3f[j]) : 0u;
+        if (!task_active(job, lens, t, nd)) continue;
+        const uint32_t kind = task_is_m8(t) ? 1u : 0u;
+        atomicAdd(&s_cnt[kind][32 - __clz(task_len(lens, t, nd))], 1u);
     }
     __syncthreads();
     if (tid < 2) {
@@ -571,9 +585,10 @@ __global__ void __launch_bounds__(1024) k_task_list(const Job* __restrict__ jobs
         const int t = (int)(e % T_COUNT);
         const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
         const Job job = jobs[j];
-        if (!task_active(job, lens, t)) continue;
-        const uint32_t kind = (t != T_LIT && (t & 1)) ? 1u : 0u;
-        const uint32_t p = atomicAdd(&s_pos[kind][32 - __clz(task_len(lens, t))], 1u);
+        const uint32_t nd = t == T_S3 && job.profile >= 2 ? s3_task_nd(s3f[j]) : 0u;
+        if (!task_active(job, lens, t, nd)) continue;
+        const uint32_t kind = task_is_m8(t) ? 1u : 0u;
+        const uint32_t p = atomicAdd(&s_pos[kind][32 - __clz(task_len(lens, t, nd))], 1u);
         lists[kind * list_cap + p] = (j << 3) | (uint32_t)t;
     }
 }
@@ -596,7 +611,8 @@ __global__ void __launch_bounds__(kRansWarps * 32) k_rans(const Job* __restrict_
                                                           const uint8_t* __restrict__ ctxlut,
                                                           const uint32_t* __restrict__ lists, uint32_t list_cap,
                                                           const uint32_t* __restrict__ counts, uint32_t nb_ad,
-                                                          TaskOut* __restrict__ outs) {
+                                                          const uint8_t* __restrict__ s3base,
+                                                          const S3Frame* __restrict__ s3f, TaskOut* __restrict__ outs) {
     extern __shared__ __align__(16) uint8_t smem_r[];
     __shared__ uint8_t s_lut[256];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -627,8 +643,8 @@ __global__ void __launch_bounds__(kRansWarps * 32) k_rans(const Job* __restrict_
             if (tk >= nlist) break;
             const uint32_t e = lists[tk];
             const uint32_t jj = e >> 3, tt = e & 7;
-            const uint32_t mi = tt == T_LIT ? 0 : 1 + (tt - 1) / 2;
-            const EncSym* src = tabs + ((uint64_t)jj * 4 + mi) * 256;
+            const uint32_t mi = tt == T_LIT ? 0 : tt == T_S3 ? 4 : 1 + (tt - 1) / 2;
+            const EncSym* src = tabs + ((uint64_t)jj * kModels + mi) * 256;
             for (uint32_t i = lane; i < 256; i += 32) wtab[k * 256 + i] = src[i];
         }
     }
@@ -636,9 +652,14 @@ __global__ void __launch_bounds__(kRansWarps * 32) k_rans(const Job* __restrict_
     if (!have) return;
     const Job job = jobs[j];
     const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
-    const uint32_t n = task_len(lens, t);
-    const int s = t == T_LIT ? S_LIT : S_OP + (t - 1) / 2;
-    const uint8_t* src = streams + job.str_off + stream_base(job, s);
+    const uint32_t n = task_len(lens, t, t == T_S3 ? s3_task_nd(s3f[j]) : 0u);
+    const uint8_t* src;
+    if (t == T_S3) {
+        src = s3base + job.s3_off;  // the distance codes
+    } else {
+        const int s = t == T_LIT ? S_LIT : S_OP + (t - 1) / 2;
+        src = streams + job.str_off + stream_base(job, s);
+    }
     uint8_t* base = ans + job.ans_off + ans_task_off(job, t);
     LaneIO io = lane_io(base, task_cap(job, t), l);
     TaskOut* o = outs + (uint64_t)j * T_COUNT + t;

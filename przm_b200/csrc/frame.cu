@@ -10,6 +10,9 @@
 // raw literals would be misread as a container), FlagNibble with a V-ANS
 // Section 4 (compress.go:990), and the uncompressed-frame fallback of
 // assembleContainer (compress.go:962-985).
+// Profile 2 is profile 1 with Section 3 as PackageOffsetsSection of the
+// frame's distances (distance.go:825-849, compress.go:956), empty when the
+// frame has no distance.
 #include "common.cuh"
 
 namespace pz {
@@ -22,9 +25,52 @@ __device__ inline uint32_t rd32b(const uint8_t* p) {
     return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
 }
 
+// Section 3 of a P2 frame (PackageOffsetsSection, distance.go:825-849 with
+// PackDistancePrefix :692-748 and SelectPrefixMode :750-758): empty without
+// distances; else the distance-prefix container (Mode 12 code stream, or the
+// codes' adaptive container for 64 codes or more when that fits 2 MiB and is
+// smaller; header 0x0B / 0x0A / 0x06 by size) when it fits the reference's
+// 2 MiB scratch and is smaller than the varints, else 0x09 + the varints.
+// The reference's errors (a distance of 0 or above 2^24, more than 2^21
+// codes, extra bits or Mode 12 bytes past 2 MiB) give the varint form.
+__device__ inline void plan_s3(Plan& p, const Job& job, const uint32_t* lens, const S3Frame& f,
+                               const TableInfo* infos, const TaskOut* outs, uint32_t j) {
+    p.l3 = 0;
+    if (f.nd == 0) {
+        p.s3_form = 3;
+        return;
+    }
+    const uint32_t nd = f.nd, xl = (f.bits + 7) / 8;
+    if (!(f.bad || nd > kS3Scratch || xl > kS3Scratch || f.m12e == 0xFFFFFFFFu)) {
+        uint32_t cl = 5 + f.m12e, code = 0;
+        if (task_active(job, lens, T_S3, nd)) {
+            const uint32_t al = 8 + infos[(uint64_t)j * kModels + 4].mat_len + 16 + tsum(outs[(uint64_t)j * T_COUNT + T_S3]);
+            if (al <= kS3Scratch && al < cl) {
+                cl = al;
+                code = 1;
+            }
+        }
+        const uint32_t orig = f.orig;
+        const uint32_t h = (orig <= 255 && nd <= 255 && cl <= 255) ? 4u : (orig <= 65535 && nd <= 65535 && cl <= 65535) ? 7u : 13u;
+        const uint64_t total = (uint64_t)h + cl + xl;
+        if (total <= kS3Scratch && total < orig) {
+            p.s3_form = 1;
+            p.s3_code = code;
+            p.s3_hlen = h;
+            p.s3_cl = cl;
+            p.s3_xl = xl;
+            p.l3 = (uint32_t)total;
+            return;
+        }
+    }
+    p.s3_form = 2;
+    p.l3 = 1 + f.orig;
+}
+
 __global__ void k_plan(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs, const uint32_t* __restrict__ job_lens,
                        const TableInfo* __restrict__ infos, const TaskOut* __restrict__ outs,
-                       const uint8_t* __restrict__ streams, Plan* __restrict__ plans, uint32_t* __restrict__ sizes) {
+                       const uint8_t* __restrict__ streams, const S3Frame* __restrict__ s3f, Plan* __restrict__ plans,
+                       uint32_t* __restrict__ sizes) {
     const uint32_t jl = blockIdx.x * blockDim.x + threadIdx.x;
     if (jl >= njobs) return;
     const uint32_t j = j0 + jl;
@@ -60,7 +106,7 @@ __global__ void k_plan(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs
                     if (sz < best) { best = sz; mode = 1; }
                 }
                 if (task_active(job, lens, ta)) {
-                    uint32_t sz = 8 + infos[(uint64_t)j * 4 + 1 + sub].mat_len + 16 + tsum(outs[(uint64_t)j * T_COUNT + ta]);
+                    uint32_t sz = 8 + infos[(uint64_t)j * kModels + 1 + sub].mat_len + 16 + tsum(outs[(uint64_t)j * T_COUNT + ta]);
                     if (sz < best) { best = sz; mode = 2; }
                 }
                 p.sub_len[sub] = best;
@@ -69,7 +115,8 @@ __global__ void k_plan(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs
             }
             if (m8 < cmd) { p.s2_mode = 1; p.l2 = m8; }
         }
-        p.l3 = lens[S_OFF] + 5;
+        if (job.profile >= 2) plan_s3(p, job, lens, s3f[j], infos, outs, j);
+        else p.l3 = lens[S_OFF] + 5;
         const uint32_t lit = lens[S_LIT];
         p.l4 = lit;
         bool fallback = false;
@@ -84,7 +131,7 @@ __global__ void k_plan(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs
             uint32_t vsz = 0;
             if (task_active(job, lens, T_LIT)) {
                 const uint32_t e = tsum(outs[(uint64_t)j * T_COUNT + T_LIT]);
-                if (e <= (8u << 20)) { vans = true; vsz = 8 + infos[(uint64_t)j * 4].mat_len + 16 + e; }
+                if (e <= (8u << 20)) { vans = true; vsz = 8 + infos[(uint64_t)j * kModels].mat_len + 16 + e; }
             }
             if (vans && (vsz < lit || !raw_ok)) { p.s4_mode = 1; p.l4 = vsz; }
             else if (!raw_ok) fallback = true;
@@ -170,7 +217,9 @@ __global__ void __launch_bounds__(kAsmThreads, 4) k_assemble(const uint8_t* __re
                                                           const Plan* __restrict__ plans, const TableInfo* __restrict__ infos,
                                                           const TaskOut* __restrict__ outs,
                                                           const uint8_t* __restrict__ streams,
-                                                          const uint8_t* __restrict__ ans, uint8_t* __restrict__ out) {
+                                                          const uint8_t* __restrict__ ans,
+                                                          const uint8_t* __restrict__ s3base,
+                                                          const S3Frame* __restrict__ s3f, uint8_t* __restrict__ out) {
     for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
         const uint32_t j = items[it].x, part = items[it].y;
         const Job job = jobs[j];
@@ -205,7 +254,7 @@ __global__ void __launch_bounds__(kAsmThreads, 4) k_assemble(const uint8_t* __re
                     const TaskOut to = outs[(uint64_t)j * T_COUNT + T_LIT];
                     const uint8_t* tb = abase + ans_task_off(job, T_LIT);
                     const uint32_t cap = task_cap(job, T_LIT);
-                    const uint32_t h = 8 + infos[(uint64_t)j * 4].mat_len + 16;
+                    const uint32_t h = 8 + infos[(uint64_t)j * kModels].mat_len + 16;
                     stitch_pass<kAsmThreads>(tb, cap, len, r0, s4 + h + stitch_offset(tb, cap, len, to, r0));
                 }
             } else {
@@ -256,20 +305,52 @@ __global__ void __launch_bounds__(kAsmThreads, 4) k_assemble(const uint8_t* __re
                     if (p.sub_mode[sub] == 1)
                         write_container(d, 0x41, len, nullptr, to, abase + ans_task_off(job, t), task_cap(job, t));
                     else
-                        write_container(d, 0x00, len, infos + (uint64_t)j * 4 + 1 + sub, to, abase + ans_task_off(job, t),
+                        write_container(d, 0x00, len, infos + (uint64_t)j * kModels + 1 + sub, to, abase + ans_task_off(job, t),
                                         task_cap(job, t));
                 }
                 o += p.sub_len[sub];
             }
         }
         w += p.l2;
-        // Section 3 (flat)
+        // Section 3
         uint8_t* s3 = f + w;
-        if (threadIdx.x == 0) { s3[0] = 0x00; put32(s3 + 1, lens[S_OFF]); }
-        block_copy(s3 + 5, sreg + stream_base(job, S_OFF), lens[S_OFF]);
+        if (job.profile < 2) {  // flat
+            if (threadIdx.x == 0) { s3[0] = 0x00; put32(s3 + 1, lens[S_OFF]); }
+            block_copy(s3 + 5, sreg + stream_base(job, S_OFF), lens[S_OFF]);
+        } else if (p.s3_form == 2) {  // 0x09 + the varints
+            if (threadIdx.x == 0) s3[0] = 0x09;
+            block_copy(s3 + 1, sreg + stream_base(job, S_OFF), lens[S_OFF]);
+        } else if (p.s3_form == 1) {  // distance-prefix container
+            const S3Frame fr = s3f[j];
+            const uint32_t h = p.s3_hlen, orig = fr.orig, nd = fr.nd, cl = p.s3_cl;
+            if (threadIdx.x == 0) {
+                if (h == 4) {
+                    s3[0] = 0x0B; s3[1] = (uint8_t)orig; s3[2] = (uint8_t)nd; s3[3] = (uint8_t)cl;
+                } else if (h == 7) {
+                    s3[0] = 0x0A;
+                    s3[1] = (uint8_t)orig; s3[2] = (uint8_t)(orig >> 8);
+                    s3[3] = (uint8_t)nd; s3[4] = (uint8_t)(nd >> 8);
+                    s3[5] = (uint8_t)cl; s3[6] = (uint8_t)(cl >> 8);
+                } else {
+                    s3[0] = 0x06; put32(s3 + 1, orig); put32(s3 + 5, nd); put32(s3 + 9, cl);
+                }
+            }
+            uint8_t* cs = s3 + h;
+            const uint8_t* rb = s3base + job.s3_off;
+            if (p.s3_code == 0) {  // Mode 12: 0x0C | LE32 state | the emitted bytes reversed
+                if (threadIdx.x == 0) { cs[0] = 0x0C; put32(cs + 1, fr.m12x); }
+                const uint8_t* em = rb + s3_em_off(job);
+                const uint32_t e = fr.m12e;
+                for (uint32_t k = threadIdx.x; k < e; k += blockDim.x) cs[5 + k] = em[e - 1 - k];
+            } else {
+                write_container(cs, 0x00, nd, infos + (uint64_t)j * kModels + 4, outs[(uint64_t)j * T_COUNT + T_S3],
+                                abase + ans_task_off(job, T_S3), task_cap(job, T_S3));
+            }
+            block_copy(cs + cl, rb + s3_extra_off(job), p.s3_xl);
+        }
         // Section 4: the container head here, the literals in parts 1, 2, ...
         if (p.s4_mode == 1)
-            container_head(s4, 0x00, lens[S_LIT], infos + (uint64_t)j * 4, outs[(uint64_t)j * T_COUNT + T_LIT]);
+            container_head(s4, 0x00, lens[S_LIT], infos + (uint64_t)j * kModels, outs[(uint64_t)j * T_COUNT + T_LIT]);
     }
 }
 

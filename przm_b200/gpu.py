@@ -32,6 +32,7 @@ MaxTileLitBytes = 36864
 
 PROFILE_D2D = 0
 PROFILE_ANS = 1
+PROFILE_ANS_DIST = 2  # PROFILE_ANS with Section 3 as PackageOffsetsSection (the CPU compressor's Section 3)
 TUNING_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
 NORM_GO = 0
 NORM_CPU = 1
@@ -457,8 +458,9 @@ class GPUCompressor:
         return self.Compress(src, PROFILE_D2D)
 
     def Compress(self, src, profile: int = PROFILE_ANS) -> tuple[bytes, GPUProfile]:
-        """One frame: PROFILE_D2D (CompressD2D bytes) or PROFILE_ANS (match +
-        tokenize + ANS frame, input < 16 MiB)."""
+        """One frame: PROFILE_D2D (CompressD2D bytes), PROFILE_ANS (match +
+        tokenize + ANS frame, input < 16 MiB) or PROFILE_ANS_DIST (that frame
+        with a coded Section 3)."""
         a = _u8(src)
         cap = FrameBound(len(a))
         out = np.zeros(cap, np.uint8)

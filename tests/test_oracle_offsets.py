@@ -201,3 +201,15 @@ def test_p2_frame_without_matches_has_empty_section3():
     l2, l3, s3 = frame_sections(f)
     assert l3 == 0 and s3 == b""
     assert O.ref_decompress(f, len(a)) == a.tobytes()
+
+
+def test_p2_section3_forms_of_the_parity_kinds():
+    # the forms tests/test_gpu_p2.py expects the device to reproduce, on the
+    # inputs it uses (the smaller half; 0x06 needs multi-MiB frames)
+    from tests import inputs as I
+    from tests.frames import section3_form
+    forms = set()
+    for n in (4096, 20_000, 200_000):
+        for a in I.kinds(n, 5 + n).values():
+            forms.add(section3_form(O.compress_p2(a)))
+    assert {"empty", "09", "0B-M12", "0A-M12", "0A-AD"} <= forms, forms
