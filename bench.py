@@ -412,6 +412,100 @@ def uneven_measure(comp, count: int, sample: int) -> dict:
     return out
 
 
+def coded_measure(comp, hin, frames, steps: int, inflight: int) -> dict:
+    """The same batch with the CPU compressor's coded sections (P2: Section 3
+    as PackageOffsetsSection; P3: also Section 4 as PackageLiteralsSection),
+    device-resident, `inflight` batches on as many streams: GB/s of input,
+    stage times of one run, compression ratio, two frames checked against the
+    oracle and the reference decoder."""
+    import torch
+    from oracle import oracle as O
+    from przm_b200 import gpu
+    sizes = [len(a) for a in frames]
+    total = sum(sizes)
+    out = {}
+    for name, profile, ref in (("p2", gpu.PROFILE_ANS_DIST, O.compress_p2), ("p3", gpu.PROFILE_ANS_SHEAF, O.compress_p3)):
+        bs = [gpu.DeviceBatch(comp, sizes, profile) for _ in range(inflight)]
+        ss = [torch.cuda.Stream() for _ in range(inflight)]
+        try:
+            for b, st in zip(bs, ss):
+                b.upload(hin, st.cuda_stream)
+            for k in range(max(3, inflight)):
+                bs[k % inflight].enqueue(ss[k % inflight].cuda_stream, graph=True)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(ss[0])
+            for st in ss[1:]:
+                st.wait_event(e0)
+            for k in range(steps):
+                bs[k % inflight].enqueue(ss[k % inflight].cuda_stream, graph=True)
+            for st in ss[1:]:
+                ev = torch.cuda.Event()
+                ev.record(st)
+                ss[0].wait_event(ev)
+            e1.record(ss[0])
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            stats = bs[0].stats()
+            fsz = bs[0].frame_sizes()
+            offs = [int(x) for x in bs[0].out_offs]
+            from przm_b200 import devmem
+            ok = True
+            for i in (0, len(frames) - 1):
+                fr = devmem.download(bs[0].d_out + offs[i], int(fsz[i]))
+                ok = ok and fr == ref(frames[i])
+                if O.ref_decoder_available():
+                    ok = ok and O.ref_decompress(fr, sizes[i]) == frames[i].tobytes()
+            out[name] = {"gbps": round(total / (ms / 1e3) / 1e9, 3), "ms_per_step": round(ms, 3),
+                         "inflight_batches": inflight,
+                         "compression_ratio": round(stats["frame_bytes"] / stats["input_bytes"], 4),
+                         "stage_ms": {k: round(v, 3) for k, v in bs[0].stage_times().items()},
+                         "verified_frames": 2 if ok else 0}
+        finally:
+            for b in bs:
+                b.close()
+    return out
+
+
+def decode_measure(comp, batch, reps: int = 3) -> dict:
+    """The batch's frames decoded on the device (przmg_decompress_batch_device),
+    device-resident: GB/s of decoded bytes (median of reps, CUDA events on
+    the call's stream), every frame compared with its input on the device
+    (przmg_batch_verify, untimed)."""
+    import torch
+    from przm_b200 import devmem
+    sizes = [int(x) for x in batch.sizes]
+    fs = batch.frame_sizes()
+    dcap = [max(n, 1) for n in sizes]
+    doffs = np.zeros(len(sizes), np.uint64)
+    o = 0
+    for i, n in enumerate(dcap):
+        doffs[i] = o
+        o += (n + 64 + 15) // 16 * 16
+    out = devmem.alloc(o + 64)
+    st = torch.cuda.Stream()
+    try:
+        runs = []
+        for _ in range(reps + 1):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            status, lens = comp.DecompressBatchDevice(batch.d_out, batch.out_offs, fs, out.ptr, doffs, dcap,
+                                                      st.cuda_stream)
+            e1.record(st)
+            e1.synchronize()
+            runs.append(e0.elapsed_time(e1))
+        ms = sorted(runs[1:])[len(runs[1:]) // 2]
+        ok = int((status == 0).sum())
+    finally:
+        out.free()
+    bad = batch.verify()
+    return {"gbps": round(sum(sizes) / (ms / 1e3) / 1e9, 3), "ms": round(ms, 3), "frames": len(sizes),
+            "frames_decoded": ok, "frames_verified_on_device": len(sizes) - bad,
+            "note": "decoded bytes per second; frames of the entropy-coded profile, device-resident"}
+
+
 def _flush_l2(buf, stream) -> None:
     """Writes a buffer larger than the 126 MB L2 on `stream` (between timed
     iterations of workloads that fit in L2)."""
@@ -577,6 +671,8 @@ def main() -> None:
                     help="sections of the Section 3 distance-coding measurement (0: skip)")
     ap.add_argument("--section4-streams", type=int, default=64,
                     help="literal streams of the Section 4 selection measurement (0: skip)")
+    ap.add_argument("--coded-steps", type=int, default=20,
+                    help="steps of the coded-sections (P2, P3) legs on the same batch (0: skip)")
     ap.add_argument("--no-configs01", dest="configs01", action="store_false",
                     help="skip the one-frame 4 MiB and the histogram + V-ANS (64 x 1 MiB Zipf) legs")
     args = ap.parse_args()
@@ -758,6 +854,12 @@ def main() -> None:
     for bt in batches[1:]:  # free the extra in-flight batches before the other workloads
         bt.close()
     batches = batches[:1]
+    decode = None
+    if world == 1:
+        try:
+            decode = decode_measure(comp, batch)
+        except Exception as e:  # an extra leg never costs the bench line
+            decode = {"error": f"{type(e).__name__}: {e}"[:300]}
     # single-GPU runs only (under torchrun the other ranks would wait for them)
     serve = (serve_measure(comp, args.serve_requests, fractions=(0.1, 0.25, 0.5, 0.75, 0.9, 1.0, 1.2))
              if args.serve_requests > 0 and world == 1 else None)
@@ -785,6 +887,13 @@ def main() -> None:
             section4 = section4_measure(comp, args.section4_streams)
         except Exception as e:  # an extra leg never costs the bench line
             section4 = {"error": f"{type(e).__name__}: {e}"[:300]}
+
+    coded = None
+    if args.coded_steps > 0 and world == 1:
+        try:
+            coded = coded_measure(comp, hin, frames, args.coded_steps, min(D, 4))
+        except Exception as e:  # an extra leg never costs the bench line
+            coded = {"error": f"{type(e).__name__}: {e}"[:300]}
 
     # roofline of the dominant kernel
     peak, peak_kind = measured_peaks()
@@ -849,7 +958,7 @@ def main() -> None:
             "roofline": roofline, "pipeline_roofline": pipeline, "stage_ms": {k: round(v, 3) for k, v in stages.items()},
             "cpu_baseline": cpu_base, "plain_per_frame": plain, "clocks": clk, "gpu_launches": gl,
             "serving": serve, "uneven_batch": uneven, "section3": section3, "section4": section4,
-            "config0_one_frame": c0, "config1_hist_vans": c1,
+            "config0_one_frame": c0, "config1_hist_vans": c1, "coded_sections": coded, "decode": decode,
         }
         print(json.dumps(line), flush=True)
     for bt in batches:

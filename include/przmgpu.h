@@ -37,6 +37,10 @@ extern "C" {
 #define PRZMG_ERR_DEVICE (-13)           /* a kernel reported an internal bound violation */
 #define PRZMG_ERR_NOT_FOUND (-14)        /* serving: unknown request id */
 #define PRZMG_ERR_BUSY (-15)             /* serving: admission refused (budget or queue full) */
+/* decoder status codes: the reference decoder's own values (przm_dec.h) */
+#define PRZMG_ERR_CORRUPTED_FRAME (-1)   /* PRZM_ERR_CORRUPTED_FRAME (also PRZMG_ERR_INVALID_ARG) */
+#define PRZMG_ERR_INVALID_MAGIC (-2)     /* PRZM_ERR_INVALID_MAGIC */
+#define PRZMG_ERR_UNSUPPORTED_MODE (-6)  /* PRZM_ERR_UNSUPPORTED_MODE: a frame feature the GPU decoder does not take */
 
 #define PRZMG_PROFILE_D2D 0   /* CompressD2D frame: flat sections, raw literals */
 #define PRZMG_PROFILE_ANS 1   /* match + tokenize + ANS frame (Mode 8 + V-ANS)   */
@@ -47,6 +51,13 @@ extern "C" {
  * varints, and an empty Section 3 when the frame has no distance.  No GPU
  * entry point of the reference writes this frame; its decoders read it. */
 #define PRZMG_PROFILE_ANS_DIST 2
+/* PRZMG_PROFILE_ANS_DIST with Section 4 as the CPU compressor writes it
+ * (PackageLiteralsSection, core/literals/literals.go:664-693, called from
+ * compress.go:957): the smallest of the raw literals, their adaptive V-ANS
+ * container and the four étale-sheaf foliations (core/literals/sheaf.go),
+ * raw under PRZMG_PROFILE_ANS's decodability rule.  No GPU entry point of
+ * the reference writes this frame; its decoders read it. */
+#define PRZMG_PROFILE_ANS_SHEAF 3
 
 #define PRZMG_NORM_GO 0       /* gpu.NormalizeFreq, container flag 0x01 */
 #define PRZMG_NORM_CPU 1      /* literals.NormalizeFrequencies, flag 0x00 */
@@ -427,6 +438,31 @@ uint64_t przmg_pinned_pool_pooled(przmg_pinned_pool* pool); /* buffers held (for
  * owned by the context).  *pool receives that pool: return the buffer with
  * przmg_pinned_pool_put(pool, buf, przmg_pinned_pool_buf_size(pool)). */
 int32_t przmg_get_pinned(przmg_ctx* ctx, uint64_t size, void** buf, przmg_pinned_pool** pool);
+
+/* ---- the GPU decoder (decompress.go:380-700, src/przm_dec.c:741-1529) -----
+ * The reference's gpu package has no decoder: these decode PRZM frames on
+ * the device with the semantics of its CPU decoder, for every frame this
+ * library writes (profiles 0-3) and the frames of the same format written
+ * elsewhere.  Frames that use an external dictionary, the base64
+ * normalisation flag, delta-masked matches, the nibble-plane literal form or
+ * the dictionary-word opcodes return PRZMG_ERR_UNSUPPORTED_MODE (decode those
+ * on the host). */
+/* Decompress (api.go:44): one frame from host memory into dst (dst_cap >=
+ * the frame's size); *out_len = decoded bytes.  An empty src gives 0 bytes. */
+int32_t przmg_decompress(przmg_ctx* ctx, const uint8_t* src, uint64_t src_len, uint8_t* dst, uint64_t dst_cap,
+                         uint64_t* out_len);
+/* count device-resident frames (d_src + src_offs[i], src_lens[i] bytes) into
+ * d_dst + dst_offs[i] (dst_caps[i] bytes): status[i] (PRZMG_OK or the frame's
+ * error) and out_lens[i] per frame; waits for the work (enqueued on
+ * `stream`, 0 = the context's).  The return value is the call's own status. */
+int32_t przmg_decompress_batch_device(przmg_ctx* ctx, uint64_t d_src, const uint64_t* src_offs,
+                                      const uint32_t* src_lens, uint64_t count, uint64_t d_dst,
+                                      const uint64_t* dst_offs, const uint32_t* dst_caps, int32_t* status,
+                                      uint64_t* out_lens, uint64_t stream);
+/* Every frame of the batch's last run decoded on the device and compared
+ * with its input there; *bad = the frames that do not decode or differ.
+ * Synchronises the device first. */
+int32_t przmg_batch_verify(przmg_batch* b, uint64_t* bad);
 
 #ifdef __cplusplus
 }

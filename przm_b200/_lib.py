@@ -127,6 +127,9 @@ SIGNATURES: dict[str, tuple] = {
     "przmg_pinned_pool_buf_size": (u64, [vp]),
     "przmg_pinned_pool_pooled": (u64, [vp]),
     "przmg_get_pinned": (i32, [vp, u64, vp, vp]),
+    "przmg_decompress": (i32, [vp, vp, u64, vp, u64, vp]),
+    "przmg_decompress_batch_device": (i32, [vp, u64, vp, vp, u64, u64, vp, vp, vp, vp, u64]),
+    "przmg_batch_verify": (i32, [vp, vp]),
 }
 
 _LIB: C.CDLL | None = None

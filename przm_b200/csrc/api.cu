@@ -22,7 +22,9 @@
 #include "common.cuh"
 #include "entropy.cu"
 #include "dists.cu"
+#include "fibers.cu"
 #include "frame.cu"
+#include "decode.cu"
 #include "match.cu"
 #include "tokenize.cu"
 #include "front.cu"
@@ -121,7 +123,7 @@ constexpr int kSizeClasses = 4;
 // upper bounds of the mean input size of classes 0..2 (class 3: above)
 constexpr uint64_t kClassBound[kSizeClasses - 1] = {64ull << 10, 768ull << 10, 2ull << 20};
 static inline bool valid_profile(int32_t p) {
-    return p == PRZMG_PROFILE_D2D || p == PRZMG_PROFILE_ANS || p == PRZMG_PROFILE_ANS_DIST;
+    return p == PRZMG_PROFILE_D2D || p == PRZMG_PROFILE_ANS || p == PRZMG_PROFILE_ANS_DIST || p == PRZMG_PROFILE_ANS_SHEAF;
 }
 static inline int size_class(uint64_t mean) {
     int k = 0;
@@ -151,7 +153,8 @@ struct przmg_batch {
     DevBuf d_tile_sched;  // tokenizer tile weights [0, ntiles) and walk order [ntiles, 2 ntiles)
     DevBuf d_asm;         // assembly work items (frame, part)
     DevBuf d_asm_job;     // the same items grouped by input (plain per-input launches)
-    DevBuf d_s3, d_s3f;   // P2: per-input Section 3 regions and their S3Frame facts
+    DevBuf d_s3, d_s3f;   // P2 and up: per-input Section 3 regions and their S3Frame facts
+    DevBuf d_fib;         // P3: per-input fiber regions
     // per input i, where its items start in each work list ([i + 1] = end)
     std::vector<uint32_t> job_small0, job_rt0, job_big0, job_tile0, job_asm0;
     int launches_plain = 0;
@@ -182,7 +185,7 @@ struct przmg_batch {
                          &d_job_lens, &d_hist, &d_tabs, &d_infos, &d_ans, &d_outs, &d_plans, &d_sizes, &d_out, &d_misc,
                          &d_lists, &d_rtiles, &d_rx_cnt, &d_rx_parts, &d_rx_ent, &d_rx_key, &d_rx_pred, &d_stage_in,
                          &d_stage_out, &d_stage_offs, &d_up_offs, &d_tile_sched, &d_asm, &d_asm_job,
-                         &d_fitems, &d_ftiles, &d_ftarget, &d_fctl, &d_s3, &d_s3f};
+                         &d_fitems, &d_ftiles, &d_ftarget, &d_fctl, &d_s3, &d_s3f, &d_fib};
         for (DevBuf* b : all) b->release();
         h_offs.release();
     }
@@ -223,6 +226,9 @@ struct Ctx {
     DevBuf d_scr_in, d_scr_out, d_scr_aux, d_scr_tab;
     DevBuf d_s3;   // scratch of przmg_package_offsets_batch
     DevBuf d_lit;  // scratch of przmg_package_literals_batch
+    // the GPU decoder: static tables, per-frame scratch, jobs, results,
+    // entropy tasks; przmg_batch_verify's decoded bytes and comparisons
+    DevBuf d_dstatic, d_dscr, d_djobs, d_dinfo, d_dtasks, d_dout, d_ddiff;
     cudaEvent_t ev[8] = {};
 };
 
@@ -293,7 +299,7 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     b->max_big_cand = 0;
     b->in_offs.assign(njobs, 0);
     b->out_offs.assign(njobs, 0);
-    uint64_t in = 0, desc = 0, str = 0, ans = 0, out = 0, s3 = 0;
+    uint64_t in = 0, desc = 0, str = 0, ans = 0, out = 0, s3 = 0, fib = 0;
     uint32_t tile0 = 0;
     for (auto* v : {&b->job_small0, &b->job_rt0, &b->job_big0, &b->job_tile0, &b->job_asm0}) v->assign(njobs + 1, 0);
     for (uint32_t i = 0; i < njobs; i++) {
@@ -324,6 +330,10 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
             j.dist_cap = (uint32_t)(n / 4 + 64);
             j.s3_off = s3;
             s3 += align16(s3_region_bytes(j));
+        }
+        if (profile >= 3) {
+            j.fib_off = fib;
+            fib += align16(fib_region_bytes(j));
         }
         j.ans_off = ans;
         if (profile >= 1) ans += align16(ans_region_bytes(j));
@@ -405,13 +415,14 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     CK(b->d_infos.ensure((size_t)njobs * kModels * sizeof(TableInfo) + 16));
     CK(b->d_s3.ensure(s3 + 64));
     CK(b->d_s3f.ensure(sizeof(S3Frame) * std::max<uint32_t>(njobs, 1)));
+    CK(b->d_fib.ensure(fib + 64));
     CK(b->d_ans.ensure(b->ans_bytes));
     CK(b->d_outs.ensure((size_t)njobs * T_COUNT * sizeof(TaskOut) + 16));
     CK(b->d_plans.ensure((size_t)njobs * sizeof(Plan) + 16));
     CK(b->d_sizes.ensure((size_t)njobs * 4 + 16));
     CK(b->d_out.ensure(b->out_bytes));
     CK(b->d_misc.ensure(64));
-    CK(b->d_lists.ensure((size_t)2 * kModels * std::max<uint32_t>(njobs, 1) * 4 + 64));
+    CK(b->d_lists.ensure((size_t)2 * kModels * std::max<uint32_t>(njobs, 1) * sizeof(TaskDesc) + 64));
     CK(b->d_up_offs.ensure(8ull * std::max<uint32_t>(njobs, 1) + 64));
     if (b->nbig) {
         CK(b->d_rtiles.ensure(sizeof(RxTile) * std::max<size_t>(b->rtiles.size(), 1)));
@@ -621,18 +632,26 @@ static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, cons
                 CK(cudaGetLastError());
                 launches++;
             }
+            if (b->profile >= 3) {  // Section 4: the literals' four foliations
+                k_frame_fibers<<<dim3(R.nj, 4), 1024, 0, s>>>(b->d_jobs.as<Job>(), R.j0, b->d_job_lens.as<uint32_t>(),
+                                                             b->d_streams.as<uint8_t>(), b->d_fib.as<uint8_t>());
+                CK(cudaGetLastError());
+                launches++;
+            }
             k_normalize<<<R.nj, 32 * kModels, 0, s>>>(b->d_jobs.as<Job>(), R.j0, b->d_hist.as<uint32_t>(),
                                                       b->d_s3.as<uint8_t>(), b->d_s3f.as<S3Frame>(),
-                                                      b->d_tabs.as<EncSym>(), b->d_infos.as<TableInfo>());
+                                                      b->d_fib.as<uint8_t>(), b->d_tabs.as<EncSym>(),
+                                                      b->d_infos.as<TableInfo>());
             CK(cudaGetLastError());
             CK(mark(6));
             const uint32_t list_cap = kModels * b->njobs;
-            uint32_t* lists = b->d_lists.as<uint32_t>();
-            uint32_t* counts = lists + 2 * list_cap;
+            TaskDesc* lists = b->d_lists.as<TaskDesc>();
+            uint32_t* counts = reinterpret_cast<uint32_t*>(lists + 2 * list_cap);
             k_task_list<<<1, 1024, 0, s>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_job_lens.as<uint32_t>(),
-                                           b->d_s3f.as<S3Frame>(), lists, list_cap, counts);
+                                           b->d_s3f.as<S3Frame>(), b->d_streams.as<uint8_t>(), b->d_s3.as<uint8_t>(),
+                                           b->d_fib.as<uint8_t>(), b->d_ans.as<uint8_t>(), lists, list_cap, counts);
             CK(cudaGetLastError());
-            const uint32_t nad = (b->profile >= 2 ? 5 : 4) * R.nj;  // adaptive tasks at most
+            const uint32_t nad = (b->profile >= 3 ? kModels : b->profile >= 2 ? 5 : 4) * R.nj;  // adaptive tasks at most
             const uint32_t nb_ad = (nad + 8 * kRansWarps - 1) / (8 * kRansWarps);
             const uint32_t nb_m8 = (3 * R.nj + 8 * kRansWarps - 1) / (8 * kRansWarps);
             if (b->profile >= 2) {  // the Mode 12 chains
@@ -641,10 +660,9 @@ static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, cons
                 CK(cudaGetLastError());
                 launches++;
             }
-            k_rans<<<nb_ad + nb_m8, kRansWarps * 32, kRansSmem, s>>>(
-                b->d_jobs.as<Job>(), b->d_job_lens.as<uint32_t>(), b->d_streams.as<uint8_t>(), b->d_ans.as<uint8_t>(),
-                b->d_tabs.as<EncSym>(), c->d_meta8.as<EncSym>(), c->d_ctxlut.as<uint8_t>(), lists, list_cap, counts, nb_ad,
-                b->d_s3.as<uint8_t>(), b->d_s3f.as<S3Frame>(), b->d_outs.as<TaskOut>());
+            k_rans<<<nb_ad + nb_m8, kRansWarps * 32, kRansSmem, s>>>(lists, list_cap, counts, nb_ad,
+                                                                    b->d_tabs.as<EncSym>(), c->d_meta8.as<EncSym>(),
+                                                                    c->d_ctxlut.as<uint8_t>(), b->d_outs.as<TaskOut>());
             CK(cudaGetLastError());
             launches += 3;
             CK(mark(7));
@@ -655,13 +673,15 @@ static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, cons
         k_plan<<<(R.nj + 127) / 128, 128, 0, s>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_job_lens.as<uint32_t>(),
                                                   b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(),
                                                   b->d_streams.as<uint8_t>(), b->d_s3f.as<S3Frame>(),
-                                                  b->d_plans.as<Plan>(), b->d_sizes.as<uint32_t>());
+                                                  b->d_fib.as<uint8_t>(), b->d_plans.as<Plan>(),
+                                                  b->d_sizes.as<uint32_t>());
         CK(cudaGetLastError());
         CK(mark(8));
         k_assemble<<<std::max<uint32_t>(1, std::min<uint32_t>(R.nasm, 1u << 20)), kAsmThreads, 0, s>>>(
             b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), R.asm_list + R.asm0, R.nasm, b->d_job_lens.as<uint32_t>(),
             b->d_plans.as<Plan>(), b->d_infos.as<TableInfo>(), b->d_outs.as<TaskOut>(), b->d_streams.as<uint8_t>(),
-            b->d_ans.as<uint8_t>(), b->d_s3.as<uint8_t>(), b->d_s3f.as<S3Frame>(), b->d_out.as<uint8_t>());
+            b->d_ans.as<uint8_t>(), b->d_s3.as<uint8_t>(), b->d_s3f.as<S3Frame>(), b->d_fib.as<uint8_t>(),
+            b->d_out.as<uint8_t>());
         CK(cudaGetLastError());
         launches += 2;
         CK(mark(9));
@@ -791,7 +811,8 @@ extern "C" int32_t przmg_close(przmg_ctx* h) {
         c->single.drop_graph();
         c->single.release();
         DevBuf* bufs[] = {&c->d_meta8, &c->d_ctxlut, &c->d_dist12, &c->d_scr_in, &c->d_scr_out, &c->d_scr_aux,
-                          &c->d_scr_tab, &c->d_s3, &c->d_lit};
+                          &c->d_scr_tab, &c->d_s3, &c->d_lit, &c->d_dstatic, &c->d_dscr, &c->d_djobs,
+                          &c->d_dinfo, &c->d_dtasks, &c->d_dout, &c->d_ddiff};
         for (DevBuf* b : bufs) b->release();
         c->h_in.release();
         c->h_out.release();
@@ -1528,6 +1549,7 @@ extern "C" int32_t przmg_batch_stats(przmg_batch* b, uint64_t stats[8]) {
     std::vector<TaskOut> outs((size_t)nj * T_COUNT + 1);
     std::vector<Plan> plans(nj + 1);
     std::vector<S3Frame> s3f(nj + 1);
+    std::vector<uint32_t> fls(16 * (size_t)nj + 16, 0);
     if (nj) {
         CK(cudaMemcpyAsync(lens.data(), b->d_job_lens.p, 4ull * nj * S_COUNT, cudaMemcpyDeviceToHost, c->stream));
         CK(cudaMemcpyAsync(sizes.data(), b->d_sizes.p, 4ull * nj, cudaMemcpyDeviceToHost, c->stream));
@@ -1536,6 +1558,10 @@ extern "C" int32_t przmg_batch_stats(przmg_batch* b, uint64_t stats[8]) {
             CK(cudaMemcpyAsync(outs.data(), b->d_outs.p, sizeof(TaskOut) * nj * T_COUNT, cudaMemcpyDeviceToHost, c->stream));
         if (b->profile >= 2)
             CK(cudaMemcpyAsync(s3f.data(), b->d_s3f.p, sizeof(S3Frame) * nj, cudaMemcpyDeviceToHost, c->stream));
+        if (b->profile >= 3)
+            for (uint32_t j = 0; j < nj; j++)
+                CK(cudaMemcpyAsync(&fls[16 * (size_t)j], b->d_fib.as<uint8_t>() + b->jobs[j].fib_off, 64,
+                                   cudaMemcpyDeviceToHost, c->stream));
     }
     CK(cudaStreamSynchronize(c->stream));
     for (uint32_t j = 0; j < nj; j++) {
@@ -1549,8 +1575,9 @@ extern "C" int32_t przmg_batch_stats(przmg_batch* b, uint64_t stats[8]) {
         if (b->profile < 1) continue;
         for (int t = 0; t < T_COUNT; t++) {
             const uint32_t nd = t == T_S3 && b->profile >= 2 ? s3_task_nd(s3f[j]) : 0u;
-            if (!task_active(b->jobs[j], l, t, nd)) continue;
-            stats[5] += task_len(l, t, nd);
+            const uint32_t* fl = b->profile >= 3 ? &fls[16 * (size_t)j] : nullptr;
+            if (!task_active(b->jobs[j], l, t, nd, fl)) continue;
+            stats[5] += task_len(l, t, nd, fl);
             const TaskOut& o = outs[(size_t)j * T_COUNT + t];
             stats[6] += (uint64_t)o.count[0] + o.count[1] + o.count[2] + o.count[3];
         }
@@ -1739,6 +1766,11 @@ extern "C" int32_t przmg_match_lz77_streaming(przmg_ctx* h, const uint8_t* src, 
 // serving: continuous batching of submitted requests
 // ---------------------------------------------------------------------------
 #include "serve.inc"
+
+// ---------------------------------------------------------------------------
+// the GPU decoder
+// ---------------------------------------------------------------------------
+#include "decode.inc"
 
 // ---------------------------------------------------------------------------
 // allocation-free single-stream V-ANS (static device scratch)

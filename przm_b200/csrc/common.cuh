@@ -31,14 +31,17 @@ constexpr uint32_t kSlotLit = 33024;
 enum Stream : int { S_CMD = 0, S_OP = 1, S_META = 2, S_VAR = 3, S_OFF = 4, S_LIT = 5, S_COUNT = 6 };
 
 // ANS task slots per job: literal stream (adaptive), the three command
-// substreams, each with the Meta8 and the adaptive model, and (P2 frames)
-// the adaptive container of the Section 3 distance codes.
+// substreams, each with the Meta8 and the adaptive model, (P2 frames and
+// up) the adaptive container of the Section 3 distance codes, and (P3) the
+// sixteen sheaf fibers, T_FIB + 4 mode + fiber.
 enum Task : int {
-    T_LIT = 0, T_OP_M8 = 1, T_OP_AD = 2, T_META_M8 = 3, T_META_AD = 4, T_VAR_M8 = 5, T_VAR_AD = 6, T_S3 = 7, T_COUNT = 8
+    T_LIT = 0, T_OP_M8 = 1, T_OP_AD = 2, T_META_M8 = 3, T_META_AD = 4, T_VAR_M8 = 5, T_VAR_AD = 6, T_S3 = 7,
+    T_FIB = 8, T_COUNT = 24
 };
 // adaptive models per job (tables and serialized matrices): literals, op,
-// meta, var, distance codes
-constexpr int kModels = 5;
+// meta, var, distance codes, then the fibers (model 5 + 4 mode + fiber)
+constexpr int kModels = 21;
+constexpr int kFibModel = 5;
 
 // error bits reported through the per-batch status word
 enum Err : uint32_t { E_SLOT_OVERFLOW = 1, E_STREAM_OVERFLOW = 2, E_BAD_TOKEN = 4, E_TABLE = 8, E_COPY_TIMEOUT = 32 };
@@ -107,7 +110,8 @@ struct Job {
     uint32_t profile;   // 0: CompressD2D frame (P0), 1: entropy-coded frame (P1), 2: P1 with coded Section 3 (P2)
     uint32_t out_cap;
     uint32_t dist_cap;  // distances a P2 frame can hold (n / 4 + 64: every match covers >= 4 bytes); 0 below P2
-    uint64_t s3_off;    // byte offset of this job's Section 3 region (P2)
+    uint64_t s3_off;    // byte offset of this job's Section 3 region (P2 and up)
+    uint64_t fib_off;   // byte offset of this job's fiber region (P3)
 };
 
 // A P2 job's Section 3 region: the distance codes (dist_cap + 16 bytes),
@@ -180,7 +184,39 @@ __host__ __device__ inline uint64_t ans_task_off(const Job& j, int t) {
     for (int k = 0; k < t; k++) o += ans_task_bytes(task_cap(j, k));
     return o;
 }
-__host__ __device__ inline uint64_t ans_region_bytes(const Job& j) { return ans_task_off(j, T_COUNT); }
+// A P3 job's fiber region: the 16 fiber lengths (u32, [mode][fiber]), their
+// 16 histograms (256 u32 each), then per mode its four fibers one after
+// another, each starting on a 16-byte boundary.  The fiber tasks' rANS
+// scratch follows the fixed tasks' in the job's ANS region, one budget per
+// mode: the four fibers' task scratch exceeds one task of their total length
+// by less than 3 KiB (per-lane rounding), so one literal task's bytes plus
+// 8 KiB always hold them.
+constexpr uint32_t kFibHistOff = 64;
+constexpr uint32_t kFibAreaOff = 64 + 16 * 256 * 4;
+constexpr uint32_t kFibMax = 8u * 1024 * 1024;  // literals split into fibers: the reference's 8 MiB literal buffers
+__host__ __device__ inline uint64_t fib_mode_bytes(const Job& j) { return (j.lit_cap + 64ull + 15) & ~15ull; }
+__host__ __device__ inline uint64_t fib_region_bytes(const Job& j) { return kFibAreaOff + 4 * fib_mode_bytes(j); }
+__host__ __device__ inline uint64_t fib_mode_ans(const Job& j) { return ans_task_bytes(j.lit_cap) + 8192; }
+__host__ __device__ inline uint64_t ans_region_bytes(const Job& j) {
+    return ans_task_off(j, T_FIB) + (j.profile >= 3 ? 4 * fib_mode_ans(j) : 0);
+}
+// Fiber k of mode m: its length (fl: the 16 lengths), its byte offset in the
+// fiber region and its rANS scratch offset in the job's ANS region.
+struct FibGeom {
+    uint32_t n;
+    uint64_t byte_off, ans_off;
+};
+__host__ __device__ inline FibGeom fib_geom(const Job& j, const uint32_t* fl, uint32_t m, uint32_t k) {
+    FibGeom g;
+    g.byte_off = kFibAreaOff + m * fib_mode_bytes(j);
+    g.ans_off = ans_task_off(j, T_FIB) + m * fib_mode_ans(j);
+    for (uint32_t q = 0; q < k; q++) {
+        g.byte_off += (fl[4 * m + q] + 15ull) & ~15ull;
+        g.ans_off += ans_task_bytes(fl[4 * m + q]);
+    }
+    g.n = fl[4 * m + k];
+    return g;
+}
 
 // Encoding table entry for one symbol of one model:
 //   m   : 32-bit reciprocal so that floor(x_r / f) == umulhi(x_r, m) >> s for
@@ -217,6 +253,9 @@ struct Plan {
     // Mode 12, 1 the adaptive container; header, code stream and extra-bit
     // bytes of the container
     uint32_t s3_form, s3_code, s3_hlen, s3_cl, s3_xl;
+    // Section 4 of a P3 frame in sheaf form (s4_mode 2): the foliation and
+    // each fiber's bytes in the container (0: empty; == its length: raw)
+    uint32_t s4_sheaf, fe[4];
 };
 
 struct TableInfo {            // adaptive model of one (job, stream)

@@ -302,13 +302,15 @@ __device__ void warp_build_table(const uint16_t* __restrict__ freq /* smem */, E
     }
 }
 
-// One block per frame of [j0, j0 + njobs), one warp per adaptive model:
-// lit, op, meta, var, and for P2 frames with a codes task the distance
-// codes (their histogram in the frame's Section 3 region).
+// One block per frame of [j0, j0 + gridDim.x), one warp per adaptive model:
+// lit, op, meta, var; for P2 frames and up with a codes task the distance
+// codes (their histogram in the frame's Section 3 region); for P3 frames
+// every non-empty fiber (histograms in the frame's fiber region).
 __global__ void __launch_bounds__(32 * kModels) k_normalize(const Job* __restrict__ jobs, uint32_t j0,
                                                             const uint32_t* __restrict__ hist,
                                                             const uint8_t* __restrict__ s3base,
-                                                            const S3Frame* __restrict__ s3f, EncSym* __restrict__ tabs,
+                                                            const S3Frame* __restrict__ s3f,
+                                                            const uint8_t* __restrict__ fibbase, EncSym* __restrict__ tabs,
                                                             TableInfo* __restrict__ infos) {
     __shared__ uint32_t s_cnt[kModels][256];
     __shared__ uint16_t s_freq[kModels][256];
@@ -319,8 +321,16 @@ __global__ void __launch_bounds__(32 * kModels) k_normalize(const Job* __restric
         src = hist + (uint64_t)j * 1024 + w * 256;
     } else {
         const Job job = jobs[j];
-        if (job.profile < 2 || s3_task_nd(s3f[j]) < 64) return;
-        src = reinterpret_cast<const uint32_t*>(s3base + job.s3_off + s3_hist_off(job));
+        if (w == 4) {
+            if (job.profile < 2 || s3_task_nd(s3f[j]) < 64) return;
+            src = reinterpret_cast<const uint32_t*>(s3base + job.s3_off + s3_hist_off(job));
+        } else {
+            if (job.profile < 3) return;
+            const uint8_t* fr = fibbase + job.fib_off;
+            const uint32_t f = w - kFibModel;
+            if (reinterpret_cast<const uint32_t*>(fr)[f] == 0) return;
+            src = reinterpret_cast<const uint32_t*>(fr + kFibHistOff) + f * 256;
+        }
     }
     for (uint32_t s = lane; s < 256; s += 32) s_cnt[w][s] = src[s];
     __syncwarp();
@@ -534,28 +544,80 @@ inline void build_meta8_tables(EncSym* tab, uint8_t* ctxlut) {
 // Task eligibility for the entropy-coded frame (packSubstream,
 // core/commands/commands.go:371-406; PackageLiteralsSection selection; the
 // adaptive container of the distance codes for 64 codes or more,
-// PackDistancePrefix, core/distance/distance.go:692-748).  nd: the frame's
-// distances for the codes' task (s3_task_nd), 0 otherwise.
+// PackDistancePrefix, core/distance/distance.go:692-748; every non-empty
+// sheaf fiber, tryEncodeFiber, core/literals/literals.go:633-643).  nd: the
+// frame's distances for the codes' task (s3_task_nd); fl: its 16 fiber
+// lengths (P3), else null.
 __host__ __device__ inline bool task_is_m8(int t) { return t == T_OP_M8 || t == T_META_M8 || t == T_VAR_M8; }
-__host__ __device__ inline uint32_t task_len(const uint32_t* lens, int t, uint32_t nd = 0) {
+__host__ __device__ inline uint32_t task_len(const uint32_t* lens, int t, uint32_t nd = 0, const uint32_t* fl = nullptr) {
+    if (t >= T_FIB) return fl ? fl[t - T_FIB] : 0u;
     return t == T_LIT ? lens[S_LIT] : t == T_S3 ? nd : lens[S_OP + (t - 1) / 2];
 }
-__host__ __device__ inline bool task_active(const Job& job, const uint32_t* lens, int t, uint32_t nd = 0) {
+__host__ __device__ inline bool task_active(const Job& job, const uint32_t* lens, int t, uint32_t nd = 0,
+                                            const uint32_t* fl = nullptr) {
     if (job.profile == 0) return false;
-    const uint32_t n = task_len(lens, t, nd);
+    const uint32_t n = task_len(lens, t, nd, fl);
+    if (t >= T_FIB) return job.profile >= 3 && n >= 1;
     if (t == T_S3) return job.profile >= 2 && n >= 64 && n <= kS3Scratch;
     if (t == T_LIT) return n >= 1 && n <= (8u << 20);
     if (lens[S_CMD] > (2u << 20)) return false;
     return n <= (2u << 20) && n >= (task_is_m8(t) ? 24u : 16u);
 }
+// The per-frame facts a task needs, from device memory.
+__device__ __forceinline__ uint32_t task_nd(const Job& job, const S3Frame* s3f, uint32_t j, int t) {
+    return t == T_S3 && job.profile >= 2 ? s3_task_nd(s3f[j]) : 0u;
+}
+__device__ __forceinline__ const uint32_t* task_fl(const Job& job, const uint8_t* fibbase) {
+    return job.profile >= 3 ? reinterpret_cast<const uint32_t*>(fibbase + job.fib_off) : nullptr;
+}
+
+// Where a task's symbols are, how many, its scratch layout's capacity and
+// its scratch offset in the job's ANS region.
+struct TaskView {
+    const uint8_t* src;
+    uint64_t ans_off;
+    uint32_t n, cap;
+};
+__device__ __forceinline__ TaskView task_view(const Job& job, const uint32_t* lens, const uint8_t* streams,
+                                              const uint8_t* s3base, const uint8_t* fibbase, uint32_t nd,
+                                              const uint32_t* fl, int t) {
+    TaskView v;
+    v.n = task_len(lens, t, nd, fl);
+    if (t >= T_FIB) {
+        const FibGeom g = fib_geom(job, fl, (uint32_t)(t - T_FIB) >> 2, (uint32_t)(t - T_FIB) & 3u);
+        v.src = fibbase + job.fib_off + g.byte_off;
+        v.ans_off = g.ans_off;
+        v.cap = g.n;
+    } else {
+        v.src = t == T_S3 ? s3base + job.s3_off
+                          : streams + job.str_off + stream_base(job, t == T_LIT ? S_LIT : S_OP + (t - 1) / 2);
+        v.ans_off = ans_task_off(job, t);
+        v.cap = task_cap(job, t);
+    }
+    return v;
+}
+__device__ __forceinline__ uint32_t task_model(int t) {
+    return t == T_LIT ? 0u : t == T_S3 ? 4u : t >= T_FIB ? (uint32_t)(kFibModel + t - T_FIB) : 1u + (uint32_t)(t - 1) / 2;
+}
+
+// One rANS task as the rANS kernel takes it, resolved by the task list.
+struct __align__(16) TaskDesc {
+    const uint8_t* src;  // the symbols
+    uint8_t* base;       // the task's rANS scratch
+    uint32_t n, cap;     // symbols; the scratch layout's capacity
+    uint32_t out;        // TaskOut index: frame * T_COUNT + task
+    uint32_t tab;        // adaptive model row: frame * kModels + model
+};
 
 // Task list: every active (frame, task) pair, split by model kind and
 // ordered longest-first (by the bit length of the symbol count) so that the
 // 8 tasks sharing a warp have similar lengths and the long chains start
-// first.  Entry = frame << 3 | task.  One block.
+// first; each entry is the task's resolved descriptor.  One block.
 __global__ void __launch_bounds__(1024) k_task_list(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs,
                                                     const uint32_t* __restrict__ job_lens,
-                                                    const S3Frame* __restrict__ s3f, uint32_t* __restrict__ lists,
+                                                    const S3Frame* __restrict__ s3f, const uint8_t* __restrict__ streams,
+                                                    const uint8_t* __restrict__ s3base, const uint8_t* __restrict__ fibbase,
+                                                    uint8_t* __restrict__ ans, TaskDesc* __restrict__ lists,
                                                     uint32_t list_cap, uint32_t* __restrict__ counts) {
     __shared__ uint32_t s_cnt[2][33];
     __shared__ uint32_t s_pos[2][33];
@@ -568,10 +630,11 @@ __global__ void __launch_bounds__(1024) k_task_list(const Job* __restrict__ jobs
         const int t = (int)(e % T_COUNT);
         const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
         const Job job = jobs[j];
-        const uint32_t nd = t == T_S3 && job.profile >= 2 ? s3_task_nd(s3f[j]) : 0u;
-        if (!task_active(job, lens, t, nd)) continue;
+        const uint32_t nd = task_nd(job, s3f, j, t);
+        const uint32_t* fl = task_fl(job, fibbase);
+        if (!task_active(job, lens, t, nd, fl)) continue;
         const uint32_t kind = task_is_m8(t) ? 1u : 0u;
-        atomicAdd(&s_cnt[kind][32 - __clz(task_len(lens, t, nd))], 1u);
+        atomicAdd(&s_cnt[kind][32 - __clz(task_len(lens, t, nd, fl))], 1u);
     }
     __syncthreads();
     if (tid < 2) {
@@ -585,11 +648,20 @@ __global__ void __launch_bounds__(1024) k_task_list(const Job* __restrict__ jobs
         const int t = (int)(e % T_COUNT);
         const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
         const Job job = jobs[j];
-        const uint32_t nd = t == T_S3 && job.profile >= 2 ? s3_task_nd(s3f[j]) : 0u;
-        if (!task_active(job, lens, t, nd)) continue;
+        const uint32_t nd = task_nd(job, s3f, j, t);
+        const uint32_t* fl = task_fl(job, fibbase);
+        if (!task_active(job, lens, t, nd, fl)) continue;
         const uint32_t kind = task_is_m8(t) ? 1u : 0u;
-        const uint32_t p = atomicAdd(&s_pos[kind][32 - __clz(task_len(lens, t, nd))], 1u);
-        lists[kind * list_cap + p] = (j << 3) | (uint32_t)t;
+        const uint32_t p = atomicAdd(&s_pos[kind][32 - __clz(task_len(lens, t, nd, fl))], 1u);
+        const TaskView v = task_view(job, lens, streams, s3base, fibbase, nd, fl, t);
+        TaskDesc d;
+        d.src = v.src;
+        d.base = ans + job.ans_off + v.ans_off;
+        d.n = v.n;
+        d.cap = v.cap;
+        d.out = j * T_COUNT + (uint32_t)t;
+        d.tab = j * kModels + task_model(t);
+        lists[kind * list_cap + p] = d;
     }
 }
 
@@ -603,21 +675,17 @@ constexpr uint32_t kRansSmem = kRansWarps * (kRansTabBytes + kRingBytesPerWarp);
 
 // Blocks [0, nb_ad) run adaptive-model tasks, the rest Meta8 tasks; each
 // warp takes 8 consecutive tasks of its list (4 lanes per task).
-__global__ void __launch_bounds__(kRansWarps * 32) k_rans(const Job* __restrict__ jobs,
-                                                          const uint32_t* __restrict__ job_lens,
-                                                          const uint8_t* __restrict__ streams, uint8_t* __restrict__ ans,
+__global__ void __launch_bounds__(kRansWarps * 32) k_rans(const TaskDesc* __restrict__ lists, uint32_t list_cap,
+                                                          const uint32_t* __restrict__ counts, uint32_t nb_ad,
                                                           const EncSym* __restrict__ tabs,
                                                           const EncSym* __restrict__ meta8,
-                                                          const uint8_t* __restrict__ ctxlut,
-                                                          const uint32_t* __restrict__ lists, uint32_t list_cap,
-                                                          const uint32_t* __restrict__ counts, uint32_t nb_ad,
-                                                          const uint8_t* __restrict__ s3base,
-                                                          const S3Frame* __restrict__ s3f, TaskOut* __restrict__ outs) {
+                                                          const uint8_t* __restrict__ ctxlut, TaskOut* __restrict__ outs) {
     extern __shared__ __align__(16) uint8_t smem_r[];
     __shared__ uint8_t s_lut[256];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool m8 = blockIdx.x >= nb_ad;
     const uint32_t nlist = counts[m8 ? 1 : 0];
+    const TaskDesc* dl = lists + (m8 ? list_cap : 0);
     const uint32_t wg = (m8 ? blockIdx.x - nb_ad : blockIdx.x) * kRansWarps + warp;  // warp index in its list
     EncSym* wtab = reinterpret_cast<EncSym*>(smem_r + warp * kRansTabBytes);
     uint4* wring = reinterpret_cast<uint4*>(smem_r + kRansWarps * kRansTabBytes + warp * kRingBytesPerWarp);
@@ -625,46 +693,24 @@ __global__ void __launch_bounds__(kRansWarps * 32) k_rans(const Job* __restrict_
         // the block shares the 8 static models; every warp holds a copy
         for (uint32_t i = lane; i < 8 * 256; i += 32) wtab[i] = meta8[i];
         if (warp == 0) for (uint32_t i = lane; i < 256; i += 32) s_lut[i] = ctxlut[i];
-    }
-    const uint32_t slot = lane >> 2, l = lane & 3;
-    const uint32_t ti = wg * 8 + slot;
-    const bool have = ti < nlist;
-    uint32_t j = 0;
-    int t = 0;
-    if (have) {
-        const uint32_t e = lists[(m8 ? 1 : 0) * list_cap + ti];
-        j = e >> 3;
-        t = (int)(e & 7);
-    }
-    if (!m8) {
+    } else {
         // this warp's 8 adaptive tables
         for (uint32_t k = 0; k < 8; k++) {
             const uint32_t tk = wg * 8 + k;
             if (tk >= nlist) break;
-            const uint32_t e = lists[tk];
-            const uint32_t jj = e >> 3, tt = e & 7;
-            const uint32_t mi = tt == T_LIT ? 0 : tt == T_S3 ? 4 : 1 + (tt - 1) / 2;
-            const EncSym* src = tabs + ((uint64_t)jj * kModels + mi) * 256;
+            const EncSym* src = tabs + (uint64_t)dl[tk].tab * 256;
             for (uint32_t i = lane; i < 256; i += 32) wtab[k * 256 + i] = src[i];
         }
     }
+    const uint32_t slot = lane >> 2, l = lane & 3;
+    const uint32_t ti = wg * 8 + slot;
     __syncthreads();
-    if (!have) return;
-    const Job job = jobs[j];
-    const uint32_t* lens = job_lens + (uint64_t)j * S_COUNT;
-    const uint32_t n = task_len(lens, t, t == T_S3 ? s3_task_nd(s3f[j]) : 0u);
-    const uint8_t* src;
-    if (t == T_S3) {
-        src = s3base + job.s3_off;  // the distance codes
-    } else {
-        const int s = t == T_LIT ? S_LIT : S_OP + (t - 1) / 2;
-        src = streams + job.str_off + stream_base(job, s);
-    }
-    uint8_t* base = ans + job.ans_off + ans_task_off(job, t);
-    LaneIO io = lane_io(base, task_cap(job, t), l);
-    TaskOut* o = outs + (uint64_t)j * T_COUNT + t;
-    if (m8) rans_lane<true>(src, n, l, wtab, s_lut, wring, io, &o->state[l], &o->count[l]);
-    else rans_lane<false>(src, n, l, wtab + slot * 256, nullptr, wring, io, &o->state[l], &o->count[l]);
+    if (ti >= nlist) return;
+    const TaskDesc d = dl[ti];
+    LaneIO io = lane_io(d.base, d.cap, l);
+    TaskOut* o = outs + d.out;
+    if (m8) rans_lane<true>(d.src, d.n, l, wtab, s_lut, wring, io, &o->state[l], &o->count[l]);
+    else rans_lane<false>(d.src, d.n, l, wtab + slot * 256, nullptr, wring, io, &o->state[l], &o->count[l]);
 }
 
 // ---------------------------------------------------------------------------

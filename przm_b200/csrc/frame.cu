@@ -12,7 +12,11 @@
 // assembleContainer (compress.go:962-985).
 // Profile 2 is profile 1 with Section 3 as PackageOffsetsSection of the
 // frame's distances (distance.go:825-849, compress.go:956), empty when the
-// frame has no distance.
+// frame has no distance.  Profile 3 is profile 2 with Section 4 as
+// PackageLiteralsSection (literals.go:664-693, compress.go:957): the
+// smallest of the raw literals, their adaptive container and the four
+// étale-sheaf foliations (PackEtaleSheaf :600-631, assembleSheafContainer
+// :645-662), under profile 1's decodability rule when raw wins.
 #include "common.cuh"
 
 namespace pz {
@@ -69,8 +73,8 @@ __device__ inline void plan_s3(Plan& p, const Job& job, const uint32_t* lens, co
 
 __global__ void k_plan(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs, const uint32_t* __restrict__ job_lens,
                        const TableInfo* __restrict__ infos, const TaskOut* __restrict__ outs,
-                       const uint8_t* __restrict__ streams, const S3Frame* __restrict__ s3f, Plan* __restrict__ plans,
-                       uint32_t* __restrict__ sizes) {
+                       const uint8_t* __restrict__ streams, const S3Frame* __restrict__ s3f,
+                       const uint8_t* __restrict__ fibbase, Plan* __restrict__ plans, uint32_t* __restrict__ sizes) {
     const uint32_t jl = blockIdx.x * blockDim.x + threadIdx.x;
     if (jl >= njobs) return;
     const uint32_t j = j0 + jl;
@@ -133,7 +137,38 @@ __global__ void k_plan(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs
                 const uint32_t e = tsum(outs[(uint64_t)j * T_COUNT + T_LIT]);
                 if (e <= (8u << 20)) { vans = true; vsz = 8 + infos[(uint64_t)j * kModels].mat_len + 16 + e; }
             }
-            if (vans && (vsz < lit || !raw_ok)) { p.s4_mode = 1; p.l4 = vsz; }
+            uint32_t choice = 0;  // 0 raw, 1 adaptive container, 2 a foliation
+            uint32_t best = lit;
+            if (job.profile >= 3 && lit <= kFibMax) {
+                // PackageLiteralsSection: strictly smaller wins, adaptive first, then modes 0-3
+                if (vans && vsz < best) { best = vsz; choice = 1; }
+                const uint32_t* fl = reinterpret_cast<const uint32_t*>(fibbase + job.fib_off);
+                for (uint32_t m = 0; m < 4; m++) {
+                    uint32_t fe[4], sl = 40;
+                    for (uint32_t k = 0; k < 4; k++) {
+                        const uint32_t l = fl[4 * m + k];
+                        fe[k] = 0;
+                        if (l == 0) continue;
+                        const uint32_t e = tsum(outs[(uint64_t)j * T_COUNT + T_FIB + 4 * m + k]);
+                        const uint32_t el = e <= (8u << 20)
+                                                ? infos[(uint64_t)j * kModels + kFibModel + 4 * m + k].mat_len + 16 + e
+                                                : 0xFFFFFFFFu;
+                        fe[k] = el < l ? el : l;
+                        sl += fe[k];
+                    }
+                    if (sl < best) {
+                        best = sl;
+                        choice = 2;
+                        p.s4_sheaf = m;
+                        for (uint32_t k = 0; k < 4; k++) p.fe[k] = fe[k];
+                    }
+                }
+            } else if (vans && (vsz < lit || !raw_ok)) {
+                choice = 1;
+            }
+            if (choice == 0 && !raw_ok && vans) choice = 1;  // the raw bytes would be misread as a container
+            if (choice == 1) { p.s4_mode = 1; p.l4 = vsz; }
+            else if (choice == 2) { p.s4_mode = 2; p.l4 = best; }
             else if (!raw_ok) fallback = true;
         }
         const bool ext = n > 65535 || p.l2 > 65535 || p.l3 > 65535 || p.wlog > 16;
@@ -208,7 +243,66 @@ __device__ void write_container(uint8_t* dst, uint8_t flags, uint32_t n, const T
 constexpr uint32_t kAsmChunk = 4 * kStitchRounds;  // literal bytes (symbols) per part
 static_assert(16 * kAsmThreads == kStitchRounds, "a literal part is one stitch pass");
 
-__host__ __device__ inline uint32_t asm_lit_parts(const Job& j) { return j.n == 0 ? 0u : (j.lit_cap + kAsmChunk - 1) / kAsmChunk; }
+// Parts after part 0: the literal chunks, and for P3 four more (the four
+// fibers of a foliation take at most floor(n / kAsmChunk) + 4 chunks).
+__host__ __device__ inline uint32_t asm_lit_parts(const Job& j) {
+    return j.n == 0 ? 0u : (j.lit_cap + kAsmChunk - 1) / kAsmChunk + (j.profile >= 3 ? 4u : 0u);
+}
+
+// Sheaf container (assembleSheafContainer, literals.go:645-662): 'V','A',01,
+// 0x01 | 0x04 | mode << 4, LE32 n, LE32 fiber lengths x 4, LE32 fiber bytes
+// x 4, then the fibers; a coded fiber is its V-ANS body (matrix, four
+// states, stream).  The head: the 40 bytes and every coded fiber's matrix
+// and states.
+__device__ void sheaf_head(const Job& job, const Plan& p, uint32_t j, uint32_t n, const uint8_t* fibbase,
+                           const TableInfo* infos, const TaskOut* outs, uint8_t* s4) {
+    const uint32_t m = p.s4_sheaf;
+    const uint32_t* fl = reinterpret_cast<const uint32_t*>(fibbase + job.fib_off) + 4 * m;
+    if (threadIdx.x == 0) {
+        s4[0] = 'V'; s4[1] = 'A'; s4[2] = 0x01; s4[3] = (uint8_t)(0x01 | 0x04 | (m << 4));
+        put32(s4 + 4, n);
+        for (int k = 0; k < 4; k++) { put32(s4 + 8 + 4 * k, fl[k]); put32(s4 + 24 + 4 * k, p.fe[k]); }
+    }
+    uint32_t o = 40;
+    for (uint32_t k = 0; k < 4; k++) {
+        if (fl[k] && p.fe[k] < fl[k]) {
+            const TableInfo* inf = infos + (uint64_t)j * kModels + kFibModel + 4 * m + k;
+            const TaskOut& to = outs[(uint64_t)j * T_COUNT + T_FIB + 4 * m + k];
+            const uint32_t ml = inf->mat_len;
+            block_copy(s4 + o, inf->mat, ml);
+            if (threadIdx.x < 4) put32(s4 + o + ml + 4 * threadIdx.x, to.state[threadIdx.x]);
+        }
+        o += p.fe[k];
+    }
+}
+
+// Chunk q of the chosen foliation's fibers (fiber after fiber, kAsmChunk
+// symbols each): a stitch pass of a coded fiber or a slice of a raw one.
+__device__ void sheaf_part(const Job& job, const Plan& p, uint32_t j, uint32_t q, const uint8_t* fibbase,
+                           const TableInfo* infos, const TaskOut* outs, const uint8_t* abase, uint8_t* s4) {
+    const uint32_t m = p.s4_sheaf;
+    const uint32_t* fl = reinterpret_cast<const uint32_t*>(fibbase + job.fib_off);
+    uint32_t o = 40;
+    for (uint32_t k = 0; k < 4; k++) {
+        const uint32_t l = fl[4 * m + k], passes = (l + kAsmChunk - 1) / kAsmChunk;
+        if (q < passes) {
+            const FibGeom g = fib_geom(job, fl, m, k);
+            if (p.fe[k] < l) {
+                const uint8_t* tb = abase + g.ans_off;
+                const TaskOut to = outs[(uint64_t)j * T_COUNT + T_FIB + 4 * m + k];
+                const uint32_t h = infos[(uint64_t)j * kModels + kFibModel + 4 * m + k].mat_len + 16;
+                const uint32_t r0 = q * kStitchRounds;
+                stitch_pass<kAsmThreads>(tb, l, l, r0, s4 + o + h + stitch_offset(tb, l, l, to, r0));
+            } else {
+                const uint32_t lo = q * kAsmChunk;
+                block_copy(s4 + o + lo, fibbase + job.fib_off + g.byte_off + lo, min(kAsmChunk, l - lo));
+            }
+            return;
+        }
+        q -= passes;
+        o += p.fe[k];
+    }
+}
 
 // Four blocks per SM (64 registers): the parts are short and latency-bound.
 __global__ void __launch_bounds__(kAsmThreads, 4) k_assemble(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
@@ -219,7 +313,8 @@ __global__ void __launch_bounds__(kAsmThreads, 4) k_assemble(const uint8_t* __re
                                                           const uint8_t* __restrict__ streams,
                                                           const uint8_t* __restrict__ ans,
                                                           const uint8_t* __restrict__ s3base,
-                                                          const S3Frame* __restrict__ s3f, uint8_t* __restrict__ out) {
+                                                          const S3Frame* __restrict__ s3f,
+                                                          const uint8_t* __restrict__ fibbase, uint8_t* __restrict__ out) {
     for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
         const uint32_t j = items[it].x, part = items[it].y;
         const Job job = jobs[j];
@@ -248,7 +343,9 @@ __global__ void __launch_bounds__(kAsmThreads, 4) k_assemble(const uint8_t* __re
         uint8_t* s4 = f + w + 8 + p.l2 + p.l3;
         if (part > 0) {  // Section 4 literals, part - 1
             const uint32_t k = part - 1, len = lens[S_LIT];
-            if (p.s4_mode == 1) {
+            if (p.s4_mode == 2) {
+                sheaf_part(job, p, j, k, fibbase, infos, outs, abase, s4);
+            } else if (p.s4_mode == 1) {
                 const uint32_t r0 = k * kStitchRounds;
                 if (r0 < (len + 3) / 4) {
                     const TaskOut to = outs[(uint64_t)j * T_COUNT + T_LIT];
@@ -351,6 +448,8 @@ __global__ void __launch_bounds__(kAsmThreads, 4) k_assemble(const uint8_t* __re
         // Section 4: the container head here, the literals in parts 1, 2, ...
         if (p.s4_mode == 1)
             container_head(s4, 0x00, lens[S_LIT], infos + (uint64_t)j * kModels, outs[(uint64_t)j * T_COUNT + T_LIT]);
+        else if (p.s4_mode == 2)
+            sheaf_head(job, p, j, lens[S_LIT], fibbase, infos, outs, s4);
     }
 }
 

@@ -33,6 +33,7 @@ MaxTileLitBytes = 36864
 PROFILE_D2D = 0
 PROFILE_ANS = 1
 PROFILE_ANS_DIST = 2  # PROFILE_ANS with Section 3 as PackageOffsetsSection (the CPU compressor's Section 3)
+PROFILE_ANS_SHEAF = 3  # PROFILE_ANS_DIST with Section 4 as PackageLiteralsSection (sheaf foliations)
 TUNING_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
 NORM_GO = 0
 NORM_CPU = 1
@@ -459,8 +460,8 @@ class GPUCompressor:
 
     def Compress(self, src, profile: int = PROFILE_ANS) -> tuple[bytes, GPUProfile]:
         """One frame: PROFILE_D2D (CompressD2D bytes), PROFILE_ANS (match +
-        tokenize + ANS frame, input < 16 MiB) or PROFILE_ANS_DIST (that frame
-        with a coded Section 3)."""
+        tokenize + ANS frame, input < 16 MiB), PROFILE_ANS_DIST (that frame
+        with a coded Section 3) or PROFILE_ANS_SHEAF (and a coded Section 4)."""
         a = _u8(src)
         cap = FrameBound(len(a))
         out = np.zeros(cap, np.uint8)
@@ -592,6 +593,32 @@ class GPUCompressor:
                                                 _ptr(ol), _ptr(nb), stream))
         return ol[: len(ln)], nb[: len(ln)]
 
+    # -- the GPU decoder (decompress.go:380-700 semantics) --
+    def Decompress(self, frame) -> bytes:
+        """Decompress (api.go:44) on the device: one frame from host memory."""
+        f = _u8(frame)
+        if len(f) >= 8 and bytes(f[:4]) == b"PRZM":
+            u = int(f[5]) | int(f[6]) << 8 | int(f[7]) << 16
+        else:
+            u = 0
+        out = np.zeros(max(u, 1), np.uint8)
+        n = C.c_uint64()
+        _check(L().przmg_decompress(self._h, _ptr(f) if len(f) else None, len(f), _ptr(out), len(out), C.byref(n)))
+        return bytes(out[: n.value])
+
+    def DecompressBatchDevice(self, dSrc: int, srcOffs, srcLens, dDst: int, dstOffs, dstCaps,
+                              stream: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        """Device-resident frames decoded on the device: (statuses, sizes)."""
+        so = np.ascontiguousarray(srcOffs, np.uint64)
+        sl = np.ascontiguousarray(srcLens, np.uint32)
+        do = np.ascontiguousarray(dstOffs, np.uint64)
+        dc = np.ascontiguousarray(dstCaps, np.uint32)
+        st = np.zeros(max(len(sl), 1), np.int32)
+        ol = np.zeros(max(len(sl), 1), np.uint64)
+        _check(L().przmg_decompress_batch_device(self._h, dSrc, _ptr(so), _ptr(sl), len(sl), dDst, _ptr(do), _ptr(dc),
+                                                 _ptr(st), _ptr(ol), stream))
+        return st[: len(sl)], ol[: len(sl)]
+
     # -- benchmarks --
     def BenchmarkVRAMBandwidth(self, sizeMB: int = 256, iterations: int = 10) -> float:
         g = C.c_double()
@@ -663,6 +690,13 @@ class DeviceBatch:
         _check(L().przmg_batch_download(self._h, C.c_void_p(host_out.ctypes.data), host_out.nbytes, C.byref(total),
                                         _ptr(sizes), stream))
         return total.value, sizes[: len(self.sizes)]
+
+    def verify(self) -> int:
+        """Every frame of the last run decoded on the device and compared with
+        its input there: the number of frames that do not round-trip."""
+        bad = C.c_uint64()
+        _check(L().przmg_batch_verify(self._h, C.byref(bad)))
+        return bad.value
 
     STAT_KEYS = ("input_bytes", "frame_bytes", "literal_bytes", "command_bytes", "offset_bytes", "rans_symbols",
                  "rans_emitted_bytes", "uncompressed_frames")

@@ -147,3 +147,29 @@ def parity_cases(max_n: int = 1 << 20, seed: int = 11) -> list[tuple[str, np.nda
         for k, a in kinds(n, seed + n).items():
             cases.append((f"{k}-{n}", a))
     return cases
+
+
+def ident_text(n: int, seed: int) -> np.ndarray:
+    """Lower-case identifiers, each followed by one syntax byte (the order-2
+    foliation, mode 3, codes it best)."""
+    rng = np.random.default_rng(seed)
+    alpha = np.frombuffer(b"abcdefghijklmnopqrstuvwxyz_", np.uint8)
+    punct = np.frombuffer(b"(){};,.=+ ", np.uint8)
+    out, size = [], 0
+    while size < n:
+        w = alpha[rng.integers(0, len(alpha), int(rng.integers(2, 9)))]
+        out += [w, punct[rng.integers(0, len(punct), 1)]]
+        size += len(w) + 1
+    return np.concatenate(out)[:n].copy()
+
+
+def tagged_numbers(n: int, seed: int) -> np.ndarray:
+    """An upper-case letter, a decimal number and a separator, repeated (the
+    two-way foliation, mode 2, codes it best)."""
+    rng = np.random.default_rng(seed)
+    parts, size = [], 0
+    while size < n:
+        s = b"%c%d%c" % (65 + int(rng.integers(0, 26)), int(rng.integers(0, 10 ** 6)), b" ,;"[int(rng.integers(0, 3))])
+        parts.append(s)
+        size += len(s)
+    return np.frombuffer(b"".join(parts)[:n], np.uint8).copy()

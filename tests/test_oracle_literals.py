@@ -103,3 +103,14 @@ def test_p3_json_frame_carries_a_foliation():
     sec, nib = O.package_literals(lits)
     assert nib == 0x80 and sec[3] & 0x04  # a sheaf container wins on this text
     assert f.endswith(sec) and f[4] & 0x80
+
+
+def test_p3_section4_forms_of_the_test_inputs():
+    # the Section 4 forms tests/test_gpu_coded_sections.py expects the device
+    # to reproduce: raw, the adaptive container and every foliation
+    from tests import inputs as I
+    from tests.frames import section4_form
+    xs = [a for n in (4096, 20_000, 200_000) for a in I.kinds(n, 5 + n).values()]
+    xs += [I.ident_text(200_000, 7), I.tagged_numbers(20_000, 7)]
+    forms = {section4_form(O.compress_p3(a)) for a in xs}
+    assert {"raw", "AD", "SH0", "SH1", "SH2", "SH3"} <= forms, forms
