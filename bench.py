@@ -473,9 +473,11 @@ def decode_measure(comp, batch, reps: int = 3) -> dict:
     device-resident: GB/s of decoded bytes (median of reps, CUDA events on
     the call's stream), every frame compared with its input on the device
     (przmg_batch_verify, untimed)."""
+    import numpy as np
     import torch
     from przm_b200 import devmem
     sizes = [int(x) for x in batch.sizes]
+    batch.enqueue(graph=True)  # the frames again: the link measurement used d_out as scratch
     fs = batch.frame_sizes()
     dcap = [max(n, 1) for n in sizes]
     doffs = np.zeros(len(sizes), np.uint64)

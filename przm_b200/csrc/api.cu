@@ -155,6 +155,11 @@ struct przmg_batch {
     DevBuf d_asm_job;     // the same items grouped by input (plain per-input launches)
     DevBuf d_s3, d_s3f;   // P2 and up: per-input Section 3 regions and their S3Frame facts
     DevBuf d_fib;         // P3: per-input fiber regions
+    // P2 and up: the Mode 12 chains run on a second stream, forked after the
+    // distance codes exist and joined before the plan (graph capture keeps
+    // the two branches)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // per input i, where its items start in each work list ([i + 1] = end)
     std::vector<uint32_t> job_small0, job_rt0, job_big0, job_tile0, job_asm0;
     int launches_plain = 0;
@@ -173,7 +178,13 @@ struct przmg_batch {
     // the batch holds one input and its match table from a completed
     // one-input call (what the tokenizer-only entry points run on)
     bool staged_single = false;
-    ~przmg_batch() { drop_graph(); release(); }
+    ~przmg_batch() {
+        drop_graph();
+        release();
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (aux) cudaStreamDestroy(aux);
+    }
     void drop_graph() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
@@ -416,6 +427,11 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     CK(b->d_s3.ensure(s3 + 64));
     CK(b->d_s3f.ensure(sizeof(S3Frame) * std::max<uint32_t>(njobs, 1)));
     CK(b->d_fib.ensure(fib + 64));
+    if (profile >= 2 && !b->aux) {
+        CK(cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
+    }
     CK(b->d_ans.ensure(b->ans_bytes));
     CK(b->d_outs.ensure((size_t)njobs * T_COUNT * sizeof(TaskOut) + 16));
     CK(b->d_plans.ensure((size_t)njobs * sizeof(Plan) + 16));
@@ -631,9 +647,18 @@ static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, cons
                                                       b->d_s3f.as<S3Frame>(), b->err_word());
                 CK(cudaGetLastError());
                 launches++;
+                // the Mode 12 chains (one thread per frame, serial by the
+                // format) on the second stream, beside the rANS launch
+                CK(cudaEventRecord(b->ev_fork, s));
+                CK(cudaStreamWaitEvent(b->aux, b->ev_fork, 0));
+                k_s3_chain<<<(R.nj + 31) / 32, 32, 0, b->aux>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_s3.as<uint8_t>(),
+                                                               b->d_s3f.as<S3Frame>(), c->d_dist12.as<EncSym>());
+                CK(cudaGetLastError());
+                CK(cudaEventRecord(b->ev_join, b->aux));
+                launches++;
             }
             if (b->profile >= 3) {  // Section 4: the literals' four foliations
-                k_frame_fibers<<<dim3(R.nj, 4), 1024, 0, s>>>(b->d_jobs.as<Job>(), R.j0, b->d_job_lens.as<uint32_t>(),
+                k_frame_fibers<<<dim3(R.nj, 4), kFibThreads, 0, s>>>(b->d_jobs.as<Job>(), R.j0, b->d_job_lens.as<uint32_t>(),
                                                              b->d_streams.as<uint8_t>(), b->d_fib.as<uint8_t>());
                 CK(cudaGetLastError());
                 launches++;
@@ -654,17 +679,12 @@ static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, cons
             const uint32_t nad = (b->profile >= 3 ? kModels : b->profile >= 2 ? 5 : 4) * R.nj;  // adaptive tasks at most
             const uint32_t nb_ad = (nad + 8 * kRansWarps - 1) / (8 * kRansWarps);
             const uint32_t nb_m8 = (3 * R.nj + 8 * kRansWarps - 1) / (8 * kRansWarps);
-            if (b->profile >= 2) {  // the Mode 12 chains
-                k_s3_chain<<<(R.nj + 31) / 32, 32, 0, s>>>(b->d_jobs.as<Job>(), R.j0, R.nj, b->d_s3.as<uint8_t>(),
-                                                          b->d_s3f.as<S3Frame>(), c->d_dist12.as<EncSym>());
-                CK(cudaGetLastError());
-                launches++;
-            }
             k_rans<<<nb_ad + nb_m8, kRansWarps * 32, kRansSmem, s>>>(lists, list_cap, counts, nb_ad,
                                                                     b->d_tabs.as<EncSym>(), c->d_meta8.as<EncSym>(),
                                                                     c->d_ctxlut.as<uint8_t>(), b->d_outs.as<TaskOut>());
             CK(cudaGetLastError());
             launches += 3;
+            if (b->profile >= 2) CK(cudaStreamWaitEvent(s, b->ev_join, 0));  // the Mode 12 chains
             CK(mark(7));
         } else {
             CK(mark(6));

@@ -383,16 +383,88 @@ __device__ uint32_t dec_matrix(const uint8_t* s, uint32_t slen, uint16_t* freq) 
     return sum == 4096 ? p : 0;
 }
 
-// One renormalisation: bytes enter x from the stream while x < 2^16.
-__device__ __forceinline__ bool dec_renorm(uint32_t& x, const uint8_t* s, uint32_t slen, uint32_t& p) {
-    while (x < 65536u) {
-        if (p >= slen) return false;
-        x = (x << 8) | s[p++];
+// The stream as the chain reads it: the next `av` bytes in w (first byte
+// lowest) and the four after them prefetched in nx, loaded a round ahead so
+// their latency stays off the chain.  renorm shifts bytes into x while x <
+// 2^16 (the reference's renormalisation) and fails where the stream ends.
+struct ByteWin {
+    const uint8_t* s;
+    uint32_t slen, q;  // q: next byte not yet loaded
+    uint64_t w;
+    uint32_t av, nx, nn;
+    __device__ __forceinline__ void init(const uint8_t* src, uint32_t len, uint32_t p) {
+        s = src;
+        slen = len;
+        q = p;
+        w = 0;
+        av = 0;
+        nx = 0;
+        nn = 0;
     }
-    return true;
-}
+    __device__ __forceinline__ void prefetch() {
+        if (nn == 0 && q < slen) {
+            const uint32_t m = min(4u, slen - q);
+            uint32_t v = 0;
+#pragma unroll
+            for (uint32_t i = 0; i < 4; i++) v |= (i < m ? (uint32_t)s[q + i] : 0u) << (8 * i);
+            nx = v;
+            nn = m;
+            q += m;
+        }
+    }
+    __device__ __forceinline__ void merge() {
+        if (nn && av <= 4) {
+            w |= (uint64_t)nx << (8 * av);
+            av += nn;
+            nn = 0;
+        }
+    }
+    // once per round: the prefetched bytes in, the next ones requested
+    __device__ __forceinline__ void step() {
+        merge();
+        prefetch();
+    }
+    __device__ __forceinline__ bool renorm(uint32_t& x) {
+        while (x < 65536u) {
+            if (av == 0) {
+                merge();
+                if (av == 0) {
+                    prefetch();
+                    merge();
+                    if (av == 0) return false;
+                }
+            }
+            x = (x << 8) | (uint32_t)(w & 0xFFu);
+            w >>= 8;
+            av--;
+        }
+        return true;
+    }
+    __device__ __forceinline__ uint32_t pos() const { return q - nn - av; }  // bytes consumed
+};
 
 constexpr uint32_t kDecEntropySmem = 4096 * 4 + 256 * 2;  // decode table + frequencies
+
+// Bytes [p, p + 8) of s as a little-endian word (two aligned loads; the
+// caller keeps p + 16 <= the stream's length, and s is never within 8 bytes
+// of its buffer's start: every coded stream follows a frame header).
+__device__ __forceinline__ uint64_t ld64_at(const uint8_t* s, uint32_t p) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(s + p);
+    const uint64_t* w = reinterpret_cast<const uint64_t*>(a & ~uintptr_t(7));
+    const uint32_t sh = (uint32_t)(a & 7) * 8;
+    const uint64_t lo = w[0], hi = w[1];
+    return sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
+}
+
+// Bytes a state needs after a decode step: x' = f (x >> 12) + j >= 16 when
+// x >= 2^16, so 0, 1 or 2 (the reference's loop runs while x < 2^16).
+__device__ __forceinline__ uint32_t renorm_bytes(uint32_t x) { return (x < 65536u ? 1u : 0u) + (x < 256u ? 1u : 0u); }
+// x shifted by k bytes, taking them from u (first byte lowest) in stream order
+__device__ __forceinline__ uint32_t renorm_apply(uint32_t x, uint32_t k, uint32_t u) {
+    const uint32_t v = k == 2 ? __byte_perm(u, 0, 0x4401) : (k == 1 ? (u & 0xFFu) : 0u);
+    return (x << (8 * k)) | v;
+}
+
 
 // One warp per task (tasks[blockIdx.x]): blocks of one warp, so the serial
 // chains spread over the SMs.
@@ -439,14 +511,44 @@ __global__ void __launch_bounds__(32) k_dec_entropy(const DecTask* __restrict__ 
         p += 16;
         uint32_t i = 0;
         bool ok = true;
+        if (x0 >= 65536u && x1 >= 65536u && x2 >= 65536u && x3 >= 65536u) {
+            // Rounds of four symbols: each lane's byte count comes from its
+            // own state, so their offsets in the round's 8 bytes are a
+            // 4-element prefix sum and the lanes renormalise side by side;
+            // only the stream position links one round to the next.
+            for (; i + 4 <= n && p + 16 <= slen; i += 4) {
+                const uint64_t v = ld64_at(s, p);
+                const uint32_t e0 = tab[x0 & 4095], e1 = tab[x1 & 4095], e2 = tab[x2 & 4095], e3 = tab[x3 & 4095];
+                x0 = dec_next(x0, e0);
+                x1 = dec_next(x1, e1);
+                x2 = dec_next(x2, e2);
+                x3 = dec_next(x3, e3);
+                const uint32_t k0 = renorm_bytes(x0), k1 = renorm_bytes(x1), k2 = renorm_bytes(x2), k3 = renorm_bytes(x3);
+                const uint32_t o1 = k0, o2 = o1 + k1, o3 = o2 + k2;
+                x0 = renorm_apply(x0, k0, (uint32_t)v);
+                x1 = renorm_apply(x1, k1, (uint32_t)(v >> (8 * o1)));
+                x2 = renorm_apply(x2, k2, (uint32_t)(v >> (8 * o2)));
+                x3 = renorm_apply(x3, k3, (uint32_t)(v >> (8 * o3)));
+                p += o3 + k3;
+                dst[i] = (uint8_t)e0;
+                dst[i + 1] = (uint8_t)e1;
+                dst[i + 2] = (uint8_t)e2;
+                dst[i + 3] = (uint8_t)e3;
+            }
+        }
+        // the rest (the stream's last 16 bytes, or initial states below 2^16)
+        // byte by byte
+        ByteWin bw;
+        bw.init(s, slen, p);
+        bw.prefetch();
         for (; i + 4 <= n && ok; i += 4) {  // vans_run_4x_loop, przm_dec.c:201-255
+            bw.step();
             const uint32_t e0 = tab[x0 & 4095], e1 = tab[x1 & 4095], e2 = tab[x2 & 4095], e3 = tab[x3 & 4095];
             x0 = dec_next(x0, e0);
             x1 = dec_next(x1, e1);
             x2 = dec_next(x2, e2);
             x3 = dec_next(x3, e3);
-            ok = dec_renorm(x0, s, slen, p) && dec_renorm(x1, s, slen, p) && dec_renorm(x2, s, slen, p) &&
-                 dec_renorm(x3, s, slen, p);
+            ok = bw.renorm(x0) && bw.renorm(x1) && bw.renorm(x2) && bw.renorm(x3);
             dst[i] = (uint8_t)e0;
             dst[i + 1] = (uint8_t)e1;
             dst[i + 2] = (uint8_t)e2;
@@ -454,10 +556,11 @@ __global__ void __launch_bounds__(32) k_dec_entropy(const DecTask* __restrict__ 
         }
         uint32_t xs[4] = {x0, x1, x2, x3};
         for (; i < n && ok; i++) {
+            bw.step();
             const uint32_t e = tab[xs[i & 3] & 4095];
             dst[i] = (uint8_t)e;
             xs[i & 3] = dec_next(xs[i & 3], e);
-            ok = dec_renorm(xs[i & 3], s, slen, p);
+            ok = bw.renorm(xs[i & 3]);
         }
         if (!ok) dec_fail(infos, t.frame, D_CORRUPT);
         return;
@@ -465,28 +568,36 @@ __global__ void __launch_bounds__(32) k_dec_entropy(const DecTask* __restrict__ 
     if (lane != 0) return;
     if (t.kind == DT_META8) {  // przm_vans_decode_meta8, przm_dec.c:459-500
         uint32_t xs[4] = {drd32(s + 8), drd32(s + 12), drd32(s + 16), drd32(s + 20)};
-        uint32_t p = 24, prev = 0;
+        uint32_t prev = 0;
+        ByteWin bw;
+        bw.init(s, slen, 24);
+        bw.prefetch();
         bool ok = true;
         for (uint32_t i = 0; i < n && ok; i++) {
             const uint32_t l = i & 3;
+            if (l == 0) bw.step();
             const uint32_t e = __ldg(&st->m8[ctx_meta8(prev)][xs[l] & 4095]);
             dst[i] = (uint8_t)e;
             prev = e & 0xFFu;
             xs[l] = dec_next(xs[l], e);
-            ok = dec_renorm(xs[l], s, slen, p);
+            ok = bw.renorm(xs[l]);
         }
-        if (!ok || p != slen) dec_fail(infos, t.frame, D_CORRUPT);
+        if (!ok || bw.pos() != slen) dec_fail(infos, t.frame, D_CORRUPT);
         return;
     }
     // DT_MODE12: przm_vans_decode_dist4, przm_dec.c:958-990
-    uint32_t x = drd32(s + 1), p = 5, prev = 0;
+    uint32_t x = drd32(s + 1), prev = 0;
+    ByteWin bw;
+    bw.init(s, slen, 5);
+    bw.prefetch();
     bool ok = true;
     for (uint32_t i = 0; i < n && ok; i++) {
+        if ((i & 1) == 0) bw.step();
         const uint32_t e = __ldg(&st->d12[s3_ctx(prev)][x & 4095]);
         dst[i] = (uint8_t)e;
         prev = e & 0xFFu;
         x = dec_next(x, e);
-        ok = dec_renorm(x, s, slen, p);
+        ok = bw.renorm(x);
     }
     if (!ok) dec_fail(infos, t.frame, D_CORRUPT);
 }
@@ -564,22 +675,32 @@ __global__ void __launch_bounds__(1024) k_dec_prefix(DecInfo* __restrict__ infos
 // Literals of a sheaf frame from their fibers (przm_reconstitute_fibers,
 // przm_dec.c:354-394); one thread per frame.
 __global__ void k_dec_sheaf(DecInfo* __restrict__ infos, uint32_t nf) {
+    __shared__ ClassLut s_lut[4];
+    for (uint32_t m = 0; m < 4; m++) class_lut_build(s_lut[m], m, threadIdx.x, blockDim.x);
+    __syncthreads();
     const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nf) return;
     const DecInfo I = infos[f];
     if (I.err || !I.sheaf) return;
-    const uint8_t* fb[4];
-    uint32_t ptr[4] = {0, 0, 0, 0};
-    for (int k = 0; k < 4; k++) fb[k] = reinterpret_cast<const uint8_t*>(I.fib[k]);
+    const ClassLut& L = s_lut[I.sheaf_mode];
+    const uint32_t mode = I.sheaf_mode, n = I.lit_len;
+    const uint32_t l0 = I.fl[0], l1 = I.fl[1], l2 = I.fl[2], l3 = I.fl[3];
+    const uint8_t *f0 = reinterpret_cast<const uint8_t*>(I.fib[0]), *f1 = reinterpret_cast<const uint8_t*>(I.fib[1]),
+                  *f2 = reinterpret_cast<const uint8_t*>(I.fib[2]), *f3 = reinterpret_cast<const uint8_t*>(I.fib[3]);
     uint8_t* lit = reinterpret_cast<uint8_t*>(I.lit);
-    uint32_t p1 = 0, p2 = 0;
-    for (uint32_t j = 0; j < I.lit_len; j++) {
-        const uint32_t c = lit_class(p2, p1, I.sheaf_mode);
-        if (ptr[c] >= I.fl[c]) {
+    uint32_t q0 = 0, q1 = 0, q2 = 0, q3 = 0, p1 = 0, p2 = 0;  // per-fiber positions in registers (selected, not indexed)
+    for (uint32_t j = 0; j < n; j++) {
+        const uint32_t c = class_lut(L, p2, p1, mode);
+        const bool ok = c == 0 ? q0 < l0 : c == 1 ? q1 < l1 : c == 2 ? q2 < l2 : q3 < l3;
+        if (!ok) {
             dec_fail(infos, f, D_CORRUPT);
             return;
         }
-        const uint32_t b = fb[c][ptr[c]++];
+        const uint32_t b = c == 0 ? f0[q0] : c == 1 ? f1[q1] : c == 2 ? f2[q2] : f3[q3];
+        q0 += c == 0;
+        q1 += c == 1;
+        q2 += c == 2;
+        q3 += c == 3;
         lit[j] = (uint8_t)b;
         p2 = p1;
         p1 = b;
@@ -659,13 +780,20 @@ __device__ __forceinline__ bool off_leb(const uint8_t* o, uint32_t ol, uint32_t&
     return false;
 }
 
-__device__ __forceinline__ void lru_repeat(uint32_t* r, uint32_t k) {  // update_lru_repeat, przm_dec.c:1161-1166
-    if (k == 0) return;
-    if (k == 1) { const uint32_t t = r[0]; r[0] = r[1]; r[1] = t; return; }
-    if (k == 2) { const uint32_t t = r[2]; r[2] = r[1]; r[1] = r[0]; r[0] = t; return; }
-    const uint32_t t = r[3]; r[3] = r[2]; r[2] = r[1]; r[1] = r[0]; r[0] = t;
-}
-__device__ __forceinline__ void lru_explicit(uint32_t* r, uint32_t d) { r[3] = r[2]; r[2] = r[1]; r[1] = r[0]; r[0] = d; }
+// The four repeat distances in registers (selected, not indexed).
+struct Reps {
+    uint32_t r0, r1, r2, r3;
+    __device__ __forceinline__ uint32_t get(uint32_t k) const { return k == 0 ? r0 : k == 1 ? r1 : k == 2 ? r2 : r3; }
+    // update_lru_repeat, przm_dec.c:1161-1166: entry k moves to the front
+    __device__ __forceinline__ void repeat(uint32_t k) {
+        const uint32_t t = get(k);
+        if (k >= 3) r3 = r2;
+        if (k >= 2) r2 = r1;
+        if (k >= 1) { r1 = r0; r0 = t; }
+    }
+    // update_lru_explicit (:1168-1170)
+    __device__ __forceinline__ void explicit_(uint32_t d) { r3 = r2; r2 = r1; r1 = r0; r0 = d; }
+};
 
 // Warp copies.  Literals: n bytes from src.  Match: n bytes from d back,
 // byte i from byte (i mod d) of the source run (the byte-wise forward copy
@@ -715,9 +843,9 @@ __global__ void __launch_bounds__(32) k_dec_exec(const uint8_t* __restrict__ src
     const uint8_t* lit = reinterpret_cast<const uint8_t*>(I.lit);
     const uint8_t* offs = reinterpret_cast<const uint8_t*>(I.off);
     const uint32_t ll = I.lit_len, ol = I.off_len, bmin = I.bmin, stride = I.stride;
-    uint32_t r[4];
-    if ((I.flags & 0x01) && stride > 1) { r[0] = 1; r[1] = stride; r[2] = 2 * stride; r[3] = 3 * stride; }
-    else { r[0] = 1; r[1] = 4; r[2] = 8; r[3] = 16; }
+    Reps r;
+    if ((I.flags & 0x01) && stride > 1) { r.r0 = 1; r.r1 = stride; r.r2 = 2 * stride; r.r3 = 3 * stride; }
+    else { r.r0 = 1; r.r1 = 4; r.r2 = 8; r.r3 = 16; }
     uint32_t dp = 0, lp = 0, opos = 0, err = D_OK;
     while (dp < u && R.more()) {
         uint32_t op;
@@ -746,8 +874,8 @@ __global__ void __launch_bounds__(32) k_dec_exec(const uint8_t* __restrict__ src
             const int32_t delta = (int32_t)(int8_t)dl;
             const uint32_t mode = (desc >> 6) & 3;
             int64_t dd;
-            if (mode < 3) dd = (int64_t)r[mode] + delta;
-            else dd = stride > 1 ? (int64_t)r[0] + (int64_t)delta * stride : (int64_t)(uint8_t)dl + 1;
+            if (mode < 3) dd = (int64_t)r.get(mode) + delta;
+            else dd = stride > 1 ? (int64_t)r.r0 + (int64_t)delta * stride : (int64_t)(uint8_t)dl + 1;
             if (dd <= 0 || dd > 0xFFFFFFFFll) { err = D_CORRUPT; break; }
             d = (uint32_t)dd;
             llit = (desc >> 3) & 7; lmatch = (desc & 7) + bmin; kind = 2;
@@ -787,11 +915,11 @@ __global__ void __launch_bounds__(32) k_dec_exec(const uint8_t* __restrict__ src
         if (kind == 0) continue;
         if (dp == u) break;
         if (kind == 1) {
-            d = r[k];
-            lru_repeat(r, k);
+            d = r.get(k);
+            r.repeat(k);
         } else {
             if (kind == 3 && !off_leb(offs, ol, opos, d)) { err = D_CORRUPT; break; }
-            lru_explicit(r, d);
+            r.explicit_(d);
         }
         if (d == 0 || d > dp || dp + lmatch > u) { err = D_CORRUPT; break; }  // no dictionary: d <= dp
         warp_copy_match(dst + dp, d, lmatch);
