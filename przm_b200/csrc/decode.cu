@@ -334,9 +334,15 @@ __global__ void k_dec_parse(const uint8_t* __restrict__ src, const DecJob* __res
 // Static decode tables in the adaptive table's entry form (below): the 8
 // Meta8 models (core/commands/vans_meta_tables.go) and the 4 Mode 12
 // distance-code models (core/distance/distance.go:67-93), built on the host.
+// Per context: the symbol of every slot, and per symbol (f - 1) << 20 | its
+// cumulative frequency.  Compact (41 KiB for Meta8), so a decoding warp keeps
+// its model in shared memory: the serial chain's lookups then never wait on
+// L2.
 struct DecStatic {
-    uint32_t m8[8][4096];
-    uint32_t d12[4][4096];
+    uint8_t m8sym[8][4096];
+    uint32_t m8fc[8][256];
+    uint8_t d12sym[4][4096];
+    uint32_t d12fc[4][64];
 };
 
 // Decode-table entry of slot j of symbol s (frequency f): s | j << 8 |
@@ -443,7 +449,10 @@ struct ByteWin {
     __device__ __forceinline__ uint32_t pos() const { return q - nn - av; }  // bytes consumed
 };
 
-constexpr uint32_t kDecEntropySmem = 4096 * 4 + 256 * 2;  // decode table + frequencies
+// the larger of an adaptive body's decode table + frequencies and the Meta8
+// models
+constexpr uint32_t kDecEntropySmem = 8 * 4096 + 8 * 256 * 4;
+static_assert(kDecEntropySmem >= 4096 * 4 + 256 * 2, "adaptive decode table");
 
 // Bytes [p, p + 8) of s as a little-endian word (two aligned loads; the
 // caller keeps p + 16 <= the stream's length, and s is never within 8 bytes
@@ -565,8 +574,18 @@ __global__ void __launch_bounds__(32) k_dec_entropy(const DecTask* __restrict__ 
         if (!ok) dec_fail(infos, t.frame, D_CORRUPT);
         return;
     }
+    // the static models into shared memory (the warp), then the chain (lane 0)
+    const bool m8 = t.kind == DT_META8;
+    const uint32_t nsym = m8 ? 8 * 4096 : 4 * 4096, nfc = m8 ? 8 * 256 : 4 * 64;
+    const uint4* gs = reinterpret_cast<const uint4*>(m8 ? &st->m8sym[0][0] : &st->d12sym[0][0]);
+    const uint4* gf = reinterpret_cast<const uint4*>(m8 ? &st->m8fc[0][0] : &st->d12fc[0][0]);
+    uint8_t* ssym = smem_d;
+    uint32_t* sfc = reinterpret_cast<uint32_t*>(smem_d + nsym);
+    for (uint32_t i = lane; i < nsym / 16; i += 32) reinterpret_cast<uint4*>(ssym)[i] = gs[i];
+    for (uint32_t i = lane; i < nfc / 4; i += 32) reinterpret_cast<uint4*>(sfc)[i] = gf[i];
+    __syncwarp();
     if (lane != 0) return;
-    if (t.kind == DT_META8) {  // przm_vans_decode_meta8, przm_dec.c:459-500
+    if (m8) {  // przm_vans_decode_meta8, przm_dec.c:459-500
         uint32_t xs[4] = {drd32(s + 8), drd32(s + 12), drd32(s + 16), drd32(s + 20)};
         uint32_t prev = 0;
         ByteWin bw;
@@ -576,10 +595,11 @@ __global__ void __launch_bounds__(32) k_dec_entropy(const DecTask* __restrict__ 
         for (uint32_t i = 0; i < n && ok; i++) {
             const uint32_t l = i & 3;
             if (l == 0) bw.step();
-            const uint32_t e = __ldg(&st->m8[ctx_meta8(prev)][xs[l] & 4095]);
-            dst[i] = (uint8_t)e;
-            prev = e & 0xFFu;
-            xs[l] = dec_next(xs[l], e);
+            const uint32_t c = ctx_meta8(prev), slot = xs[l] & 4095;
+            const uint32_t sym = ssym[c * 4096 + slot], fc = sfc[c * 256 + sym];
+            dst[i] = (uint8_t)sym;
+            prev = sym;
+            xs[l] = ((fc >> 20) + 1) * (xs[l] >> 12) + slot - (fc & 0xFFFFFu);
             ok = bw.renorm(xs[l]);
         }
         if (!ok || bw.pos() != slen) dec_fail(infos, t.frame, D_CORRUPT);
@@ -593,10 +613,11 @@ __global__ void __launch_bounds__(32) k_dec_entropy(const DecTask* __restrict__ 
     bool ok = true;
     for (uint32_t i = 0; i < n && ok; i++) {
         if ((i & 1) == 0) bw.step();
-        const uint32_t e = __ldg(&st->d12[s3_ctx(prev)][x & 4095]);
-        dst[i] = (uint8_t)e;
-        prev = e & 0xFFu;
-        x = dec_next(x, e);
+        const uint32_t c = s3_ctx(prev), slot = x & 4095;
+        const uint32_t sym = ssym[c * 4096 + slot], fc = sfc[c * 64 + sym];
+        dst[i] = (uint8_t)sym;
+        prev = sym;
+        x = ((fc >> 20) + 1) * (x >> 12) + slot - (fc & 0xFFFFFu);
         ok = bw.renorm(x);
     }
     if (!ok) dec_fail(infos, t.frame, D_CORRUPT);
