@@ -187,12 +187,14 @@ def measured_peaks() -> tuple[float, str]:
         return 6650.0, "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per encoded
-# symbol of one k_rans launch, from an ncu capture of the same kernel on a
-# smaller batch of the same workload (its traffic grows with the symbols it
-# encodes, so it scales to a full launch by the launch's symbols).  The
-# capture and its command are summarised in profiles/k_rans_mixed16.md.
-RANS_TRAFFIC_PER_SYMBOL: float | None = None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_rans
+# launch per algorithmic byte of that launch (symbols read + bytes emitted),
+# from an ncu capture of the same kernel on the same workload at 128 frames
+# (315 606 784 / 208 174 588): its traffic grows with the symbols it encodes
+# and the bytes it emits, so it scales to a full launch by the launch's
+# algorithmic bytes.  The capture and its command are summarised in
+# profiles/k_rans_mixed128.md.
+RANS_TRAFFIC_PER_ALG_BYTE: float | None = 1.5161
 
 
 def gpu_local_cpus(dev: int) -> dict:
@@ -909,8 +911,8 @@ def main() -> None:
         "assemble": stats["frame_bytes"] + stats["rans_emitted_bytes"] + stats["input_bytes"] // 64,
     }.get(dom, stats["input_bytes"] + stats["frame_bytes"])
     achieved = alg / (stages[dom] / 1e3) / 1e9
-    traffic = (RANS_TRAFFIC_PER_SYMBOL * stats["rans_symbols"]
-               if RANS_TRAFFIC_PER_SYMBOL is not None and dom == "rans" else None)
+    traffic = (int(RANS_TRAFFIC_PER_ALG_BYTE * alg)
+               if RANS_TRAFFIC_PER_ALG_BYTE is not None and dom == "rans" else None)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 5), "peak_source": peak_kind,
                 "traffic": traffic, "algorithmic_bytes_per_launch": int(alg),
