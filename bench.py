@@ -470,23 +470,29 @@ def coded_measure(comp, hin, frames, steps: int, inflight: int) -> dict:
     return out
 
 
-def decode_measure(comp, batch, reps: int = 3) -> dict:
+def decode_measure(comp, batch, copies: int = 10, reps: int = 3) -> dict:
     """The batch's frames decoded on the device (przmg_decompress_batch_device),
-    device-resident: GB/s of decoded bytes (median of reps, CUDA events on
-    the call's stream), every frame compared with its input on the device
-    (przmg_batch_verify, untimed)."""
+    device-resident, `copies` times over in one call (each copy a full decode
+    into its own output), as the compression leg keeps ten batches in flight:
+    a frame decodes as one serial chain per coded stream, so one batch alone
+    leaves most of the GPU idle.  GB/s of decoded bytes (median of reps,
+    CUDA events on the call's stream); every frame is also compared with its
+    input on the device (przmg_batch_verify, untimed)."""
     import numpy as np
     import torch
     from przm_b200 import devmem
     sizes = [int(x) for x in batch.sizes]
     batch.enqueue(graph=True)  # the frames again: the link measurement used d_out as scratch
     fs = batch.frame_sizes()
-    dcap = [max(n, 1) for n in sizes]
-    doffs = np.zeros(len(sizes), np.uint64)
+    nf = len(sizes) * copies
+    soffs = np.tile(np.asarray(batch.out_offs[: len(sizes)], np.uint64), copies)
+    slens = np.tile(np.asarray(fs, np.uint32), copies)
+    dcap = np.tile(np.asarray([max(n, 1) for n in sizes], np.uint32), copies)
+    doffs = np.zeros(nf, np.uint64)
     o = 0
-    for i, n in enumerate(dcap):
+    for i in range(nf):
         doffs[i] = o
-        o += (n + 64 + 15) // 16 * 16
+        o += (int(dcap[i]) + 64 + 15) // 16 * 16
     out = devmem.alloc(o + 64)
     st = torch.cuda.Stream()
     try:
@@ -495,18 +501,19 @@ def decode_measure(comp, batch, reps: int = 3) -> dict:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(st)
-            status, lens = comp.DecompressBatchDevice(batch.d_out, batch.out_offs, fs, out.ptr, doffs, dcap,
-                                                      st.cuda_stream)
+            status, lens = comp.DecompressBatchDevice(batch.d_out, soffs, slens, out.ptr, doffs, dcap, st.cuda_stream)
             e1.record(st)
             e1.synchronize()
             runs.append(e0.elapsed_time(e1))
         ms = sorted(runs[1:])[len(runs[1:]) // 2]
         ok = int((status == 0).sum())
+        same = all(lens[i] == lens[i % len(sizes)] for i in range(nf))
     finally:
         out.free()
     bad = batch.verify()
-    return {"gbps": round(sum(sizes) / (ms / 1e3) / 1e9, 3), "ms": round(ms, 3), "frames": len(sizes),
-            "frames_decoded": ok, "frames_verified_on_device": len(sizes) - bad,
+    return {"gbps": round(copies * sum(sizes) / (ms / 1e3) / 1e9, 3), "ms": round(ms, 3), "frames": nf,
+            "copies_of_the_batch": copies, "frames_decoded": ok, "same_sizes_every_copy": bool(same),
+            "frames_verified_on_device": len(sizes) - bad,
             "note": "decoded bytes per second; frames of the entropy-coded profile, device-resident"}
 
 

@@ -240,6 +240,8 @@ struct Ctx {
     // the GPU decoder: static tables, per-frame scratch, jobs, results,
     // entropy tasks; przmg_batch_verify's decoded bytes and comparisons
     DevBuf d_dstatic, d_dscr, d_djobs, d_dinfo, d_dtasks, d_dout, d_ddiff;
+    cudaStream_t dec_aux = nullptr;  // the decoder's static-model chains
+    cudaEvent_t dec_fork = nullptr, dec_join = nullptr;
     cudaEvent_t ev[8] = {};
 };
 
@@ -838,6 +840,9 @@ extern "C" int32_t przmg_close(przmg_ctx* h) {
         c->h_out.release();
         c->h_aux.release();
         for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+        if (c->dec_fork) cudaEventDestroy(c->dec_fork);
+        if (c->dec_join) cudaEventDestroy(c->dec_join);
+        if (c->dec_aux) cudaStreamDestroy(c->dec_aux);
         cudaStreamDestroy(c->stream);
     }
     {

@@ -449,10 +449,13 @@ struct ByteWin {
     __device__ __forceinline__ uint32_t pos() const { return q - nn - av; }  // bytes consumed
 };
 
-// the larger of an adaptive body's decode table + frequencies and the Meta8
-// models
-constexpr uint32_t kDecEntropySmem = 8 * 4096 + 8 * 256 * 4;
-static_assert(kDecEntropySmem >= 4096 * 4 + 256 * 2, "adaptive decode table");
+// Shared memory of an adaptive body's task (decode table + frequencies) and
+// of a static-model task (the Meta8 models, the larger of the two).  The two
+// kinds run as separate launches so the long adaptive chains are not held
+// to the occupancy of the larger allotment.
+constexpr uint32_t kDecAdaptiveSmem = 4096 * 4 + 256 * 2;
+constexpr uint32_t kDecStaticSmem = 8 * 4096 + 8 * 256 * 4;
+static_assert(kDecStaticSmem >= 4 * 4096 + 4 * 64 * 4, "Mode 12 models");
 
 // Bytes [p, p + 8) of s as a little-endian word (two aligned loads; the
 // caller keeps p + 16 <= the stream's length, and s is never within 8 bytes
@@ -476,15 +479,16 @@ __device__ __forceinline__ uint32_t renorm_apply(uint32_t x, uint32_t k, uint32_
 
 
 // One warp per task (tasks[blockIdx.x]): blocks of one warp, so the serial
-// chains spread over the SMs.
+// chains spread over the SMs.  statics: run the Meta8 and Mode 12 tasks
+// (else the adaptive ones).
 __global__ void __launch_bounds__(32) k_dec_entropy(const DecTask* __restrict__ tasks, const DecStatic* __restrict__ st,
-                                                    DecInfo* __restrict__ infos) {
+                                                    DecInfo* __restrict__ infos, uint32_t statics) {
     extern __shared__ __align__(16) uint8_t smem_d[];
     uint32_t* tab = reinterpret_cast<uint32_t*>(smem_d);
     uint16_t* freq = reinterpret_cast<uint16_t*>(smem_d + 4096 * 4);
     const DecTask t = tasks[blockIdx.x];
     const uint32_t lane = threadIdx.x;
-    if (t.kind == DT_NONE || t.n == 0) return;
+    if (t.kind == DT_NONE || t.n == 0 || (t.kind == DT_ADAPTIVE) == (statics != 0)) return;
     const uint8_t* s = reinterpret_cast<const uint8_t*>(t.src);
     uint8_t* dst = reinterpret_cast<uint8_t*>(t.dst);
     const uint32_t n = t.n, slen = t.slen;
