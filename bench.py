@@ -259,9 +259,10 @@ def link_gbs(hin, nbytes: int, dev_buf: int, stream) -> dict:
 def section3_measure(comp, sections: int, per: int = 20_000, calls: int = 5) -> dict:
     """Section 3 distance coding on the device (przmg_package_offsets_batch,
     PackageOffsetsSection) of `sections` arrays of `per` distances each,
-    log-uniform in [2, 2^20 + 1] (the match window), seeded.  A call
-    synchronises (the host picks each section's form from the sizes), so the
-    figure is wall time per call, best of `calls` after one warm-up."""
+    log-uniform in [2, 2^20 + 1] (the match window), seeded.  Each section's
+    form is chosen on the device; a call returns the section lengths, so it
+    synchronises once and the figure is wall time per call, best of `calls`
+    after one warm-up."""
     import numpy as np
     from przm_b200 import devmem
     rng = np.random.default_rng(0x50525A4D + 5)
@@ -296,8 +297,9 @@ def section4_measure(comp, streams: int, size: int = 256 << 10, calls: int = 5) 
     """Section 4 selection on the device (przmg_package_literals_batch,
     PackageLiteralsSection: adaptive V-ANS or one of four sheaf foliations)
     of `streams` literal-like streams of `size` bytes (seeded order-1 Markov
-    text).  A call synchronises (the host compares the candidates), so the
-    figure is wall time per call, best of `calls` after one warm-up."""
+    text).  The candidates are compared on the device; a call returns the
+    section lengths, so it synchronises once and the figure is wall time per
+    call, best of `calls` after one warm-up."""
     import numpy as np
     from przm_b200 import devmem
     from przm_b200 import workloads as W

@@ -347,8 +347,9 @@ int32_t przmg_vans_encode_batch(przmg_ctx* ctx, uint64_t d_in, const uint64_t* i
  * holds counts[i] <= 2^21 uint32 distances; section i goes to
  * d_out + out_offs[i], whose out_caps[i] bytes must hold 1 + 5 * counts[i]
  * in the worst case; out_lens[i] receives its size.  Synchronises the stream.
- * PRZMG_ERR_EXCEEDS_MAX_BLOCK for an array above 2^21 distances,
- * PRZMG_ERR_BUFFER_TOO_SMALL when a section does not fit its capacity. */
+ * PRZMG_ERR_EXCEEDS_MAX_BLOCK for an array above 2^21 distances (nothing
+ * runs), PRZMG_ERR_BUFFER_TOO_SMALL when a section does not fit its capacity
+ * (that section is left empty with out_lens[i] = 0; the others are written). */
 int32_t przmg_package_offsets_batch(przmg_ctx* ctx, uint64_t d_dist, const uint64_t* dist_offs, const uint32_t* counts,
                                     uint64_t count, uint64_t d_out, const uint64_t* out_offs, const uint64_t* out_caps,
                                     uint64_t* out_lens, uint64_t stream);
@@ -360,7 +361,10 @@ int32_t przmg_package_offsets_batch(przmg_ctx* ctx, uint64_t d_dist, const uint6
  * flag nibble (nibbles[i] = 0x80 for a container, 0 for raw).  Stream i is
  * lens[i] <= 4 MiB bytes at d_in + in_offs[i]; its section goes to
  * d_out + out_offs[i] (out_caps[i] >= lens[i] always suffices).  At most
- * 65535 streams per call.  Synchronises the stream. */
+ * 65535 streams per call.  Synchronises the stream.
+ * PRZMG_ERR_EXCEEDS_MAX_BLOCK for a stream above 4 MiB (nothing runs),
+ * PRZMG_ERR_BUFFER_TOO_SMALL when a section does not fit its capacity (that
+ * section is left empty with out_lens[i] = 0; the others are written). */
 int32_t przmg_package_literals_batch(przmg_ctx* ctx, uint64_t d_in, const uint64_t* in_offs, const uint32_t* lens,
                                      uint64_t count, uint64_t d_out, const uint64_t* out_offs, const uint64_t* out_caps,
                                      uint64_t* out_lens, uint8_t* nibbles, uint64_t stream);

@@ -103,6 +103,7 @@ struct HostBuf {
 };
 
 static inline uint64_t align16(uint64_t v) { return (v + 15) & ~15ull; }
+static inline uint64_t align64(uint64_t v) { return (v + 63) & ~63ull; }
 
 extern "C" uint64_t przmg_frame_bound(uint64_t n) { return 2 * n + (n >> 13) + 4096; }
 

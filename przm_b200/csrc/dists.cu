@@ -147,26 +147,17 @@ __device__ __forceinline__ bool m12_step(uint32_t& x, uint32_t& e, const EncSym&
     return true;
 }
 
-// The Mode 12 chains of frames [j0, j0 + njobs), one thread each.  tab12:
-// the 4 x 64 static weights in EncSym form.  Codes are taken eight at a
-// time from aligned words, so the table entries of a group load before its
-// dependent steps run.
-__global__ void __launch_bounds__(32) k_s3_chain(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs,
-                                                 uint8_t* __restrict__ s3base, S3Frame* __restrict__ s3f,
-                                                 const EncSym* __restrict__ tab12) {
-    __shared__ EncSym s_tab[4 * 64];
-    for (uint32_t i = threadIdx.x; i < 4 * 64; i += 32) s_tab[i] = tab12[i];
-    __syncwarp();
-    const uint32_t jl = blockIdx.x * 32 + threadIdx.x;
-    if (jl >= njobs) return;
-    const uint32_t j = j0 + jl;
-    const Job job = jobs[j];
-    if (job.profile < 2) return;
-    const uint32_t nd = s3f[j].nd;
-    if (nd == 0 || s3f[j].bad || nd > job.dist_cap) return;
-    const uint8_t* codes = s3base + job.s3_off;
-    uint8_t* em = s3base + job.s3_off + s3_em_off(job);
-    uint32_t x = 65536, e = 0;
+// The Mode 12 chain over codes[0, nd) (one thread): codes from the last to
+// the first, each with the model of its predecessor's class (s_tab: the
+// 4 x 64 static weights in EncSym form); the emitted bytes go to em in
+// emission order.  Codes are taken eight at a time from aligned words (codes
+// 16-byte aligned), so the table entries of a group load before its
+// dependent steps run.  False where the reference's 2 MiB emission scratch
+// would overflow.
+__device__ bool m12_chain(const uint8_t* __restrict__ codes, uint32_t nd, uint8_t* __restrict__ em,
+                          const EncSym* s_tab, uint32_t& x, uint32_t& e) {
+    x = 65536;
+    e = 0;
     bool ok = true;
     const uint32_t full = nd & ~7u;  // codes [0, full) in aligned groups of eight
     for (uint32_t i = nd; i > full && ok;) {
@@ -190,6 +181,26 @@ __global__ void __launch_bounds__(32) k_s3_chain(const Job* __restrict__ jobs, u
         for (int r = 7; r >= 0; r--)
             if (ok) ok = m12_step(x, e, es[r], em);
     }
+    return ok;
+}
+
+// The Mode 12 chains of frames [j0, j0 + njobs), one thread each.  tab12:
+// the 4 x 64 static weights in EncSym form.
+__global__ void __launch_bounds__(32) k_s3_chain(const Job* __restrict__ jobs, uint32_t j0, uint32_t njobs,
+                                                 uint8_t* __restrict__ s3base, S3Frame* __restrict__ s3f,
+                                                 const EncSym* __restrict__ tab12) {
+    __shared__ EncSym s_tab[4 * 64];
+    for (uint32_t i = threadIdx.x; i < 4 * 64; i += 32) s_tab[i] = tab12[i];
+    __syncwarp();
+    const uint32_t jl = blockIdx.x * 32 + threadIdx.x;
+    if (jl >= njobs) return;
+    const uint32_t j = j0 + jl;
+    const Job job = jobs[j];
+    if (job.profile < 2) return;
+    const uint32_t nd = s3f[j].nd;
+    if (nd == 0 || s3f[j].bad || nd > job.dist_cap) return;
+    uint32_t x, e;
+    const bool ok = m12_chain(s3base + job.s3_off, nd, s3base + job.s3_off + s3_em_off(job), s_tab, x, e);
     s3f[j].m12e = ok ? e : 0xFFFFFFFFu;
     s3f[j].m12x = x;
 }

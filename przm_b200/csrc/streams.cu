@@ -15,15 +15,14 @@ struct STask {
     uint32_t flags;  // container flag byte
 };
 
-// Byte histogram of task blockIdx.y, 64 KiB per block, privatised per warp
+// Byte histogram of a task, 64 KiB per block (blockIdx.x: the chunk), privatised per warp
 // and merged with one global atomic per (block, symbol) -- the reference's
 // przm_byte_histogram_kernel (przm_ans.cu:73-192) with warp-aggregated
 // shared-memory increments (__match_any_sync groups equal bytes of a warp).
 constexpr uint32_t kHistChunk = 65536;
 
-__global__ void __launch_bounds__(256) k_stream_hist(const STask* __restrict__ tasks, uint32_t* __restrict__ counts) {
-    __shared__ uint32_t s_h[8][256];
-    const STask t = tasks[blockIdx.y];
+__device__ __forceinline__ void stream_hist_task(const STask t, uint32_t ti, uint32_t (&s_h)[8][256],
+                                                 uint32_t* __restrict__ counts) {
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for (uint32_t i = tid; i < 8 * 256; i += 256) (&s_h[0][0])[i] = 0;
     __syncthreads();
@@ -52,7 +51,15 @@ __global__ void __launch_bounds__(256) k_stream_hist(const STask* __restrict__ t
     uint32_t sum = 0;
 #pragma unroll
     for (int w = 0; w < 8; w++) sum += s_h[w][tid];
-    if (sum) atomicAdd(&counts[(uint64_t)blockIdx.y * 256 + tid], sum);
+    if (sum) atomicAdd(&counts[(uint64_t)ti * 256 + tid], sum);
+    __syncthreads();  // s_h is cleared for the next task
+}
+
+// Tasks blockIdx.y, blockIdx.y + gridDim.y, ... (grid y is at most 65535).
+__global__ void __launch_bounds__(256) k_stream_hist(const STask* __restrict__ tasks, uint32_t ntasks,
+                                                     uint32_t* __restrict__ counts) {
+    __shared__ uint32_t s_h[8][256];
+    for (uint32_t ti = blockIdx.y; ti < ntasks; ti += gridDim.y) stream_hist_task(tasks[ti], ti, s_h, counts);
 }
 
 // One warp per task: normalise and build the encoding table + matrix.

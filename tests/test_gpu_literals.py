@@ -62,3 +62,31 @@ def test_sections_match_oracle_twice(comp, oracle):
 def test_stream_limit(comp):
     with pytest.raises(gpu.GPUError):
         comp.PackageLiteralsBatch(0, [0], [(4 << 20) + 1], 0, [0], [8 << 20])
+
+
+def test_many_small_streams(comp, oracle):
+    """4000 streams in one call (68 000 V-ANS tasks, more than one grid row
+    of tasks), at every byte offset: JSON-like text, Markov text, empty and
+    one-byte streams."""
+    ss = []
+    for i in range(4000):
+        n = (i * 37) % 1500
+        ss.append(json_lines(i, n) if i % 3 == 0 else b"" if i % 97 == 0 else W.gen("markov", 50 + i, max(n, 1)).tobytes())
+    want = [oracle.package_literals(x) for x in ss]
+    assert any(w[1] and w[0][3] & 0x04 for w in want)
+    got = run(comp, ss)
+    bad = [i for i, (g, w) in enumerate(zip(got, want)) if g != w]
+    assert not bad, f"{len(bad)} streams differ, first {bad[0]}"
+
+
+def test_capacity_too_small(comp, oracle):
+    """A section above its capacity fails the call (BUFFER_TOO_SMALL); the
+    context stays usable."""
+    from przm_b200 import devmem
+    x = W.gen("uniform", 7, 10_000)
+    d_in = devmem.upload(np.concatenate([x, np.zeros(64, np.uint8)]))
+    d_out = devmem.alloc(20_000)
+    with pytest.raises(gpu.GPUError):
+        comp.PackageLiteralsBatch(d_in.ptr, [0], [len(x)], d_out.ptr, [0], [len(x) - 1])
+    ss = [json_lines(3, 50_000)]
+    assert run(comp, ss) == [oracle.package_literals(ss[0])]
