@@ -150,7 +150,7 @@ struct przmg_batch {
     // radix-strike tables (one per finder CTA) and the packed upload/download
     // staging belong to the batch, so batches on different streams never
     // share scratch
-    DevBuf d_rtiles, d_rx_cnt, d_rx_parts, d_rx_ent, d_rx_key, d_rx_pred, d_stage_in, d_stage_out, d_stage_offs, d_up_offs;
+    DevBuf d_rtiles, d_rx_toff, d_rx_list, d_rx_pred, d_stage_in, d_stage_out, d_stage_offs, d_up_offs;
     DevBuf d_tile_sched;  // tokenizer tile weights [0, ntiles) and walk order [ntiles, 2 ntiles)
     DevBuf d_asm;         // assembly work items (frame, part)
     DevBuf d_asm_job;     // the same items grouped by input (plain per-input launches)
@@ -195,7 +195,7 @@ struct przmg_batch {
     void release() {
         DevBuf* all[] = {&d_in, &d_jobs, &d_small, &d_big, &d_tiles, &d_desc, &d_slots, &d_tile_lens, &d_streams,
                          &d_job_lens, &d_hist, &d_tabs, &d_infos, &d_ans, &d_outs, &d_plans, &d_sizes, &d_out, &d_misc,
-                         &d_lists, &d_rtiles, &d_rx_cnt, &d_rx_parts, &d_rx_ent, &d_rx_key, &d_rx_pred, &d_stage_in,
+                         &d_lists, &d_rtiles, &d_rx_toff, &d_rx_list, &d_rx_pred, &d_stage_in,
                          &d_stage_out, &d_stage_offs, &d_up_offs, &d_tile_sched, &d_asm, &d_asm_job,
                          &d_fitems, &d_ftiles, &d_ftarget, &d_fctl, &d_s3, &d_s3f, &d_fib};
         for (DevBuf* b : all) b->release();
@@ -266,25 +266,20 @@ static void front_build(const przmg_batch* b, uint32_t chunk, bool unreachable, 
     auto nv = [&](uint32_t j) { return (rx_ncand(b->jobs[j].n) + chunk - 1) / chunk; };
     auto big = [&](uint32_t j) { return b->job_big0[j + 1] > b->job_big0[j]; };
     for (uint32_t j : ord)
-        for (uint32_t t = b->job_rt0[j]; t < b->job_rt0[j + 1]; t++) items.push_back({FS_RX_COUNT, j, t, 0});
+        for (uint32_t t = b->job_rt0[j]; t < b->job_rt0[j + 1]; t++) items.push_back({FS_RX_SORT, j, t, 0});
     for (uint32_t j : ord)
         for (uint32_t t = b->job_small0[j]; t < b->job_small0[j + 1]; t++) items.push_back({FS_TILE_FIND, j, t, 0});
     for (uint32_t j : ord)
-        if (big(j)) items.push_back({FS_RX_SCAN, j, j, nrt(j)});
-    for (uint32_t j : ord)
-        if (big(j))
-            for (uint32_t t = b->job_rt0[j]; t < b->job_rt0[j + 1]; t++) items.push_back({FS_RX_SCATTER, j, t, nrt(j) + 1});
-    for (uint32_t j : ord)
         if (big(j))
             for (uint32_t g = 0; g < kFrontResolveItems; g++)
-                items.push_back({FS_RX_RESOLVE, j, g * kFrontWarps, 2 * nrt(j) + 1});
+                items.push_back({FS_RX_RESOLVE, j, g * kFrontWarps, nrt(j)});
     for (uint32_t j : ord)
         if (big(j))
             for (uint32_t c = 0; c < nv(j); c++)
-                items.push_back({FS_RX_VERIFY, j, c * chunk, 2 * nrt(j) + 1 + kFrontResolveItems});
+                items.push_back({FS_RX_VERIFY, j, c * chunk, nrt(j) + kFrontResolveItems});
     for (uint32_t j : ord) {
         const uint32_t nt = b->job_tile0[j + 1] - b->job_tile0[j];
-        tok_target[j] = big(j) ? 2 * nrt(j) + 1 + kFrontResolveItems + nv(j) : nt;
+        tok_target[j] = big(j) ? nrt(j) + kFrontResolveItems + nv(j) : nt;
         for (uint32_t t = b->job_tile0[j]; t < b->job_tile0[j + 1]; t++) ftiles.push_back(b->tiles[t]);
     }
     for (uint32_t t = 0; t < ftiles.size(); t += kFrontWarps)
@@ -445,10 +440,8 @@ static int32_t batch_prepare(przmg_batch* b, const uint64_t* sizes, uint32_t njo
     CK(b->d_up_offs.ensure(8ull * std::max<uint32_t>(njobs, 1) + 64));
     if (b->nbig) {
         CK(b->d_rtiles.ensure(sizeof(RxTile) * std::max<size_t>(b->rtiles.size(), 1)));
-        CK(b->d_rx_cnt.ensure((size_t)b->ntiles * kRxParts * 4 + 64));
-        CK(b->d_rx_parts.ensure((size_t)njobs * kRxParts * sizeof(uint2) + 64));
-        CK(b->d_rx_ent.ensure(b->desc_words * 4));
-        CK(b->d_rx_key.ensure(b->desc_words * 2));
+        CK(b->d_rx_toff.ensure((size_t)b->ntiles * kRxParts * 4 + 64));
+        CK(b->d_rx_list.ensure(b->desc_words * 4));
         CK(b->d_rx_pred.ensure(b->desc_words * 4));
     }
     b->up_offs.assign(njobs, 0);
@@ -565,10 +558,8 @@ static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, cons
         a.ntiles = (uint32_t)b->tiles.size();
         a.verify_chunk = std::max<uint32_t>(256, b->tune.verify_chunk);
         a.desc = b->d_desc.as<uint32_t>();
-        a.rx_cnt = b->d_rx_cnt.as<uint32_t>();
-        a.rx_parts = b->d_rx_parts.as<uint2>();
-        a.rx_ent = b->d_rx_ent.as<uint32_t>();
-        a.rx_key = b->d_rx_key.as<uint16_t>();
+        a.rx_toff = b->d_rx_toff.as<uint32_t>();
+        a.rx_list = b->d_rx_list.as<uint32_t>();
         a.rx_pred = b->d_rx_pred.as<uint32_t>();
         a.slots = b->d_slots.as<uint8_t>();
         a.tile_lens = b->d_tile_lens.as<uint32_t>();
@@ -594,26 +585,21 @@ static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, cons
         const uint32_t gt = std::min<uint32_t>(R.nrt, 16u * c->sms);
         const RxTile* rt = b->d_rtiles.as<RxTile>() + R.rt0;
         const uint32_t* big = b->d_big.as<uint32_t>() + R.big0;
-        k_rx_count<<<gt, 256, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), rt, R.nrt, b->d_rx_cnt.as<uint32_t>());
-        CK(cudaGetLastError());
-        k_rx_scan<<<std::min<uint32_t>(R.nbig, 16u * c->sms), kRxParts, 0, s>>>(
-            b->d_jobs.as<Job>(), big, R.nbig, b->d_rx_cnt.as<uint32_t>(), b->d_rx_parts.as<uint2>());
-        CK(cudaGetLastError());
-        k_rx_scatter<<<gt, 256, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), rt, R.nrt, b->d_rx_cnt.as<uint32_t>(),
-                                        b->d_rx_ent.as<uint32_t>(), b->d_rx_key.as<uint16_t>());
+        k_rx_sort<<<gt, 256, 0, s>>>(b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), rt, R.nrt, b->d_rx_toff.as<uint32_t>(),
+                                     b->d_rx_list.as<uint32_t>());
         CK(cudaGetLastError());
         const uint32_t nwarps = R.nbig * kRxParts;
         const uint32_t gr = std::min<uint32_t>((nwarps + kRxResolveWarps - 1) / kRxResolveWarps, 4u * c->sms);
         k_rx_resolve<<<gr, kRxResolveWarps * 32, kRxResolveSmem, s>>>(
-            b->d_jobs.as<Job>(), big, R.nbig, b->d_rx_parts.as<uint2>(), b->d_rx_ent.as<uint32_t>(),
-            b->d_rx_key.as<uint16_t>(), b->d_rx_pred.as<uint32_t>());
+            b->d_jobs.as<Job>(), big, R.nbig, b->d_rx_toff.as<uint32_t>(), b->d_rx_list.as<uint32_t>(),
+            b->d_rx_pred.as<uint32_t>());
         CK(cudaGetLastError());
         const uint32_t vx = std::max<uint32_t>(1, std::min<uint32_t>(64u, (uint32_t)((R.max_big_cand + 255) / 256)));
         k_rx_verify<<<dim3(vx, std::min<uint32_t>(R.nbig, 65535u)), 256, 0, s>>>(
-            b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), big, b->d_rx_ent.as<uint32_t>(), b->d_rx_pred.as<uint32_t>(),
+            b->d_in.as<uint8_t>(), b->d_jobs.as<Job>(), big, b->d_rx_list.as<uint32_t>(), b->d_rx_pred.as<uint32_t>(),
             R.nbig, b->d_desc.as<uint32_t>());
         CK(cudaGetLastError());
-        launches += 5;
+        launches += 3;
     }
     CK(mark(2));
     if (stop_after >= 1 && R.nt) {

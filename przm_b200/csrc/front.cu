@@ -1,9 +1,9 @@
 // front.cu -- the persistent front end: one launch that runs the match
 // finders, the tokenizer and the gather for every input of a batch.
 //
-// The work of a batch is a list of items in stage order (radix counts and
-// tile-finder tiles, radix scans, scatters, partition resolves, verify
-// chunks, tokenizer tiles, gathers), built on the host when the batch is laid
+// The work of a batch is a list of items in stage order (radix tile sorts
+// and tile-finder tiles, partition resolves, verify chunks, tokenizer tiles,
+// gathers), built on the host when the batch is laid
 // out.  Blocks stay resident and take the next item from a device counter
 // (atomicAdd), so a block that finishes a short item -- a 1 KiB input's
 // tile, a 2048-candidate verify chunk -- takes another at once, and inputs of
@@ -23,8 +23,8 @@
 // An item's progress is published with a fence and an atomic add after the
 // block's barrier, and a waiting item reads it with ld.acquire.gpu before its
 // block's barrier.  Data that other blocks of the same launch wrote
-// (descriptors, radix lists and counts, tokenizer slots and tile lengths) is
-// read with ld.global.cg, which goes to L2, never through the non-coherent
+// (descriptors, radix lists, run starts and predecessors, tokenizer slots
+// and tile lengths) is read with ld.global.cg, which goes to L2, never through the non-coherent
 // read-only path, whose contents are only valid for data that no block of
 // the running kernel writes.
 #include "common.cuh"
@@ -33,9 +33,7 @@ namespace pz {
 
 enum FrontStage : uint32_t {
     FS_TILE_FIND = 0,  // idx = small tile (TileRef list)
-    FS_RX_COUNT,       // idx = radix tile (RxTile list)
-    FS_RX_SCAN,        // idx = large frame's input index
-    FS_RX_SCATTER,     // idx = radix tile
+    FS_RX_SORT,        // idx = radix tile (RxTile list)
     FS_RX_RESOLVE,     // idx = first partition (8 per item, one per warp)
     FS_RX_VERIFY,      // idx = first candidate of the chunk
     FS_TOKENIZE,       // idx = first tile (tile list), up to 8 tiles (one per warp)
@@ -56,7 +54,7 @@ constexpr uint32_t kFrontSmem = (kTileFindSmem > kRxResolveSmem ? kTileFindSmem 
                                         kFrontWarps * sizeof(TokSmem)
                                     ? (kTileFindSmem > kRxResolveSmem ? kTileFindSmem : kRxResolveSmem)
                                     : (uint32_t)(kFrontWarps * sizeof(TokSmem));
-static_assert(kFrontSmem >= kFrontGatherSmem && kFrontSmem >= 8 * kRxParts * 4, "front shared memory");
+static_assert(kFrontSmem >= kFrontGatherSmem && kFrontSmem >= sizeof(RxSortSmem), "front shared memory");
 static_assert(kRxResolveWarps == kFrontWarps, "a resolve item is one partition per warp");
 
 constexpr uint32_t E_SCHED_TIMEOUT = 16;  // a front-end wait ran out (error word bit)
@@ -77,10 +75,8 @@ struct FrontArgs {
     uint32_t ntiles;
     uint32_t verify_chunk;
     uint32_t* desc;
-    uint32_t* rx_cnt;
-    uint2* rx_parts;
-    uint32_t* rx_ent;
-    uint16_t* rx_key;
+    uint32_t* rx_toff;
+    uint32_t* rx_list;
     uint32_t* rx_pred;
     uint8_t* slots;
     uint32_t* tile_lens;
@@ -152,24 +148,17 @@ __global__ void __launch_bounds__(kFrontThreads, 3) k_front(const FrontArgs a) {
             case FS_TILE_FIND:
                 tile_find_item(a.in, a.jobs, a.small[fi.idx], a.desc, smem_f, a.err);
                 break;
-            case FS_RX_COUNT:
-                rx_count_item(a.in, a.jobs, a.rtiles[fi.idx], a.rx_cnt, reinterpret_cast<uint32_t*>(smem_f));
-                break;
-            case FS_RX_SCAN:
-                rx_scan_item<true>(a.jobs, fi.idx, a.rx_cnt, a.rx_parts, reinterpret_cast<uint32_t*>(smem_f));
-                break;
-            case FS_RX_SCATTER:
-                rx_scatter_item<true>(a.in, a.jobs, a.rtiles[fi.idx], a.rx_cnt, a.rx_ent, a.rx_key,
-                                reinterpret_cast<uint32_t(*)[kRxParts]>(smem_f));
+            case FS_RX_SORT:
+                rx_sort_item(a.in, a.jobs, a.rtiles[fi.idx], a.rx_toff, a.rx_list, *reinterpret_cast<RxSortSmem*>(smem_f));
                 break;
             case FS_RX_RESOLVE:
-                rx_resolve_warp<true>(a.jobs, fi.job, fi.idx + warp, a.rx_parts, a.rx_ent, a.rx_key, a.rx_pred,
+                rx_resolve_warp<true>(a.jobs, fi.job, fi.idx + warp, a.rx_toff, a.rx_list, a.rx_pred,
                                 reinterpret_cast<uint32_t*>(smem_f) + warp * kRxKeys);
                 break;
             case FS_RX_VERIFY: {
                 const Job job = a.jobs[fi.job];
                 const uint32_t hi = min(rx_ncand(job.n), fi.idx + a.verify_chunk);
-                rx_verify_range<true>(a.in, job, a.rx_ent, a.rx_pred, a.desc, fi.idx, hi, tid, kFrontThreads);
+                rx_verify_range<true>(a.in, job, a.rx_list, a.rx_pred, a.desc, fi.idx, hi, tid, kFrontThreads);
                 break;
             }
             case FS_GATHER:

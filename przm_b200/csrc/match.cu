@@ -148,18 +148,19 @@ __global__ void __launch_bounds__(256) k_tile_find(const uint8_t* __restrict__ i
 //
 // Candidates with equal hashes share the hash's top 8 bits, so each frame is
 // split into 256 partitions that never interact:
-//   k_rx_count   per 32 KiB tile (4096 candidates): candidates per partition;
-//   k_rx_scan    per frame: where each (tile, partition) run starts in the
-//                frame's partition-ordered candidate list;
-//   k_rx_scatter per tile: writes each candidate index (and its low 11 hash
-//                bits) to its slot, keeping position order inside a partition;
-//   k_rx_resolve one warp per (frame, partition): walks the partition's
-//                candidates in position order 32 at a time with a 2048-entry
-//                shared table of the latest candidate per low-11-bit key
-//                (ties inside the 32 resolved with warp_match) and
-//                stores each candidate's predecessor next to it;
-//   k_rx_verify  one thread per candidate: verifies and extends the match
-//                against the predecessor and writes the descriptor.
+//   k_rx_sort    per 32 KiB tile (4096 candidates): hashes, then a stable
+//                sort of the tile's candidates by partition in shared memory,
+//                written out as the tile's slice of the candidate list (one
+//                word per candidate: its low 11 hash bits and its index in
+//                the tile) with the start of every partition's run;
+//   k_rx_resolve one warp per (frame, partition): walks the partition's runs
+//                tile by tile (so in position order) 32 candidates at a time
+//                with a 2048-entry shared table of the latest candidate per
+//                low-11-bit key (ties inside the 32 resolved with
+//                warp_match) and stores each candidate's predecessor in its
+//                slot of the list;
+//   k_rx_verify  one thread per slot: verifies and extends the match against
+//                the predecessor and writes the descriptor.
 // Output: one descriptor per 8-aligned position (d8[c]), every candidate
 // written exactly once.
 // ---------------------------------------------------------------------------
@@ -168,6 +169,7 @@ constexpr uint32_t kRxParts = 256;       // partitions: hash >> 11
 constexpr uint32_t kRxKeys = 2048;       // keys inside a partition: hash & 2047
 constexpr uint32_t kRxResolveWarps = 8;  // warps per k_rx_resolve block
 constexpr uint32_t kRxResolveSmem = kRxResolveWarps * kRxKeys * 4;
+static_assert(kCandPerTile == 4096, "a list word holds a 12-bit index in the tile");
 
 struct RxTile { uint32_t job; uint32_t tile; };
 
@@ -176,132 +178,84 @@ __device__ __forceinline__ uint32_t kmer_hash(uint64_t k) {
 }
 __host__ __device__ inline uint32_t rx_ncand(uint32_t n) { return n >= 8 ? (n - 8) / 8 + 1 : 0; }
 
-// One radix tile, block of 256; s_cnt = kRxParts words of shared memory.
-__device__ void rx_count_item(const uint8_t* __restrict__ in, const Job* __restrict__ jobs, const RxTile tt,
-                              uint32_t* __restrict__ cnt, uint32_t* s_cnt) {
+struct RxSortSmem {
+    uint32_t w[8][kRxParts];         // per warp and partition: count, then next slot
+    uint32_t list[kCandPerTile];     // the tile's list, partition-sorted
+    uint32_t warp[32];
+};
+
+// One radix tile by a block of 256 threads: warp w takes candidates
+// [c0 + 512 w, c0 + 512 w + 512) in 16 rounds of 32.  Slots follow
+// (partition, warp, round, lane), i.e. position order inside a partition.
+// toff[(tile0 + t) * 256 + b]: where partition b's run starts in the tile's
+// slice; the slice of tile t is list[c0, c1) of the frame.
+__device__ void rx_sort_item(const uint8_t* __restrict__ in, const Job* __restrict__ jobs, const RxTile tt,
+                             uint32_t* __restrict__ toff, uint32_t* __restrict__ list, RxSortSmem& sm) {
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
     const Job job = jobs[tt.job];
     const uint64_t* src = reinterpret_cast<const uint64_t*>(in + job.in_off);
     const uint32_t C = rx_ncand(job.n), c0 = tt.tile * kCandPerTile, c1 = min(C, c0 + kCandPerTile);
+    __syncthreads();  // the previous item no longer reads sm
+    for (uint32_t i = tid; i < 8 * kRxParts; i += 256) (&sm.w[0][0])[i] = 0;
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < kRxParts; i += 256) s_cnt[i] = 0;
-    __syncthreads();
-    for (uint32_t c = c0 + threadIdx.x; c < c1; c += 256) atomicAdd(&s_cnt[kmer_hash(__ldg(src + c)) >> kRxKeyBits], 1u);
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < kRxParts; i += 256) cnt[(uint64_t)(job.tile0 + tt.tile) * kRxParts + i] = s_cnt[i];
-}
-
-__global__ void __launch_bounds__(256) k_rx_count(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
-                                                  const RxTile* __restrict__ rt, uint32_t nrt,
-                                                  uint32_t* __restrict__ cnt) {
-    __shared__ uint32_t s_cnt[kRxParts];
-    for (uint32_t T = blockIdx.x; T < nrt; T += gridDim.x) rx_count_item(in, jobs, rt[T], cnt, s_cnt);
-}
-
-// One block of kRxParts threads per large frame: thread b owns partition b.
-// Turns the per-tile counts into per-tile starting slots (in place) and
-// writes the partition's (start, length) pair.
-// One large frame j, block of kRxParts (256) threads; s_warp = 8 words.
-template <bool kC>
-__device__ void rx_scan_item(const Job* __restrict__ jobs, uint32_t j, uint32_t* __restrict__ cnt,
-                             uint2* __restrict__ parts, uint32_t* s_warp) {
-    const uint32_t b = threadIdx.x, lane = b & 31, warp = b >> 5;
-    {
-        const Job job = jobs[j];
-        const uint32_t nt = (rx_ncand(job.n) + kCandPerTile - 1) / kCandPerTile;
-        uint32_t* cj = cnt + (uint64_t)job.tile0 * kRxParts + b;
-        uint32_t total = 0;
-        for (uint32_t t = 0; t < nt; t++) total += ld_stage<kC>(cj + (uint64_t)t * kRxParts);
-        // exclusive scan of the partition totals
-        uint32_t v = total;
+    uint32_t h[16], peers[16];  // hash and same-partition lanes of each round
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, v, o);
-            if (lane >= (uint32_t)o) v += y;
-        }
-        __syncthreads();
-        if (lane == 31) s_warp[warp] = v;
-        __syncthreads();
-        uint32_t start = v - total;
-        for (uint32_t w = 0; w < warp; w++) start += s_warp[w];
-        parts[(uint64_t)j * kRxParts + b] = make_uint2(start, total);
-        uint32_t run = start;
-        for (uint32_t t = 0; t < nt; t++) {
-            const uint32_t k = ld_stage<kC>(cj + (uint64_t)t * kRxParts);
-            cj[(uint64_t)t * kRxParts] = run;
+    for (int r = 0; r < 16; r++) {
+        const uint32_t c = c0 + 512 * warp + 32 * r + lane;
+        h[r] = c < c1 ? kmer_hash(__ldg(src + c)) : 0xFFFFFFFFu;
+    }
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+        peers[r] = warp_match<9>(h[r] != 0xFFFFFFFFu ? h[r] >> kRxKeyBits : kRxParts);  // 256: no candidate
+        if (h[r] != 0xFFFFFFFFu && (peers[r] & lt) == 0) sm.w[warp][h[r] >> kRxKeyBits] += __popc(peers[r]);
+        __syncwarp();
+    }
+    __syncthreads();
+    {  // thread b: partition b's start in the slice, then each warp's first slot in it
+        const uint32_t b = tid;
+        uint32_t tot = 0;
+#pragma unroll
+        for (int w = 0; w < 8; w++) tot += sm.w[w][b];
+        uint32_t all;
+        uint32_t run = block_exclusive_scan<256>(tot, sm.warp, all);
+        toff[(uint64_t)(job.tile0 + tt.tile) * kRxParts + b] = run;
+#pragma unroll
+        for (int w = 0; w < 8; w++) {
+            const uint32_t k = sm.w[w][b];
+            sm.w[w][b] = run;
             run += k;
         }
     }
-}
-
-__global__ void __launch_bounds__(kRxParts) k_rx_scan(const Job* __restrict__ jobs, const uint32_t* __restrict__ big,
-                                                      uint32_t nbig, uint32_t* __restrict__ cnt,
-                                                      uint2* __restrict__ parts) {
-    __shared__ uint32_t s_warp[kRxParts / 32];
-    for (uint32_t x = blockIdx.x; x < nbig; x += gridDim.x) rx_scan_item<false>(jobs, big[x], cnt, parts, s_warp);
-}
-
-// 8 warps per tile, warp w taking candidates [c0 + 512w, c0 + 512w + 512)
-// in 16 rounds of 32; slots are assigned in position order.
-// One radix tile, block of 256; s_w = 8 x kRxParts words of shared memory.
-template <bool kC>
-__device__ void rx_scatter_item(const uint8_t* __restrict__ in, const Job* __restrict__ jobs, const RxTile tt,
-                                const uint32_t* off, uint32_t* __restrict__ ent,
-                                uint16_t* __restrict__ key, uint32_t (*s_w)[kRxParts]) {
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t lt = (1u << lane) - 1u;
-    {
-        const Job job = jobs[tt.job];
-        const uint64_t* src = reinterpret_cast<const uint64_t*>(in + job.in_off);
-        const uint32_t C = rx_ncand(job.n), c0 = tt.tile * kCandPerTile, c1 = min(C, c0 + kCandPerTile);
-        __syncthreads();
-        for (uint32_t i = tid; i < 8 * kRxParts; i += 256) (&s_w[0][0])[i] = 0;
-        __syncthreads();
-        uint32_t h[16], peers[16];  // hash and same-partition lanes of each round
+    __syncthreads();
 #pragma unroll
-        for (int r = 0; r < 16; r++) {
-            const uint32_t c = c0 + 512 * warp + 32 * r + lane;
-            h[r] = c < c1 ? kmer_hash(__ldg(src + c)) : 0xFFFFFFFFu;
+    for (int r = 0; r < 16; r++) {
+        const uint32_t c = c0 + 512 * warp + 32 * r + lane;
+        uint32_t slot = 0;
+        if (h[r] != 0xFFFFFFFFu) slot = sm.w[warp][h[r] >> kRxKeyBits] + __popc(peers[r] & lt);
+        __syncwarp();
+        if (h[r] != 0xFFFFFFFFu) {
+            if ((peers[r] & lt) == 0) sm.w[warp][h[r] >> kRxKeyBits] += __popc(peers[r]);
+            sm.list[slot] = (h[r] & (kRxKeys - 1)) << 12 | (c - c0);
         }
-#pragma unroll
-        for (int r = 0; r < 16; r++) {
-            peers[r] = warp_match<9>(h[r] != 0xFFFFFFFFu ? h[r] >> kRxKeyBits : kRxParts);  // 256: no candidate
-            if (h[r] != 0xFFFFFFFFu && (peers[r] & lt) == 0) s_w[warp][h[r] >> kRxKeyBits] += __popc(peers[r]);
-            __syncwarp();
-        }
-        __syncthreads();
-        for (uint32_t pt = tid; pt < kRxParts; pt += 256) {
-            uint32_t base = ld_stage<kC>(off + (uint64_t)(job.tile0 + tt.tile) * kRxParts + pt);
-            for (int w = 0; w < 8; w++) {
-                const uint32_t k = s_w[w][pt];
-                s_w[w][pt] = base;
-                base += k;
-            }
-        }
-        __syncthreads();
-        uint32_t* ej = ent + job.desc_off;
-        uint16_t* kj = key + job.desc_off;
-#pragma unroll
-        for (int r = 0; r < 16; r++) {
-            const uint32_t c = c0 + 512 * warp + 32 * r + lane;
-            uint32_t slot = 0;
-            if (h[r] != 0xFFFFFFFFu) slot = s_w[warp][h[r] >> kRxKeyBits] + __popc(peers[r] & lt);
-            __syncwarp();
-            if (h[r] != 0xFFFFFFFFu) {
-                if ((peers[r] & lt) == 0) s_w[warp][h[r] >> kRxKeyBits] += __popc(peers[r]);
-                ej[slot] = c;
-                kj[slot] = (uint16_t)(h[r] & (kRxKeys - 1));
-            }
-            __syncwarp();
-        }
+        __syncwarp();
+    }
+    __syncthreads();
+    uint32_t* lj = list + job.desc_off + c0;
+    const uint32_t m = c1 - c0;
+    if ((reinterpret_cast<uintptr_t>(lj) & 15) == 0) {
+        for (uint32_t i = tid; i < m / 4; i += 256) reinterpret_cast<uint4*>(lj)[i] = reinterpret_cast<const uint4*>(sm.list)[i];
+        for (uint32_t i = (m & ~3u) + tid; i < m; i += 256) lj[i] = sm.list[i];
+    } else {
+        for (uint32_t i = tid; i < m; i += 256) lj[i] = sm.list[i];
     }
 }
 
-__global__ void __launch_bounds__(256) k_rx_scatter(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
-                                                    const RxTile* __restrict__ rt, uint32_t nrt,
-                                                    const uint32_t* __restrict__ off, uint32_t* __restrict__ ent,
-                                                    uint16_t* __restrict__ key) {
-    __shared__ uint32_t s_w[8][kRxParts];
-    for (uint32_t T = blockIdx.x; T < nrt; T += gridDim.x) rx_scatter_item<false>(in, jobs, rt[T], off, ent, key, s_w);
+__global__ void __launch_bounds__(256) k_rx_sort(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
+                                                 const RxTile* __restrict__ rt, uint32_t nrt,
+                                                 uint32_t* __restrict__ toff, uint32_t* __restrict__ list) {
+    __shared__ RxSortSmem sm;
+    for (uint32_t T = blockIdx.x; T < nrt; T += gridDim.x) rx_sort_item(in, jobs, rt[T], toff, list, sm);
 }
 
 // Verification and extension of candidate c against its predecessor q
@@ -347,37 +301,66 @@ bytes:
 }
 
 // Partition b of large frame j, by one warp; table = kRxKeys words of
-// shared memory (latest candidate + 1 per key, 0 = none).
+// shared memory (latest candidate + 1 per key, 0 = none).  The partition is
+// the concatenation of its runs in tiles 0, 1, ...: 32 tiles at a time, lane
+// l holds tile t0 + l's run, and the slot of the warp's i-th entry is found
+// by a binary search over the runs' prefix sums.  pred[slot] = predecessor
+// + 1 (0: none).
 template <bool kC>
-__device__ void rx_resolve_warp(const Job* __restrict__ jobs, uint32_t j, uint32_t b, const uint2* parts,
-                                const uint32_t* ent, const uint16_t* key, uint32_t* __restrict__ pred,
-                                uint32_t* table) {
+__device__ void rx_resolve_warp(const Job* __restrict__ jobs, uint32_t j, uint32_t b, const uint32_t* toff,
+                                const uint32_t* list, uint32_t* __restrict__ pred, uint32_t* table) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
-    {
-        const Job job = jobs[j];
-        const uint2 pr = ld_stage<kC>(parts + (uint64_t)j * kRxParts + b);
-        if (pr.y == 0) return;
-        for (uint32_t i = lane; i < kRxKeys / 4; i += 32) reinterpret_cast<uint4*>(table)[i] = make_uint4(0, 0, 0, 0);
-        __syncwarp();
-        const uint32_t* ej = ent + job.desc_off + pr.x;
-        const uint16_t* kj = key + job.desc_off + pr.x;
-        uint32_t* pj = pred + job.desc_off + pr.x;
+    const Job job = jobs[j];
+    const uint32_t C = rx_ncand(job.n), nt = (C + kCandPerTile - 1) / kCandPerTile;
+    const uint32_t* lj = list + job.desc_off;
+    uint32_t* pj = pred + job.desc_off;
+    for (uint32_t i = lane; i < kRxKeys / 4; i += 32) reinterpret_cast<uint4*>(table)[i] = make_uint4(0, 0, 0, 0);
+    __syncwarp();
+    for (uint32_t t0 = 0; t0 < nt; t0 += 32) {
+        // lane l: the run of tile t0 + l, as slots [st, st + len) of the frame's list
+        const uint32_t t = t0 + lane;
+        uint32_t st = 0, len = 0;
+        if (t < nt) {
+            const uint32_t* to = toff + (uint64_t)(job.tile0 + t) * kRxParts;
+            const uint32_t tc = min(C - t * kCandPerTile, kCandPerTile);
+            const uint32_t a = ld_stage<kC>(to + b);
+            const uint32_t e = b + 1 < kRxParts ? ld_stage<kC>(to + b + 1) : tc;
+            st = t * kCandPerTile + a;
+            len = e - a;
+        }
+        uint32_t incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= (uint32_t)o) incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        const uint32_t excl = incl - len;
         // 256 entries per round trip: each lane loads 8 (one per chunk of 32)
         // together, then the 8 chunks resolve in order from registers
-        for (uint32_t b0 = 0; b0 < pr.y; b0 += 256) {
-            uint32_t cc[8], kk[8];
+        for (uint32_t b0 = 0; b0 < total; b0 += 256) {
+            uint32_t ee[8], sl[8];
 #pragma unroll
             for (int u = 0; u < 8; u++) {
                 const uint32_t i = b0 + 32 * u + lane;
-                cc[u] = i < pr.y ? ld_stage<kC>(ej + i) : 0u;
-                kk[u] = i < pr.y ? ld_stage<kC>(kj + i) : 0xFFFFu;
+                // the run holding entry i: the first lane whose inclusive sum exceeds i
+                uint32_t k = 0;
+#pragma unroll
+                for (uint32_t w = 16; w >= 1; w >>= 1) {
+                    const uint32_t probe = __shfl_sync(0xFFFFFFFFu, incl, k + w - 1);
+                    if (probe <= i) k += w;
+                }
+                const uint32_t sk = __shfl_sync(0xFFFFFFFFu, st, k & 31), xk = __shfl_sync(0xFFFFFFFFu, excl, k & 31);
+                sl[u] = i < total ? sk + (i - xk) : 0u;
+                ee[u] = i < total ? ld_stage<kC>(lj + sl[u]) : 0xFFFFFFFFu;
             }
 #pragma unroll
             for (int u = 0; u < 8; u++) {
                 const uint32_t i = b0 + 32 * u + lane;
-                const bool v = i < pr.y;
-                const uint32_t c = cc[u], k = kk[u];
+                const bool v = i < total;
+                const uint32_t k = ee[u] >> 12;
+                const uint32_t c = (sl[u] & ~(kCandPerTile - 1)) | (ee[u] & (kCandPerTile - 1));
                 const uint32_t peers = warp_match<12>(v ? k : kRxKeys);  // 2048: no entry
                 const uint32_t lower = peers & lt;
                 const uint32_t from = lower ? 31u - __clz(lower) : lane;
@@ -387,65 +370,62 @@ __device__ void rx_resolve_warp(const Job* __restrict__ jobs, uint32_t j, uint32
                 __syncwarp();
                 if (v && (peers >> lane) == 1u) table[k] = c + 1;
                 __syncwarp();
-                if (v) pj[i] = pv;
+                if (v) pj[sl[u]] = pv;
             }
         }
-        __syncwarp();
     }
+    __syncwarp();
 }
 
 __global__ void __launch_bounds__(kRxResolveWarps * 32) k_rx_resolve(const Job* __restrict__ jobs,
                                                                      const uint32_t* __restrict__ big, uint32_t nbig,
-                                                                     const uint2* __restrict__ parts,
-                                                                     const uint32_t* __restrict__ ent,
-                                                                     const uint16_t* __restrict__ key,
+                                                                     const uint32_t* __restrict__ toff,
+                                                                     const uint32_t* __restrict__ list,
                                                                      uint32_t* __restrict__ pred) {
     extern __shared__ __align__(16) uint32_t smem_rx[];
     const uint32_t warp = threadIdx.x >> 5;
     uint32_t* table = smem_rx + warp * kRxKeys;
     const uint32_t nw = gridDim.x * kRxResolveWarps;
     for (uint32_t x = blockIdx.x * kRxResolveWarps + warp; x < nbig * kRxParts; x += nw)
-        rx_resolve_warp<false>(jobs, big[x / kRxParts], x % kRxParts, parts, ent, key, pred, table);
+        rx_resolve_warp<false>(jobs, big[x / kRxParts], x % kRxParts, toff, list, pred, table);
 }
 
-// One thread per candidate of every large frame (grid.y = frame): verify and
-// extend against the resolved predecessor, write the descriptor.
-// Entries [lo, hi) of large frame `job`'s candidate list, thread t of
-// nthr: two entries per thread per step, their first loads in flight
-// together.
+// Slots [lo, hi) of large frame `job`'s list, thread t of nthr: verify and
+// extend each slot's candidate against its predecessor and write the
+// descriptor; two slots per thread per step, their first loads in flight
+// together.  Slot i lies in tile i / 4096's slice, so its candidate is that
+// tile's base plus the index in the list word.
 template <bool kC>
 __device__ __forceinline__ void rx_verify_range(const uint8_t* __restrict__ in, const Job& job,
-                                                const uint32_t* ent, const uint32_t* pred,
+                                                const uint32_t* list, const uint32_t* pred,
                                                 uint32_t* __restrict__ desc, uint32_t lo, uint32_t hi, uint32_t t,
                                                 uint32_t nthr) {
-    {
-        const uint32_t C = hi;
-        const uint8_t* src = in + job.in_off;
-        const uint32_t* ej = ent + job.desc_off;
-        const uint32_t* pj = pred + job.desc_off;
-        uint32_t* d8 = desc + job.desc_off;
-        const uint32_t stride = nthr;
-        for (uint32_t i = lo + t; i < C; i += 2 * stride) {
-            const uint32_t i2 = i + stride;
-            const bool two = i2 < C;
-            const uint32_t c1 = ld_stage<kC>(ej + i), p1 = ld_stage<kC>(pj + i);
-            const uint32_t c2 = two ? ld_stage<kC>(ej + i2) : 0u, p2 = two ? ld_stage<kC>(pj + i2) : 0u;
-            uint64_t x1[4], x2[4];
-            if (p1) rx_first(src, c1, p1 - 1, x1);
-            if (p2) rx_first(src, c2, p2 - 1, x2);
-            d8[c1] = p1 ? rx_finish(src, job.n, c1, p1 - 1, x1) : 0u;
-            if (two) d8[c2] = p2 ? rx_finish(src, job.n, c2, p2 - 1, x2) : 0u;
-        }
+    const uint8_t* src = in + job.in_off;
+    const uint32_t* lj = list + job.desc_off;
+    const uint32_t* pj = pred + job.desc_off;
+    uint32_t* d8 = desc + job.desc_off;
+    const uint32_t stride = nthr;
+    constexpr uint32_t kHi = ~(kCandPerTile - 1), kLo = kCandPerTile - 1;
+    for (uint32_t i = lo + t; i < hi; i += 2 * stride) {
+        const uint32_t i2 = i + stride;
+        const bool two = i2 < hi;
+        const uint32_t c1 = (i & kHi) | (ld_stage<kC>(lj + i) & kLo), p1 = ld_stage<kC>(pj + i);
+        const uint32_t c2 = two ? (i2 & kHi) | (ld_stage<kC>(lj + i2) & kLo) : 0u, p2 = two ? ld_stage<kC>(pj + i2) : 0u;
+        uint64_t x1[4], x2[4];
+        if (p1) rx_first(src, c1, p1 - 1, x1);
+        if (p2) rx_first(src, c2, p2 - 1, x2);
+        d8[c1] = p1 ? rx_finish(src, job.n, c1, p1 - 1, x1) : 0u;
+        if (two) d8[c2] = p2 ? rx_finish(src, job.n, c2, p2 - 1, x2) : 0u;
     }
 }
 
 __global__ void __launch_bounds__(256) k_rx_verify(const uint8_t* __restrict__ in, const Job* __restrict__ jobs,
-                                                   const uint32_t* __restrict__ big, const uint32_t* __restrict__ ent,
+                                                   const uint32_t* __restrict__ big, const uint32_t* __restrict__ list,
                                                    const uint32_t* __restrict__ pred, uint32_t nbig,
                                                    uint32_t* __restrict__ desc) {
     for (uint32_t y = blockIdx.y; y < nbig; y += gridDim.y) {
         const Job job = jobs[big[y]];
-        rx_verify_range<false>(in, job, ent, pred, desc, 0, rx_ncand(job.n), blockIdx.x * 256 + threadIdx.x, gridDim.x * 256);
+        rx_verify_range<false>(in, job, list, pred, desc, 0, rx_ncand(job.n), blockIdx.x * 256 + threadIdx.x, gridDim.x * 256);
     }
 }
 
