@@ -589,7 +589,9 @@ static int32_t launch_range(przmg_batch* b, cudaStream_t s, int stop_after, cons
                                      b->d_rx_list.as<uint32_t>());
         CK(cudaGetLastError());
         const uint32_t nwarps = R.nbig * kRxParts;
-        const uint32_t gr = std::min<uint32_t>((nwarps + kRxResolveWarps - 1) / kRxResolveWarps, 4u * c->sms);
+        // one block per 8 partitions: partitions differ in size, so the
+        // hardware's block scheduling balances the SMs (3 blocks fit per SM)
+        const uint32_t gr = (nwarps + kRxResolveWarps - 1) / kRxResolveWarps;
         k_rx_resolve<<<gr, kRxResolveWarps * 32, kRxResolveSmem, s>>>(
             b->d_jobs.as<Job>(), big, R.nbig, b->d_rx_toff.as<uint32_t>(), b->d_rx_list.as<uint32_t>(),
             b->d_rx_pred.as<uint32_t>());
