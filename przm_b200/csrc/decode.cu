@@ -457,24 +457,15 @@ constexpr uint32_t kDecAdaptiveSmem = 4096 * 4 + 256 * 2;
 constexpr uint32_t kDecStaticSmem = 8 * 4096 + 8 * 256 * 4;
 static_assert(kDecStaticSmem >= 4 * 4096 + 4 * 64 * 4, "Mode 12 models");
 
-// Bytes [p, p + 8) of s as a little-endian word (two aligned loads; the
-// caller keeps p + 16 <= the stream's length, and s is never within 8 bytes
-// of its buffer's start: every coded stream follows a frame header).
-__device__ __forceinline__ uint64_t ld64_at(const uint8_t* s, uint32_t p) {
-    const uintptr_t a = reinterpret_cast<uintptr_t>(s + p);
-    const uint64_t* w = reinterpret_cast<const uint64_t*>(a & ~uintptr_t(7));
-    const uint32_t sh = (uint32_t)(a & 7) * 8;
-    const uint64_t lo = w[0], hi = w[1];
-    return sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
-}
-
 // Bytes a state needs after a decode step: x' = f (x >> 12) + j >= 16 when
 // x >= 2^16, so 0, 1 or 2 (the reference's loop runs while x < 2^16).
 __device__ __forceinline__ uint32_t renorm_bytes(uint32_t x) { return (x < 65536u ? 1u : 0u) + (x < 256u ? 1u : 0u); }
-// x shifted by k bytes, taking them from u (first byte lowest) in stream order
-__device__ __forceinline__ uint32_t renorm_apply(uint32_t x, uint32_t k, uint32_t u) {
-    const uint32_t v = k == 2 ? __byte_perm(u, 0, 0x4401) : (k == 1 ? (u & 0xFFu) : 0u);
-    return (x << (8 * k)) | v;
+// x shifted by k bytes taken in stream order from byte o (o <= 6) of the
+// round's eight bytes lo (bytes 0-3) and hi (bytes 4-7): one byte permute
+// gives bytes o, o + 1 as a big-endian pair, of which the top k are used.
+__device__ __forceinline__ uint32_t renorm_pair(uint32_t x, uint32_t k, uint32_t lo, uint32_t hi, uint32_t o) {
+    const uint32_t y = __byte_perm(lo, hi, 17u * o + 1u) & 0xFFFFu;
+    return (x << (8 * k)) | (y >> (16 - 8 * k));
 }
 
 
@@ -519,36 +510,38 @@ __global__ void __launch_bounds__(32) k_dec_entropy(const DecTask* __restrict__ 
             c += f8[k];
         }
         __syncwarp();
-        if (lane != 0) return;
-        uint32_t x0 = drd32(s + p), x1 = drd32(s + p + 4), x2 = drd32(s + p + 8), x3 = drd32(s + p + 12);
+        if (lane >= 4) return;
+        // lane l holds state l (the state of symbols l, l + 4, ...)
+        uint32_t xl = drd32(s + p + 4 * lane);
         p += 16;
         uint32_t i = 0;
         bool ok = true;
-        if (x0 >= 65536u && x1 >= 65536u && x2 >= 65536u && x3 >= 65536u) {
-            // Rounds of four symbols: each lane's byte count comes from its
-            // own state, so their offsets in the round's 8 bytes are a
-            // 4-element prefix sum and the lanes renormalise side by side;
-            // only the stream position links one round to the next.
+        if (__all_sync(0xFu, xl >= 65536u)) {
+            // Rounds of four symbols, one per lane: each lane's byte count
+            // comes from its own state; two ballots give every lane all four,
+            // hence its offset in the round's 8 bytes and the stream's
+            // advance, so only the stream position links one round to the
+            // next.
+            const uintptr_t sa = reinterpret_cast<uintptr_t>(s);
+            const uint32_t lt = (1u << lane) - 1u;
             for (; i + 4 <= n && p + 16 <= slen; i += 4) {
-                const uint64_t v = ld64_at(s, p);
-                const uint32_t e0 = tab[x0 & 4095], e1 = tab[x1 & 4095], e2 = tab[x2 & 4095], e3 = tab[x3 & 4095];
-                x0 = dec_next(x0, e0);
-                x1 = dec_next(x1, e1);
-                x2 = dec_next(x2, e2);
-                x3 = dec_next(x3, e3);
-                const uint32_t k0 = renorm_bytes(x0), k1 = renorm_bytes(x1), k2 = renorm_bytes(x2), k3 = renorm_bytes(x3);
-                const uint32_t o1 = k0, o2 = o1 + k1, o3 = o2 + k2;
-                x0 = renorm_apply(x0, k0, (uint32_t)v);
-                x1 = renorm_apply(x1, k1, (uint32_t)(v >> (8 * o1)));
-                x2 = renorm_apply(x2, k2, (uint32_t)(v >> (8 * o2)));
-                x3 = renorm_apply(x3, k3, (uint32_t)(v >> (8 * o3)));
-                p += o3 + k3;
-                dst[i] = (uint8_t)e0;
-                dst[i + 1] = (uint8_t)e1;
-                dst[i + 2] = (uint8_t)e2;
-                dst[i + 3] = (uint8_t)e3;
+                // the round's eight bytes from three aligned words (below p + 12)
+                const uint32_t* w = reinterpret_cast<const uint32_t*>((sa + p) & ~uintptr_t(3));
+                const uint32_t sh = 8u * (uint32_t)((sa + p) & 3u);
+                const uint32_t w0 = w[0], w1 = w[1], w2 = w[2];
+                const uint32_t lo = __funnelshift_r(w0, w1, sh), hi = __funnelshift_r(w1, w2, sh);
+                const uint32_t e = tab[xl & 4095];
+                xl = dec_next(xl, e);
+                const uint32_t k = renorm_bytes(xl);
+                const uint32_t b1 = __ballot_sync(0xFu, k >= 1u), b2 = __ballot_sync(0xFu, k >= 2u);
+                xl = renorm_pair(xl, k, lo, hi, __popc(b1 & lt) + __popc(b2 & lt));
+                p += __popc(b1) + __popc(b2);
+                dst[i + lane] = (uint8_t)e;
             }
         }
+        uint32_t x0 = __shfl_sync(0xFu, xl, 0), x1 = __shfl_sync(0xFu, xl, 1), x2 = __shfl_sync(0xFu, xl, 2),
+                 x3 = __shfl_sync(0xFu, xl, 3);
+        if (lane != 0) return;
         // the rest (the stream's last 16 bytes, or initial states below 2^16)
         // byte by byte
         ByteWin bw;
