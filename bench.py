@@ -684,6 +684,8 @@ def main() -> None:
                     help="sections of the Section 3 distance-coding measurement (0: skip)")
     ap.add_argument("--section4-streams", type=int, default=64,
                     help="literal streams of the Section 4 selection measurement (0: skip)")
+    ap.add_argument("--decode-copies", type=int, default=10,
+                    help="copies of the batch's frames decoded in one call by the decode leg (0: skip)")
     ap.add_argument("--coded-steps", type=int, default=20,
                     help="steps of the coded-sections (P2, P3) legs on the same batch (0: skip)")
     ap.add_argument("--no-configs01", dest="configs01", action="store_false",
@@ -868,9 +870,9 @@ def main() -> None:
         bt.close()
     batches = batches[:1]
     decode = None
-    if world == 1:
+    if world == 1 and args.decode_copies > 0:
         try:
-            decode = decode_measure(comp, batch)
+            decode = decode_measure(comp, batch, copies=args.decode_copies)
         except Exception as e:  # an extra leg never costs the bench line
             decode = {"error": f"{type(e).__name__}: {e}"[:300]}
     # single-GPU runs only (under torchrun the other ranks would wait for them)
