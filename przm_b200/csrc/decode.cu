@@ -457,15 +457,32 @@ constexpr uint32_t kDecAdaptiveSmem = 4096 * 4 + 256 * 2;
 constexpr uint32_t kDecStaticSmem = 8 * 4096 + 8 * 256 * 4;
 static_assert(kDecStaticSmem >= 4 * 4096 + 4 * 64 * 4, "Mode 12 models");
 
-// Bytes a state needs after a decode step: x' = f (x >> 12) + j >= 16 when
-// x >= 2^16, so 0, 1 or 2 (the reference's loop runs while x < 2^16).
-__device__ __forceinline__ uint32_t renorm_bytes(uint32_t x) { return (x < 65536u ? 1u : 0u) + (x < 256u ? 1u : 0u); }
-// x shifted by k bytes taken in stream order from byte o (o <= 6) of the
-// round's eight bytes lo (bytes 0-3) and hi (bytes 4-7): one byte permute
-// gives bytes o, o + 1 as a big-endian pair, of which the top k are used.
-__device__ __forceinline__ uint32_t renorm_pair(uint32_t x, uint32_t k, uint32_t lo, uint32_t hi, uint32_t o) {
-    const uint32_t y = __byte_perm(lo, hi, 17u * o + 1u) & 0xFFFFu;
-    return (x << (8 * k)) | (y >> (16 - 8 * k));
+// After a decode step x' = f (x >> 12) + j >= 16 when x >= 2^16, so a state
+// takes 0, 1 or 2 bytes (the reference's loop runs while x < 2^16).
+// One round of an adaptive body on lanes 0-3 (lane l: state l, stream
+// pointer p in every lane): the lane's symbol (returned with its table
+// entry) and its state renormalised.  The round's eight stream bytes come
+// from three aligned words (below p + 12; the caller keeps p + 16 <= the
+// stream's length).  A state needs 0, 1 or 2 bytes (x < 2^16, x < 2^8
+// after the step, the reference's loop); two ballots of those tests give
+// every lane all four counts, hence its offset o (the bytes of the lanes
+// before it) and the pointer's advance.  One byte permute puts bytes o,
+// o + 1 in the low half of y, a second shifts them into x.
+__device__ __forceinline__ uint32_t dec_round(const uint32_t* tab, uintptr_t sa, uint32_t lt, uint32_t& x,
+                                              uint32_t& p) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>((sa + p) & ~uintptr_t(3));
+    const uint32_t sh = 8u * (uint32_t)((sa + p) & 3u);
+    const uint32_t w0 = w[0], w1 = w[1], w2 = w[2];
+    const uint32_t lo = __funnelshift_r(w0, w1, sh), hi = __funnelshift_r(w1, w2, sh);
+    const uint32_t e = tab[x & 4095];
+    x = dec_next(x, e);
+    const bool r1 = x < 65536u, r2 = x < 256u;
+    const uint32_t b1 = __ballot_sync(0xFu, r1), b2 = __ballot_sync(0xFu, r2);
+    const uint32_t o = __popc(b1 & lt) + __popc(b2 & lt);
+    const uint32_t y = __byte_perm(lo, hi, 17u * o + 16u);  // byte 0: stream byte o, byte 1: byte o + 1
+    x = __byte_perm(x, y, r2 ? 0x1045u : (r1 ? 0x2104u : 0x3210u));  // (x << 16 | o, o + 1), (x << 8 | o), x
+    p += __popc(b1) + __popc(b2);
+    return e;
 }
 
 
@@ -524,20 +541,12 @@ __global__ void __launch_bounds__(32) k_dec_entropy(const DecTask* __restrict__ 
             // next.
             const uintptr_t sa = reinterpret_cast<uintptr_t>(s);
             const uint32_t lt = (1u << lane) - 1u;
-            for (; i + 4 <= n && p + 16 <= slen; i += 4) {
-                // the round's eight bytes from three aligned words (below p + 12)
-                const uint32_t* w = reinterpret_cast<const uint32_t*>((sa + p) & ~uintptr_t(3));
-                const uint32_t sh = 8u * (uint32_t)((sa + p) & 3u);
-                const uint32_t w0 = w[0], w1 = w[1], w2 = w[2];
-                const uint32_t lo = __funnelshift_r(w0, w1, sh), hi = __funnelshift_r(w1, w2, sh);
-                const uint32_t e = tab[xl & 4095];
-                xl = dec_next(xl, e);
-                const uint32_t k = renorm_bytes(xl);
-                const uint32_t b1 = __ballot_sync(0xFu, k >= 1u), b2 = __ballot_sync(0xFu, k >= 2u);
-                xl = renorm_pair(xl, k, lo, hi, __popc(b1 & lt) + __popc(b2 & lt));
-                p += __popc(b1) + __popc(b2);
-                dst[i + lane] = (uint8_t)e;
+            uint8_t* dl = dst + lane;
+            for (; i + 8 <= n && p + 24 <= slen; i += 8) {  // two rounds per trip
+                dl[i] = (uint8_t)dec_round(tab, sa, lt, xl, p);
+                dl[i + 4] = (uint8_t)dec_round(tab, sa, lt, xl, p);
             }
+            for (; i + 4 <= n && p + 16 <= slen; i += 4) dl[i] = (uint8_t)dec_round(tab, sa, lt, xl, p);
         }
         uint32_t x0 = __shfl_sync(0xFu, xl, 0), x1 = __shfl_sync(0xFu, xl, 1), x2 = __shfl_sync(0xFu, xl, 2),
                  x3 = __shfl_sync(0xFu, xl, 3);
@@ -813,19 +822,39 @@ struct Reps {
     __device__ __forceinline__ void explicit_(uint32_t d) { r3 = r2; r2 = r1; r1 = r0; r0 = d; }
 };
 
-// Warp copies.  Literals: n bytes from src.  Match: n bytes from d back,
-// byte i from byte (i mod d) of the source run (the byte-wise forward copy
-// of an overlapping match repeats with period d).
-__device__ __forceinline__ void warp_copy_lits(uint8_t* dst, const uint8_t* src, uint32_t n) {
-    for (uint32_t i = threadIdx.x & 31; i < n; i += 32) dst[i] = src[i];
+// Warp copies into dst (the output at position pos) and into the ring, the
+// last kExecRing output bytes in shared memory.  Literals: n bytes from src.
+// Match: n bytes from d back, byte i from byte (i mod d) of the source run
+// (the byte-wise forward copy of an overlapping match repeats with period
+// d); read from the ring when d + n <= kExecRing (every source byte is then
+// in it and no byte the match writes lands on one it still reads), else from
+// the output in global memory.
+constexpr uint32_t kExecRing = 8192;
+__device__ __forceinline__ void warp_copy_lits(uint8_t* dst, uint8_t* ring, uint32_t pos, const uint8_t* src,
+                                               uint32_t n) {
+    for (uint32_t i = threadIdx.x & 31; i < n; i += 32) {
+        const uint8_t b = src[i];
+        dst[i] = b;
+        ring[(pos + i) & (kExecRing - 1)] = b;
+    }
     __syncwarp();
 }
-__device__ __forceinline__ void warp_copy_match(uint8_t* dst, uint32_t d, uint32_t n) {
-    const uint8_t* s = dst - d;
-    if (d >= n) {
-        for (uint32_t i = threadIdx.x & 31; i < n; i += 32) dst[i] = s[i];
+__device__ __forceinline__ void warp_copy_match(uint8_t* dst, uint8_t* ring, uint32_t pos, uint32_t d, uint32_t n) {
+    const uint32_t lane = threadIdx.x & 31;
+    if (d + n <= kExecRing) {
+        const uint32_t base = pos - d;
+        for (uint32_t i = lane; i < n; i += 32) {
+            const uint8_t b = ring[(base + (d >= n ? i : i % d)) & (kExecRing - 1)];
+            dst[i] = b;
+            ring[(pos + i) & (kExecRing - 1)] = b;
+        }
     } else {
-        for (uint32_t i = threadIdx.x & 31; i < n; i += 32) dst[i] = s[i % d];
+        const uint8_t* s = dst - d;
+        for (uint32_t i = lane; i < n; i += 32) {
+            const uint8_t b = s[d >= n ? i : i % d];
+            dst[i] = b;
+            ring[(pos + i) & (kExecRing - 1)] = b;
+        }
     }
     __syncwarp();
 }
@@ -844,8 +873,9 @@ __global__ void __launch_bounds__(32) k_dec_exec(const uint8_t* __restrict__ src
     const DecJob jb = jobs[f];
     uint8_t* dst = out + jb.out_off;
     const uint32_t u = I.u_size;
+    __shared__ __align__(16) uint8_t ring[kExecRing];
     if (I.stored) {
-        warp_copy_lits(dst, src + jb.src_off + 8, u);
+        warp_copy_lits(dst, ring, 0, src + jb.src_off + 8, u);
         return;
     }
     CmdReader R;
@@ -921,13 +951,16 @@ __global__ void __launch_bounds__(32) k_dec_exec(const uint8_t* __restrict__ src
         if (kind == 4) {  // byte run
             if (lp >= ll || dp + lmatch > u) { err = D_CORRUPT; break; }
             const uint8_t b = lit[lp++];
-            for (uint32_t i = lane; i < lmatch; i += 32) dst[dp + i] = b;
+            for (uint32_t i = lane; i < lmatch; i += 32) {
+                dst[dp + i] = b;
+                ring[(dp + i) & (kExecRing - 1)] = b;
+            }
             __syncwarp();
             dp += lmatch;
             continue;
         }
         if (lp + llit > ll || dp + llit > u) { err = D_CORRUPT; break; }
-        warp_copy_lits(dst + dp, lit + lp, llit);
+        warp_copy_lits(dst + dp, ring, dp, lit + lp, llit);
         lp += llit;
         dp += llit;
         if (kind == 0) continue;
@@ -940,7 +973,7 @@ __global__ void __launch_bounds__(32) k_dec_exec(const uint8_t* __restrict__ src
             r.explicit_(d);
         }
         if (d == 0 || d > dp || dp + lmatch > u) { err = D_CORRUPT; break; }  // no dictionary: d <= dp
-        warp_copy_match(dst + dp, d, lmatch);
+        warp_copy_match(dst + dp, ring, dp, d, lmatch);
         dp += lmatch;
     }
     if (!err && dp != u) err = D_CORRUPT;
