@@ -7,13 +7,16 @@
 //   k_dec_parse    one thread per frame: header, directory and sections
 //                  (stage_parse_header / stage_resolve_sections); the form
 //                  of each section; one entropy task per coded stream.
-//   k_dec_entropy  one warp per entropy task: the adaptive V-ANS body
-//                  (matrix -> frequencies -> decode table, built by the
-//                  warp), the Meta8 container (8 static context models) or
-//                  the Mode 12 code stream (4 static context models), then
-//                  the serial rANS chain on lane 0: the four interleaved
-//                  states share one stream pointer, so the chain is one
-//                  symbol at a time by the format.
+//   k_dec_static   one warp per Meta8 container (8 static context models)
+//                  or Mode 12 code stream (4 static context models), the
+//                  chain on lane 0, one symbol at a time (each symbol's
+//                  context is the symbol before it);
+//   k_dec_lists    the adaptive V-ANS bodies, longest first;
+//   k_dec_adaptive eight bodies per warp: a group of four lanes per body,
+//                  lane l holding interleaved state l; the four states share
+//                  one stream pointer, so each round of four symbols waits
+//                  for the one before it (matrix -> frequencies -> model,
+//                  built by the warp).
 //   k_dec_prefix   one block per frame with a distance-prefix Section 3:
 //                  extra-bit offsets and varint lengths by block scans, the
 //                  distances rebuilt and written as LEB128 varints.
@@ -331,27 +334,18 @@ __global__ void k_dec_parse(const uint8_t* __restrict__ src, const DecJob* __res
     for (int k = 0; k < kDecTasks; k++) tasks[(uint64_t)f * kDecTasks + k] = T[k];
 }
 
-// Static decode tables in the adaptive table's entry form (below): the 8
-// Meta8 models (core/commands/vans_meta_tables.go) and the 4 Mode 12
-// distance-code models (core/distance/distance.go:67-93), built on the host.
-// Per context: the symbol of every slot, and per symbol (f - 1) << 20 | its
-// cumulative frequency.  Compact (41 KiB for Meta8), so a decoding warp keeps
-// its model in shared memory: the serial chain's lookups then never wait on
-// L2.
+// Static decode models: the 8 Meta8 models (core/commands/vans_meta_tables.go)
+// and the 4 Mode 12 distance-code models (core/distance/distance.go:67-93),
+// built on the host.  Per context: the symbol of every slot, and per symbol
+// (f - 1) << 20 | its cumulative frequency (the adaptive models' form too).
+// Compact (41 KiB for Meta8), so a decoding warp keeps its model in shared
+// memory: the serial chain's lookups then never wait on L2.
 struct DecStatic {
     uint8_t m8sym[8][4096];
     uint32_t m8fc[8][256];
     uint8_t d12sym[4][4096];
     uint32_t d12fc[4][64];
 };
-
-// Decode-table entry of slot j of symbol s (frequency f): s | j << 8 |
-// (f - 1) << 20, so x' = f (x >> 12) + j is ((e >> 20) + 1) (x >> 12) +
-// ((e >> 8) & 0xFFF) (the rANS decode step, przm_dec.c:187-199).
-__host__ __device__ inline uint32_t dec_entry(uint32_t f, uint32_t j, uint32_t s) { return ((f - 1) << 20) | (j << 8) | s; }
-__device__ __forceinline__ uint32_t dec_next(uint32_t x, uint32_t e) {
-    return ((e >> 20) + 1) * (x >> 12) + ((e >> 8) & 0xFFFu);
-}
 
 __device__ __forceinline__ uint32_t ctx_meta8(uint32_t p) {  // ContextMeta, core/commands/vans_meta.go:46-69
     return p == 0 ? 0u : p < 4 ? 1u : p < 16 ? 2u : p < 32 ? 3u : p < 64 ? 4u : p < 128 ? 5u : p < 192 ? 6u : 7u;
@@ -449,137 +443,28 @@ struct ByteWin {
     __device__ __forceinline__ uint32_t pos() const { return q - nn - av; }  // bytes consumed
 };
 
-// Shared memory of an adaptive body's task (decode table + frequencies) and
-// of a static-model task (the Meta8 models, the larger of the two).  The two
-// kinds run as separate launches so the long adaptive chains are not held
-// to the occupancy of the larger allotment.
-constexpr uint32_t kDecAdaptiveSmem = 4096 * 4 + 256 * 2;
+// Shared memory of a static-model task (the Meta8 models, the larger of the
+// two kinds).  Static-model and adaptive tasks run as separate launches so the
+// long adaptive chains are not held to the occupancy of this allotment.
 constexpr uint32_t kDecStaticSmem = 8 * 4096 + 8 * 256 * 4;
 static_assert(kDecStaticSmem >= 4 * 4096 + 4 * 64 * 4, "Mode 12 models");
 
 // After a decode step x' = f (x >> 12) + j >= 16 when x >= 2^16, so a state
 // takes 0, 1 or 2 bytes (the reference's loop runs while x < 2^16).
-// One round of an adaptive body on lanes 0-3 (lane l: state l, stream
-// pointer p in every lane): the lane's symbol (returned with its table
-// entry) and its state renormalised.  The round's eight stream bytes come
-// from three aligned words (below p + 12; the caller keeps p + 16 <= the
-// stream's length).  A state needs 0, 1 or 2 bytes (x < 2^16, x < 2^8
-// after the step, the reference's loop); two ballots of those tests give
-// every lane all four counts, hence its offset o (the bytes of the lanes
-// before it) and the pointer's advance.  One byte permute puts bytes o,
-// o + 1 in the low half of y, a second shifts them into x.
-__device__ __forceinline__ uint32_t dec_round(const uint32_t* tab, uintptr_t sa, uint32_t lt, uint32_t& x,
-                                              uint32_t& p) {
-    const uint32_t* w = reinterpret_cast<const uint32_t*>((sa + p) & ~uintptr_t(3));
-    const uint32_t sh = 8u * (uint32_t)((sa + p) & 3u);
-    const uint32_t w0 = w[0], w1 = w[1], w2 = w[2];
-    const uint32_t lo = __funnelshift_r(w0, w1, sh), hi = __funnelshift_r(w1, w2, sh);
-    const uint32_t e = tab[x & 4095];
-    x = dec_next(x, e);
-    const bool r1 = x < 65536u, r2 = x < 256u;
-    const uint32_t b1 = __ballot_sync(0xFu, r1), b2 = __ballot_sync(0xFu, r2);
-    const uint32_t o = __popc(b1 & lt) + __popc(b2 & lt);
-    const uint32_t y = __byte_perm(lo, hi, 17u * o + 16u);  // byte 0: stream byte o, byte 1: byte o + 1
-    x = __byte_perm(x, y, r2 ? 0x1045u : (r1 ? 0x2104u : 0x3210u));  // (x << 16 | o, o + 1), (x << 8 | o), x
-    p += __popc(b1) + __popc(b2);
-    return e;
-}
 
-
-// One warp per task (tasks[blockIdx.x]): blocks of one warp, so the serial
-// chains spread over the SMs.  statics: run the Meta8 and Mode 12 tasks
-// (else the adaptive ones).
-__global__ void __launch_bounds__(32) k_dec_entropy(const DecTask* __restrict__ tasks, const DecStatic* __restrict__ st,
-                                                    DecInfo* __restrict__ infos, uint32_t statics) {
+// Static-model tasks (Meta8 containers, Mode 12 code streams), one warp per
+// task slot (tasks[blockIdx.x]; other kinds return at once): the warp copies
+// the models into shared memory, lane 0 runs the chain (one symbol at a
+// time: each symbol's context is the symbol before it).
+__global__ void __launch_bounds__(32) k_dec_static(const DecTask* __restrict__ tasks, const DecStatic* __restrict__ st,
+                                                   DecInfo* __restrict__ infos) {
     extern __shared__ __align__(16) uint8_t smem_d[];
-    uint32_t* tab = reinterpret_cast<uint32_t*>(smem_d);
-    uint16_t* freq = reinterpret_cast<uint16_t*>(smem_d + 4096 * 4);
     const DecTask t = tasks[blockIdx.x];
     const uint32_t lane = threadIdx.x;
-    if (t.kind == DT_NONE || t.n == 0 || (t.kind == DT_ADAPTIVE) == (statics != 0)) return;
+    if ((t.kind != DT_META8 && t.kind != DT_MODE12) || t.n == 0) return;
     const uint8_t* s = reinterpret_cast<const uint8_t*>(t.src);
     uint8_t* dst = reinterpret_cast<uint8_t*>(t.dst);
     const uint32_t n = t.n, slen = t.slen;
-    if (t.kind == DT_ADAPTIVE) {
-        for (uint32_t i = lane; i < 256; i += 32) freq[i] = 0;
-        __syncwarp();
-        uint32_t p = 0;
-        if (lane == 0) p = dec_matrix(s, slen, freq);
-        p = __shfl_sync(0xFFFFFFFFu, p, 0);
-        if (p == 0 || p + 16 > slen) {
-            if (lane == 0) dec_fail(infos, t.frame, D_CORRUPT);
-            return;
-        }
-        __syncwarp();
-        // decode table: lane l takes symbols 8l .. 8l + 7
-        uint32_t f8[8], loc = 0;
-#pragma unroll
-        for (int k = 0; k < 8; k++) { f8[k] = freq[lane * 8 + k]; loc += f8[k]; }
-        uint32_t x = loc;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-            if (lane >= (uint32_t)o) x += y;
-        }
-        uint32_t c = x - loc;
-        for (int k = 0; k < 8; k++) {
-            for (uint32_t j = 0; j < f8[k]; j++) tab[c + j] = dec_entry(f8[k], j, lane * 8 + k);
-            c += f8[k];
-        }
-        __syncwarp();
-        if (lane >= 4) return;
-        // lane l holds state l (the state of symbols l, l + 4, ...)
-        uint32_t xl = drd32(s + p + 4 * lane);
-        p += 16;
-        uint32_t i = 0;
-        bool ok = true;
-        if (__all_sync(0xFu, xl >= 65536u)) {
-            // Rounds of four symbols, one per lane: each lane's byte count
-            // comes from its own state; two ballots give every lane all four,
-            // hence its offset in the round's 8 bytes and the stream's
-            // advance, so only the stream position links one round to the
-            // next.
-            const uintptr_t sa = reinterpret_cast<uintptr_t>(s);
-            const uint32_t lt = (1u << lane) - 1u;
-            uint8_t* dl = dst + lane;
-            for (; i + 8 <= n && p + 24 <= slen; i += 8) {  // two rounds per trip
-                dl[i] = (uint8_t)dec_round(tab, sa, lt, xl, p);
-                dl[i + 4] = (uint8_t)dec_round(tab, sa, lt, xl, p);
-            }
-            for (; i + 4 <= n && p + 16 <= slen; i += 4) dl[i] = (uint8_t)dec_round(tab, sa, lt, xl, p);
-        }
-        uint32_t x0 = __shfl_sync(0xFu, xl, 0), x1 = __shfl_sync(0xFu, xl, 1), x2 = __shfl_sync(0xFu, xl, 2),
-                 x3 = __shfl_sync(0xFu, xl, 3);
-        if (lane != 0) return;
-        // the rest (the stream's last 16 bytes, or initial states below 2^16)
-        // byte by byte
-        ByteWin bw;
-        bw.init(s, slen, p);
-        bw.prefetch();
-        for (; i + 4 <= n && ok; i += 4) {  // vans_run_4x_loop, przm_dec.c:201-255
-            bw.step();
-            const uint32_t e0 = tab[x0 & 4095], e1 = tab[x1 & 4095], e2 = tab[x2 & 4095], e3 = tab[x3 & 4095];
-            x0 = dec_next(x0, e0);
-            x1 = dec_next(x1, e1);
-            x2 = dec_next(x2, e2);
-            x3 = dec_next(x3, e3);
-            ok = bw.renorm(x0) && bw.renorm(x1) && bw.renorm(x2) && bw.renorm(x3);
-            dst[i] = (uint8_t)e0;
-            dst[i + 1] = (uint8_t)e1;
-            dst[i + 2] = (uint8_t)e2;
-            dst[i + 3] = (uint8_t)e3;
-        }
-        uint32_t xs[4] = {x0, x1, x2, x3};
-        for (; i < n && ok; i++) {
-            bw.step();
-            const uint32_t e = tab[xs[i & 3] & 4095];
-            dst[i] = (uint8_t)e;
-            xs[i & 3] = dec_next(xs[i & 3], e);
-            ok = bw.renorm(xs[i & 3]);
-        }
-        if (!ok) dec_fail(infos, t.frame, D_CORRUPT);
-        return;
-    }
     // the static models into shared memory (the warp), then the chain (lane 0)
     const bool m8 = t.kind == DT_META8;
     const uint32_t nsym = m8 ? 8 * 4096 : 4 * 4096, nfc = m8 ? 8 * 256 : 4 * 64;
@@ -625,6 +510,183 @@ __global__ void __launch_bounds__(32) k_dec_entropy(const DecTask* __restrict__ 
         prev = sym;
         x = ((fc >> 20) + 1) * (x >> 12) + slot - (fc & 0xFFFFFu);
         ok = bw.renorm(x);
+    }
+    if (!ok) dec_fail(infos, t.frame, D_CORRUPT);
+}
+
+// Adaptive bodies, eight per warp: lane group g (lanes 4g .. 4g + 3) of
+// block b decodes task list[8 b + g], lane 4g + l holding state l.  The warp
+// builds the eight models one after another (per model the symbol of every
+// slot and (f - 1) << 20 | cumulative frequency per symbol, 5 KiB), then all
+// groups run their rounds together, so one warp instruction advances eight
+// chains; the list is sorted by length (k_dec_lists), so a warp's chains
+// end close together.
+constexpr uint32_t kDecGroups = 8;
+constexpr uint32_t kDecModel = 4096 + 256 * 4;
+constexpr uint32_t kDecAdaptiveSmem = kDecGroups * kDecModel + 256 * 2 + kDecGroups * 4;
+
+// The decoded state after symbol slot x & 4095 with model word g = (f - 1)
+// << 20 | cumulative frequency: f (x >> 12) + (x & 4095) - cum (the rANS
+// decode step, przm_dec.c:187-199).
+__device__ __forceinline__ uint32_t dec_step(uint32_t x, uint32_t g) {
+    return ((g >> 20) + 1) * (x >> 12) + (x & 4095u) - (g & 0xFFFFFu);
+}
+
+// The adaptive tasks of the slots, longest first by bit length of their
+// symbol count: list[0] = their number, list[4 ..] their slot indices.  One
+// block of 1024 threads (counts per bit length, their offsets, then places).
+__global__ void __launch_bounds__(1024) k_dec_lists(const DecTask* __restrict__ tasks, uint32_t nslots,
+                                                    uint32_t* __restrict__ list) {
+    __shared__ uint32_t s_cnt[32], s_off[32];
+    if (threadIdx.x < 32) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nslots; i += 1024) {
+        const DecTask t = tasks[i];
+        if (t.kind == DT_ADAPTIVE && t.n) atomicAdd(&s_cnt[31 - __clz(t.n)], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t o = 0;
+        for (int b = 31; b >= 0; b--) {
+            s_off[b] = o;
+            o += s_cnt[b];
+        }
+        list[0] = o;
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nslots; i += 1024) {
+        const DecTask t = tasks[i];
+        if (t.kind == DT_ADAPTIVE && t.n) list[4 + atomicAdd(&s_off[31 - __clz(t.n)], 1u)] = i;
+    }
+}
+
+__global__ void __launch_bounds__(32) k_dec_adaptive(const DecTask* __restrict__ tasks, const uint32_t* __restrict__ list,
+                                                     DecInfo* __restrict__ infos) {
+    extern __shared__ __align__(16) uint8_t smem_d[];
+    uint16_t* freq = reinterpret_cast<uint16_t*>(smem_d + kDecGroups * kDecModel);
+    uint32_t* gp = reinterpret_cast<uint32_t*>(smem_d + kDecGroups * kDecModel + 512);
+    const uint32_t lane = threadIdx.x, g = lane >> 2, l = lane & 3;
+    const uint32_t base = blockIdx.x * kDecGroups, cnt = list[0];
+    if (base >= cnt) return;
+    // the models, one after another by the whole warp; gp[k]: group k's
+    // stream offset after its matrix (0: no task, or a corrupt matrix)
+    for (uint32_t k = 0; k < kDecGroups; k++) {
+        uint32_t p = 0;
+        if (base + k < cnt) {
+            const DecTask t = tasks[list[4 + base + k]];
+            const uint8_t* s = reinterpret_cast<const uint8_t*>(t.src);
+            for (uint32_t i = lane; i < 256; i += 32) freq[i] = 0;
+            __syncwarp();
+            if (lane == 0) p = dec_matrix(s, t.slen, freq);
+            p = __shfl_sync(0xFFFFFFFFu, p, 0);
+            if (p == 0 || p + 16 > t.slen) {
+                if (lane == 0) dec_fail(infos, t.frame, D_CORRUPT);
+                p = 0;
+            } else {
+                // lane l takes symbols 8l .. 8l + 7 (the frequencies sum to
+                // 4096, so every slot is written)
+                uint8_t* sym = smem_d + k * kDecModel;
+                uint32_t* fct = reinterpret_cast<uint32_t*>(sym + 4096);
+                uint32_t f8[8], loc = 0;
+#pragma unroll
+                for (int q = 0; q < 8; q++) { f8[q] = freq[lane * 8 + q]; loc += f8[q]; }
+                uint32_t x = loc;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+                    if (lane >= (uint32_t)o) x += y;
+                }
+                uint32_t c = x - loc;
+                for (int q = 0; q < 8; q++) {
+                    fct[lane * 8 + q] = f8[q] ? ((f8[q] - 1) << 20) | c : 0u;
+                    for (uint32_t j = 0; j < f8[q]; j++) sym[c + j] = (uint8_t)(lane * 8 + q);
+                    c += f8[q];
+                }
+            }
+        }
+        if (lane == 0) gp[k] = p;
+        __syncwarp();
+    }
+    // this lane's group and state
+    const bool has = base + g < cnt;
+    DecTask t = {};
+    if (has) t = tasks[list[4 + base + g]];
+    uint32_t p = gp[g];
+    const bool valid = has && p != 0;
+    const uint8_t* s = reinterpret_cast<const uint8_t*>(t.src);
+    uint8_t* dst = reinterpret_cast<uint8_t*>(t.dst);
+    const uint32_t n = t.n, slen = t.slen;
+    const uint8_t* sym = smem_d + g * kDecModel;
+    const uint32_t* fct = reinterpret_cast<const uint32_t*>(sym + 4096);
+    uint32_t x = valid ? drd32(s + p + 4 * l) : 0u;
+    p += 16;
+    const uint32_t gm = 0xFu << (4 * g), lt = (1u << lane) - 1u;
+    // every lane takes part in each warp vote below, whether its group has a
+    // task or not (a lane that skipped one would leave the others waiting)
+    const uint32_t vb = __ballot_sync(0xFFFFFFFFu, valid && x >= 65536u);
+    const bool fast = valid && (vb & gm) == gm;
+    uint32_t i = 0;
+    const uintptr_t sa = reinterpret_cast<uintptr_t>(s);
+    // Rounds of four symbols per group.  The round's eight stream bytes come
+    // from three aligned words (below p + 12; the loop keeps p + 16 <= the
+    // stream's length).  A state needs 0, 1 or 2 bytes (x < 2^16, x < 2^8
+    // after the step); two ballots of those tests, each group reading its
+    // own four bits, give every lane its offset o (the bytes of the group's
+    // lanes before it) and the pointer's advance.  One byte permute puts
+    // bytes o, o + 1 in the low half of y, a second shifts them into x.
+    for (;;) {
+        const bool act = fast && i + 4 <= n && p + 16 <= slen;
+        if (!__any_sync(0xFFFFFFFFu, act)) break;
+        uint32_t lo = 0, hi = 0, sv = 0;
+        if (act) {
+            const uint32_t* w = reinterpret_cast<const uint32_t*>((sa + p) & ~uintptr_t(3));
+            const uint32_t sh = 8u * (uint32_t)((sa + p) & 3u);
+            const uint32_t w0 = w[0], w1 = w[1], w2 = w[2];
+            lo = __funnelshift_r(w0, w1, sh);
+            hi = __funnelshift_r(w1, w2, sh);
+            sv = sym[x & 4095];
+            x = dec_step(x, fct[sv]);
+        }
+        const bool r1 = act && x < 65536u, r2 = act && x < 256u;
+        const uint32_t b1 = __ballot_sync(0xFFFFFFFFu, r1) & gm, b2 = __ballot_sync(0xFFFFFFFFu, r2) & gm;
+        if (act) {
+            const uint32_t o = __popc(b1 & lt) + __popc(b2 & lt);
+            const uint32_t y = __byte_perm(lo, hi, 17u * o + 16u);
+            x = __byte_perm(x, y, r2 ? 0x1045u : (r1 ? 0x2104u : 0x3210u));
+            p += __popc(b1) + __popc(b2);
+            dst[i + l] = (uint8_t)sv;
+            i += 4;
+        }
+    }
+    uint32_t x0 = __shfl_sync(0xFFFFFFFFu, x, 4 * g), x1 = __shfl_sync(0xFFFFFFFFu, x, 4 * g + 1),
+             x2 = __shfl_sync(0xFFFFFFFFu, x, 4 * g + 2), x3 = __shfl_sync(0xFFFFFFFFu, x, 4 * g + 3);
+    if (l != 0 || !valid) return;
+    // the rest (the stream's last 16 bytes, or initial states below 2^16)
+    // byte by byte, on the group's first lane
+    bool ok = true;
+    ByteWin bw;
+    bw.init(s, slen, p);
+    bw.prefetch();
+    for (; i + 4 <= n && ok; i += 4) {  // vans_run_4x_loop, przm_dec.c:201-255
+        bw.step();
+        const uint32_t s0 = sym[x0 & 4095], s1 = sym[x1 & 4095], s2 = sym[x2 & 4095], s3 = sym[x3 & 4095];
+        x0 = dec_step(x0, fct[s0]);
+        x1 = dec_step(x1, fct[s1]);
+        x2 = dec_step(x2, fct[s2]);
+        x3 = dec_step(x3, fct[s3]);
+        ok = bw.renorm(x0) && bw.renorm(x1) && bw.renorm(x2) && bw.renorm(x3);
+        dst[i] = (uint8_t)s0;
+        dst[i + 1] = (uint8_t)s1;
+        dst[i + 2] = (uint8_t)s2;
+        dst[i + 3] = (uint8_t)s3;
+    }
+    uint32_t xs[4] = {x0, x1, x2, x3};
+    for (; i < n && ok; i++) {
+        bw.step();
+        const uint32_t v = sym[xs[i & 3] & 4095];
+        dst[i] = (uint8_t)v;
+        xs[i & 3] = dec_step(xs[i & 3], fct[v]);
+        ok = bw.renorm(xs[i & 3]);
     }
     if (!ok) dec_fail(infos, t.frame, D_CORRUPT);
 }
