@@ -514,6 +514,136 @@ __global__ void __launch_bounds__(32) k_dec_static(const DecTask* __restrict__ t
     if (!ok) dec_fail(infos, t.frame, D_CORRUPT);
 }
 
+// Decode-table entry of slot j of symbol s (frequency f): s | j << 8 |
+// (f - 1) << 20, so x' = f (x >> 12) + j is ((e >> 20) + 1) (x >> 12) +
+// ((e >> 8) & 0xFFF) (the rANS decode step, przm_dec.c:187-199).
+__host__ __device__ inline uint32_t dec_entry(uint32_t f, uint32_t j, uint32_t s) { return ((f - 1) << 20) | (j << 8) | s; }
+__device__ __forceinline__ uint32_t dec_next(uint32_t x, uint32_t e) {
+    return ((e >> 20) + 1) * (x >> 12) + ((e >> 8) & 0xFFFu);
+}
+
+// One round of an adaptive body on lanes 0-3 (lane l: state l, stream
+// pointer p in every lane): the lane's symbol (returned with its table
+// entry) and its state renormalised.  The round's eight stream bytes come
+// from three aligned words (below p + 12; the caller keeps p + 16 <= the
+// stream's length).  A state needs 0, 1 or 2 bytes (x < 2^16, x < 2^8
+// after the step, the reference's loop); two ballots of those tests give
+// every lane all four counts, hence its offset o (the bytes of the lanes
+// before it) and the pointer's advance.  One byte permute puts bytes o,
+// o + 1 in the low half of y, a second shifts them into x.
+__device__ __forceinline__ uint32_t dec_round(const uint32_t* tab, uintptr_t sa, uint32_t lt, uint32_t& x,
+                                              uint32_t& p) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>((sa + p) & ~uintptr_t(3));
+    const uint32_t sh = 8u * (uint32_t)((sa + p) & 3u);
+    const uint32_t w0 = w[0], w1 = w[1], w2 = w[2];
+    const uint32_t lo = __funnelshift_r(w0, w1, sh), hi = __funnelshift_r(w1, w2, sh);
+    const uint32_t e = tab[x & 4095];
+    x = dec_next(x, e);
+    const bool r1 = x < 65536u, r2 = x < 256u;
+    const uint32_t b1 = __ballot_sync(0xFu, r1), b2 = __ballot_sync(0xFu, r2);
+    const uint32_t o = __popc(b1 & lt) + __popc(b2 & lt);
+    const uint32_t y = __byte_perm(lo, hi, 17u * o + 16u);  // byte 0: stream byte o, byte 1: byte o + 1
+    x = __byte_perm(x, y, r2 ? 0x1045u : (r1 ? 0x2104u : 0x3210u));  // (x << 16 | o, o + 1), (x << 8 | o), x
+    p += __popc(b1) + __popc(b2);
+    return e;
+}
+
+// One adaptive body per warp (task slot blockIdx.x; other kinds return at
+// once), for batches whose bodies all fit on the SMs at once: the warp builds
+// a 4096-entry table (s | j << 8 | (f - 1) << 20 per slot, one shared load
+// per step), lanes 0-3 run the body's four states.  Its rounds are the
+// shortest of the two adaptive kernels; k_dec_adaptive trades them for eight
+// bodies per warp when there are many.
+constexpr uint32_t kDecAdaptive1Smem = 4096 * 4 + 256 * 2;
+__global__ void __launch_bounds__(32) k_dec_adaptive1(const DecTask* __restrict__ tasks, DecInfo* __restrict__ infos) {
+    extern __shared__ __align__(16) uint8_t smem_d[];
+    uint32_t* tab = reinterpret_cast<uint32_t*>(smem_d);
+    uint16_t* freq = reinterpret_cast<uint16_t*>(smem_d + 4096 * 4);
+    const DecTask t = tasks[blockIdx.x];
+    const uint32_t lane = threadIdx.x;
+    if (t.kind != DT_ADAPTIVE || t.n == 0) return;
+    const uint8_t* s = reinterpret_cast<const uint8_t*>(t.src);
+    uint8_t* dst = reinterpret_cast<uint8_t*>(t.dst);
+    const uint32_t n = t.n, slen = t.slen;
+    for (uint32_t i = lane; i < 256; i += 32) freq[i] = 0;
+    __syncwarp();
+    uint32_t p = 0;
+    if (lane == 0) p = dec_matrix(s, slen, freq);
+    p = __shfl_sync(0xFFFFFFFFu, p, 0);
+    if (p == 0 || p + 16 > slen) {
+        if (lane == 0) dec_fail(infos, t.frame, D_CORRUPT);
+        return;
+    }
+    __syncwarp();
+    // decode table: lane l takes symbols 8l .. 8l + 7
+    uint32_t f8[8], loc = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) { f8[k] = freq[lane * 8 + k]; loc += f8[k]; }
+    uint32_t x = loc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    uint32_t c = x - loc;
+    for (int k = 0; k < 8; k++) {
+        for (uint32_t j = 0; j < f8[k]; j++) tab[c + j] = dec_entry(f8[k], j, lane * 8 + k);
+        c += f8[k];
+    }
+    __syncwarp();
+    if (lane >= 4) return;
+    // lane l holds state l (the state of symbols l, l + 4, ...)
+    uint32_t xl = drd32(s + p + 4 * lane);
+    p += 16;
+    uint32_t i = 0;
+    bool ok = true;
+    if (__all_sync(0xFu, xl >= 65536u)) {
+        // Rounds of four symbols, one per lane: each lane's byte count
+        // comes from its own state; two ballots give every lane all four,
+        // hence its offset in the round's 8 bytes and the stream's
+        // advance, so only the stream position links one round to the
+        // next.
+        const uintptr_t sa = reinterpret_cast<uintptr_t>(s);
+        const uint32_t lt = (1u << lane) - 1u;
+        uint8_t* dl = dst + lane;
+        for (; i + 8 <= n && p + 24 <= slen; i += 8) {  // two rounds per trip
+            dl[i] = (uint8_t)dec_round(tab, sa, lt, xl, p);
+            dl[i + 4] = (uint8_t)dec_round(tab, sa, lt, xl, p);
+        }
+        for (; i + 4 <= n && p + 16 <= slen; i += 4) dl[i] = (uint8_t)dec_round(tab, sa, lt, xl, p);
+    }
+    uint32_t x0 = __shfl_sync(0xFu, xl, 0), x1 = __shfl_sync(0xFu, xl, 1), x2 = __shfl_sync(0xFu, xl, 2),
+             x3 = __shfl_sync(0xFu, xl, 3);
+    if (lane != 0) return;
+    // the rest (the stream's last 16 bytes, or initial states below 2^16)
+    // byte by byte
+    ByteWin bw;
+    bw.init(s, slen, p);
+    bw.prefetch();
+    for (; i + 4 <= n && ok; i += 4) {  // vans_run_4x_loop, przm_dec.c:201-255
+        bw.step();
+        const uint32_t e0 = tab[x0 & 4095], e1 = tab[x1 & 4095], e2 = tab[x2 & 4095], e3 = tab[x3 & 4095];
+        x0 = dec_next(x0, e0);
+        x1 = dec_next(x1, e1);
+        x2 = dec_next(x2, e2);
+        x3 = dec_next(x3, e3);
+        ok = bw.renorm(x0) && bw.renorm(x1) && bw.renorm(x2) && bw.renorm(x3);
+        dst[i] = (uint8_t)e0;
+        dst[i + 1] = (uint8_t)e1;
+        dst[i + 2] = (uint8_t)e2;
+        dst[i + 3] = (uint8_t)e3;
+    }
+    uint32_t xs[4] = {x0, x1, x2, x3};
+    for (; i < n && ok; i++) {
+        bw.step();
+        const uint32_t e = tab[xs[i & 3] & 4095];
+        dst[i] = (uint8_t)e;
+        xs[i & 3] = dec_next(xs[i & 3], e);
+        ok = bw.renorm(xs[i & 3]);
+    }
+    if (!ok) dec_fail(infos, t.frame, D_CORRUPT);
+}
+
 // Adaptive bodies, eight per warp: lane group g (lanes 4g .. 4g + 3) of
 // block b decodes task list[8 b + g], lane 4g + l holding state l.  The warp
 // builds the eight models one after another (per model the symbol of every
@@ -522,6 +652,12 @@ __global__ void __launch_bounds__(32) k_dec_static(const DecTask* __restrict__ t
 // chains; the list is sorted by length (k_dec_lists), so a warp's chains
 // end close together.
 constexpr uint32_t kDecGroups = 8;
+// Batches of up to this many frames decode their adaptive bodies one per
+// warp (k_dec_adaptive1): at 13 such warps per SM their bodies all run at
+// once.  Measured on 1 MiB frames: 128 frames 29.4 ms one per warp against
+// 67 ms eight per warp; 2560 frames 89 ms (whole decode) eight per warp
+// against 97 ms.
+constexpr uint32_t kDecOneWarpFrames = 512;
 constexpr uint32_t kDecModel = 4096 + 256 * 4;
 constexpr uint32_t kDecAdaptiveSmem = kDecGroups * kDecModel + 256 * 2 + kDecGroups * 4;
 

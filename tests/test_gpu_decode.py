@@ -145,3 +145,18 @@ def test_corrupted_frames_fail_like_the_reference(comp, oracle):
             assert o == ref
         agree += 1
     assert agree > 300
+
+
+def test_batch_device_decode_many_frames(comp, oracle):
+    """More than 512 frames in one call: the adaptive bodies decode eight per
+    warp (the other tests' calls decode them one per warp).  640 frames of
+    every entropy-coded profile, sizes from 1 byte to 40 000, several
+    workloads, each equal to its input."""
+    kinds = ("markov", "table", "records", "uniform")
+    xs = [W.gen(kinds[i % 4], 300 + i, 1 + (i * 7919) % 40_000) for i in range(640)]
+    frames = [_frame(oracle, 1 + i % 3, a) for i, a in enumerate(xs)]
+    want = [bytes(a) for a in xs]
+    st, outs = _device_decode(comp, frames, [max(len(w), 1) for w in want])
+    assert list(st) == [0] * len(frames)
+    bad = [i for i, (o, w) in enumerate(zip(outs, want)) if o != w]
+    assert not bad, f"{len(bad)} frames differ, first {bad[0]}"
