@@ -192,8 +192,8 @@ def measured_peaks() -> tuple[float, str]:
 # from an ncu capture of the same kernel on the same workload at 128 frames
 # (315 606 784 / 208 174 588): its traffic grows with the symbols it encodes
 # and the bytes it emits, so it scales to a full launch by the launch's
-# algorithmic bytes.  The capture and its command are summarised in
-# profiles/k_rans_mixed128.md.
+# algorithmic bytes.  The capture and its command are summarised under
+# profiles/.
 RANS_TRAFFIC_PER_ALG_BYTE: float | None = 1.5161
 
 

@@ -1182,8 +1182,8 @@ int or_raw_literals_misparse(const uint8_t *lit, uint64_t n) {
     return rd32(lit + 4) == (uint32_t)(((uint64_t)rd32(lit) + 1) / 2);
 }
 
-/* Profiles P1 and P2.  P1 == match + tokenize + ANS frame (this build's
- * compress format):
+/* Profiles P1 and P2.  P1 == match + tokenize + ANS frame (the batch
+ * pipeline's entropy-coded frame format):
  *   header and Section 1 as P0;
  *   Section 2 = PackageCommandsSection(cmds) when cmds <= 2 MiB (every
  *     substream then fits the decoders' 2 MiB substream buffers), else
